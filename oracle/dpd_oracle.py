@@ -1,0 +1,179 @@
+"""ctypes binding of the CPU oracle (dpd_oracle.c) and a runner for the
+reference harness (ref_driver.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py, never by the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libdpd_oracle.so")
+REF_DRIVER = os.path.join(HERE, "_ref", "osprey_ref_driver")
+
+NOISE_LCG = 0
+NOISE_PHILOX = 1
+
+
+class _Params(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("wx", C.c_double), ("wy", C.c_double), ("wz", C.c_double),
+                ("dt", C.c_double), ("lam", C.c_double), ("kT", C.c_double),
+                ("ntypes", C.c_int32), ("a", C.POINTER(C.c_double)), ("gamma", C.POINTER(C.c_double)),
+                ("seed", C.c_uint64), ("noise", C.c_int32)]
+
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.dpdo_create.restype = vp
+        L.dpdo_create.argtypes = [C.POINTER(_Params)]
+        L.dpdo_destroy.argtypes = [vp]
+        L.dpdo_set_beads.argtypes = [vp, C.c_int64] + [vp] * 7
+        L.dpdo_set_topology.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
+        L.dpdo_step.argtypes = [vp, C.c_int64, C.c_int32]
+        L.dpdo_get.argtypes = [vp] + [vp] * 5
+        L.dpdo_get_cells.argtypes = [vp, vp]
+        L.dpdo_cell_errors.argtypes = [vp]
+        L.dpdo_cell_errors.restype = C.c_int64
+        L.dpdo_pair_count.argtypes = [vp]
+        L.dpdo_pair_count.restype = C.c_int64
+        L.dpdo_philox_pair.argtypes = [C.c_uint64, C.c_int64, C.c_uint32, C.c_uint32]
+        L.dpdo_philox_pair.restype = C.c_uint32
+        L.dpdo_set_dt.argtypes = [vp, C.c_double]
+        L.dpdo_set_pair.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class Oracle:
+    """One oracle simulation of a DpdSystem (osprey_dpd_b200.workloads)."""
+
+    def __init__(self, system, noise: int = NOISE_LCG, kT: float = None, gamma_scale: float = 1.0,
+                 seed: int = None):
+        L = lib()
+        self._a = np.ascontiguousarray(system.a, dtype=np.float64)
+        self._g = np.ascontiguousarray(system.gamma * gamma_scale, dtype=np.float64)
+        seed = abs(int(system.seed if seed is None else seed))
+        p = _Params(system.cells[0], system.cells[1], system.cells[2], *system.widths,
+                    system.dt, system.lam, float(system.kT if kT is None else kT),
+                    len(system.type_names), self._a.ctypes.data_as(C.POINTER(C.c_double)),
+                    self._g.ctypes.data_as(C.POINTER(C.c_double)), seed, noise)
+        self.h = L.dpdo_create(C.byref(p))
+        if not self.h:
+            raise RuntimeError("dpdo_create failed")
+        self.n = system.n
+        arrs = [np.ascontiguousarray(system.ids, np.int64), np.ascontiguousarray(system.types, np.int32),
+                np.ascontiguousarray(system.movable, np.uint8), np.ascontiguousarray(system.x, np.float64),
+                np.ascontiguousarray(system.unpbc, np.float64), np.ascontiguousarray(system.v, np.float64),
+                np.ascontiguousarray(system.f, np.float64)]
+        rc = L.dpdo_set_beads(self.h, self.n, *[_p(a) for a in arrs])
+        if rc != 0:
+            raise RuntimeError(f"dpdo_set_beads failed ({rc})")
+        t = [np.ascontiguousarray(system.bond_head, np.int64), np.ascontiguousarray(system.bond_tail, np.int64),
+             np.ascontiguousarray(system.bond_k2, np.float64), np.ascontiguousarray(system.bond_l0, np.float64),
+             np.ascontiguousarray(system.angle_first, np.int64), np.ascontiguousarray(system.angle_second, np.int64),
+             np.ascontiguousarray(system.angle_k3, np.float64), np.ascontiguousarray(system.angle_phi0, np.float64)]
+        rc = L.dpdo_set_topology(self.h, len(t[0]), _p(t[0]), _p(t[1]), _p(t[2]), _p(t[3]),
+                                 len(t[4]), _p(t[4]), _p(t[5]), _p(t[6]), _p(t[7]))
+        if rc != 0:
+            raise RuntimeError(f"dpdo_set_topology failed ({rc})")
+
+    def step(self, first_step: int, nsteps: int) -> None:
+        if lib().dpdo_step(self.h, first_step, nsteps) != 0:
+            raise RuntimeError("dpdo_step failed")
+
+    def state(self):
+        n = self.n
+        out = {k: np.zeros((n, 3)) for k in ("x", "unpbc", "v", "f")}
+        out["stress"] = np.zeros((n, 9))
+        lib().dpdo_get(self.h, _p(out["x"]), _p(out["unpbc"]), _p(out["v"]), _p(out["f"]), _p(out["stress"]))
+        return out
+
+    def cells(self) -> np.ndarray:
+        c = np.zeros(self.n, dtype=np.int32)
+        lib().dpdo_get_cells(self.h, _p(c))
+        return c
+
+    def cell_errors(self) -> int:
+        return int(lib().dpdo_cell_errors(self.h))
+
+    def pair_count(self) -> int:
+        return int(lib().dpdo_pair_count(self.h))
+
+    def set_dt(self, dt: float) -> None:
+        lib().dpdo_set_dt(self.h, dt)
+
+    def set_pair(self, ti: int, tj: int, a: float, gamma: float) -> None:
+        lib().dpdo_set_pair(self.h, ti, tj, a, gamma)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().dpdo_destroy(h)
+            self.h = None
+
+
+def philox_pair(seed: int, step: int, id_lo: int, id_hi: int) -> int:
+    return int(lib().dpdo_philox_pair(seed, step, id_lo, id_hi))
+
+
+def run_reference(system, steps: int, workdir: str = None, kT: float = None, gamma_scale: float = 1.0,
+                  inject: bool = True, dump: bool = True, topology: bool = False, timeout: float = None,
+                  rng_seed: int = None):
+    """Runs the unmodified reference (oracle/_ref/osprey_ref_driver) on
+    ``system`` for ``steps`` steps; ``rng_seed`` restarts its pair-noise LCG
+    at that value just before the step loop.  Returns (json summary, dump dict or None,
+    topology dict or None)."""
+    from osprey_dpd_b200 import workloads  # local import: test-side helper
+
+    if not os.path.exists(REF_DRIVER):
+        raise FileNotFoundError(REF_DRIVER)
+    own = workdir is None
+    wd = workdir or tempfile.mkdtemp(prefix="dpdref_")
+    run = "r"
+    workloads.write_dmpci(system, os.path.join(wd, "dmpci." + run), steps, kT=kT, gamma_scale=gamma_scale)
+    args = [REF_DRIVER, run]
+    if inject:
+        workloads.write_state(system, os.path.join(wd, "state.bin"))
+        args += ["--inject", "state.bin"]
+    if dump:
+        args += ["--dump", "out.bin"]
+    if topology:
+        args += ["--topology", "topo.bin"]
+    if rng_seed is not None:
+        args += ["--rng-seed", str(int(rng_seed))]
+    cp = subprocess.run(args, cwd=wd, capture_output=True, text=True, timeout=timeout)
+    if cp.returncode != 0:
+        raise RuntimeError(f"reference driver failed: {cp.stderr.strip()} {cp.stdout.strip()}")
+    line = [l for l in cp.stdout.splitlines() if l.startswith("{")][-1]
+    summary = json.loads(line)
+    d = workloads.read_dump(os.path.join(wd, "out.bin")) if dump else None
+    t = workloads.read_topology(os.path.join(wd, "topo.bin")) if topology else None
+    if own:
+        import shutil
+        shutil.rmtree(wd, ignore_errors=True)
+    return summary, d, t
