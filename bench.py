@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""DPD step throughput on one or more B200s, in bead-steps/s.
+
+Workload (default): the H3T6 lipid bilayer in water, 64x64x32 cells of unit
+width at density 3 -> 393,216 beads, 6,000 lipids (48,000 bonds, 24,000 tail
+bond pairs), a_ij of the reference's bilayer example, gamma = 4.5, kT = 1,
+dt = 0.02.  Synthetic, seeded (osprey_dpd_b200/workloads.py).
+
+A step is one full DPD timestep (UpdatePos, cell re-binning, pair forces,
+bond + bond-pair forces, UpdateMom).  `value` is the mixed-precision
+(FP32 forces, FP64 positions/velocities/sums) throughput with the state
+resident in HBM; the all-FP64 form is timed the same way.  L2 is flushed (a
+256 MiB write) before every timed step, each step is timed with CUDA events on
+the engine's stream, and the max over ranks is reported.  `e2e` is the same
+metric through the C ABI with host buffers: upload the bead state, run one
+reference sample period (100 steps), read back the single-bead sums and the
+full bead state.
+
+`--impl reference` times the reference itself: Osprey-DPD's own serial step
+loop, compiled from its sources (oracle/_ref), on the host cores.
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload
+(weak scaling; no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "bead-steps/s, 393k-bead bilayer: FP32/FP64-mixed vs all-FP64, 1 B200"
+UNIT = "bead-steps/s"
+E2E_PERIOD = 100          # SamplePeriod of the reference's bilayer example (examples/dmpci.bilayer)
+L2_FLUSH_BYTES = 256 << 20
+SLOTS_PER_BEAD_STEP = 755.0   # pair-force issue work per bead-step (half shell, rho = 3)
+ALG_BYTES_PER_BEAD_STEP = {"mixed": 124.0, "fp64": 148.0}   # whole-step algorithmic HBM bytes
+
+
+def workload(name: str, seed_offset: int = 0):
+    from osprey_dpd_b200 import workloads as W
+    if name == "bilayer":
+        s = W.bilayer(seed=W.BASE_SEED + 3 + 7919 * seed_offset)
+        desc = "H3T6 bilayer in water, 64x64x32 cells, 393,216 beads, 6,000 lipids"
+    elif name == "water":
+        s = W.water(10, seed=W.BASE_SEED + 1 + 7919 * seed_offset)
+        desc = "DPD water 10x10x10, 3,000 beads"
+    elif name == "binary":
+        s = W.binary_mixture(32, seed=W.BASE_SEED + 2 + 7919 * seed_offset)
+        desc = "A/B mixture 32^3, 98,304 beads, a_AB = 50"
+    elif name == "polymer":
+        s = W.polymer_solution(128, seed=W.BASE_SEED + 4 + 7919 * seed_offset)
+        desc = "16-bead chains (30%) in solvent, 128^3, 6,291,456 beads"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return s, desc
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(system, steps: int, timeout: float = 600.0) -> dict:
+    """Times the reference's own step loop (oracle/_ref) on `steps` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dpd_oracle
+    if os.path.exists(dpd_oracle.REF_DRIVER):
+        summary, _, _ = dpd_oracle.run_reference(system, steps, dump=False, timeout=timeout)
+        return {"value": summary["bead_steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{steps} steps of the full {system.n}-bead workload, reference step loop "
+                          f"(CSimBox::Run) timed without set-up, 1 thread",
+                "run_seconds": summary["run_seconds"]}
+    o = dpd_oracle.Oracle(system)
+    t0 = time.perf_counter()
+    o.step(1, steps)
+    dt = time.perf_counter() - t0
+    return {"value": system.n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} steps of the full {system.n}-bead workload, C restatement, 1 thread",
+            "run_seconds": dt}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return 0
+    system, desc = workload(args.workload)
+    # bounded sample: about a minute of the serial reference at most
+    per_step_est = system.n / 0.5e6
+    steps = max(1, min(args.steps, int(60.0 / per_step_est)))
+    cb = cpu_reference_sample(system, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": ws,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * cb["run_seconds"] / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": desc, "n_beads": system.n,
+                                                     "precision": "reference FP64"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool):
+    """Per-step device time (ms) with L2 flushed before each step."""
+    eng = engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
+    stream = torch.cuda.Stream(device=dev)
+    eng.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    t = 1
+    for _ in range(warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        eng.step(t, 1)
+        t += 1
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if profile:
+        eng.profile(True)
+    launches0 = eng.launch_count()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            evs[k][0].record(stream)
+        eng.step(t, 1)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+        t += 1
+    torch.cuda.synchronize(dev)
+    launches = eng.launch_count() - launches0
+    ms = [a.elapsed_time(b) for a, b in evs]
+    prof = eng.profile_read() if profile else None
+    status = eng.status()
+    eng.close()
+    return ms, prof, launches, status
+
+
+def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch):
+    """Reference-facing call sequence with host buffers: upload, one sample
+    period of steps, single-bead sums and the full state back to the host."""
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    ids, types, mov = pin(system.ids), pin(system.types), pin(system.movable)
+    x, u, v, f = pin(system.x), pin(system.unpbc), pin(system.v), pin(system.f)
+    out = {k: torch.empty((system.n, 3), dtype=torch.float64).pin_memory().numpy() for k in ("x", "u", "v", "f")}
+    eng = engine_mod.DpdEngine(system.cells, system.widths, system.dt, system.lam, system.kT, system.a,
+                               system.gamma, abs(int(system.seed)), precision, dev.index)
+    h2d = ids.nbytes + types.nbytes + mov.nbytes + x.nbytes + u.nbytes + v.nbytes + f.nbytes
+    d2h = sum(a.nbytes for a in out.values()) + 8 * 23
+    times = []
+    t = 1
+    for r in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        eng.upload_beads(ids, types, mov, x, u, v, f)
+        eng.upload_topology(system.bond_head, system.bond_tail, system.bond_k2, system.bond_l0,
+                            system.angle_first, system.angle_second, system.angle_k3, system.angle_phi0)
+        eng.step(t, E2E_PERIOD)
+        eng.observables()
+        eng.download_into(out["x"], out["u"], out["v"], out["f"])
+        t1 = time.perf_counter()
+        if r > 0:           # the first call also pays library/context start-up
+            times.append(t1 - t0)
+        t += E2E_PERIOD
+    eng.close()
+    topo_bytes = (system.bond_head.nbytes * 2 + system.bond_k2.nbytes * 2 +
+                  system.angle_first.nbytes * 2 + system.angle_k3.nbytes * 2)
+    return times, (h2d + topo_bytes) / E2E_PERIOD, d2h / E2E_PERIOD
+
+
+def read_traffic(n_beads: int):
+    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "pair_forces_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    per_bead = d.get("dram_bytes_per_bead")
+    return None if per_bead is None else per_bead * n_beads
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", default="bilayer", choices=["bilayer", "water", "binary", "polymer"])
+    ap.add_argument("--e2e-reps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=12, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    ws, rank, local = dist_info()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from osprey_dpd_b200 import engine as E
+
+    system, desc = workload(args.workload, seed_offset=rank)
+    peaks, peak_kind = load_peaks()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    results = {}
+    clocks = None
+    for prec_name, prec in (("mixed", E.MIXED), ("fp64", E.FP64)):
+        barrier()
+        sampler = ClockSampler(local) if prec_name == "mixed" else None
+        if sampler:
+            sampler.start()
+        torch.cuda.synchronize(dev)
+        ms, prof, launches, status = time_engine(E, system, prec, args.steps, args.warmup, dev, torch, True)
+        torch.cuda.synchronize(dev)
+        barrier()
+        if sampler:
+            clocks = sampler.stop()
+        total_ms = max_over_ranks(sum(ms))
+        results[prec_name] = {"ms": ms, "total_ms": total_ms, "prof": prof, "launches": launches,
+                              "status": status,
+                              "value": ws * system.n * args.steps / (total_ms / 1000.0)}
+
+    e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch)
+    e2e_t = max_over_ranks(sum(e2e_times))
+    e2e_value = ws * system.n * E2E_PERIOD * len(e2e_times) / e2e_t
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_reference_sample(system, args.cpu_steps)
+            cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    mixed = results["mixed"]
+    pair = mixed["prof"]["pair_forces"]
+    t_pair = pair["ms"] / max(pair["launches"], 1) / 1000.0
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    issue_peak = sms * 128 * sm_max * 1e6
+    achieved = SLOTS_PER_BEAD_STEP * system.n / t_pair
+    kern_share = {k: round(v["ms"] / max(sum(x["ms"] for x in mixed["prof"].values()), 1e-12), 4)
+                  for k, v in mixed["prof"].items() if v["launches"]}
+    step_s = mixed["total_ms"] / 1000.0 / args.steps
+    hbm_ach = ALG_BYTES_PER_BEAD_STEP["mixed"] * system.n / step_s
+    line = {
+        "metric": METRIC, "value": mixed["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 state",
+        "data": "synthetic (seeded generator, reference workload shapes)",
+        "config": {"workload": desc, "n_beads": system.n, "cells": list(system.cells), "dt": system.dt,
+                   "precision": "mixed", "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if ws > 1 else "single GPU"},
+        "fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
+                 "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]},
+        "roofline": {"bound": "issue", "kernel": "pair_forces (mixed)",
+                     "achieved": achieved / 1e9, "peak": issue_peak / 1e9, "unit": "Gslot/s",
+                     "frac": achieved / issue_peak,
+                     "peak_basis": f"{sms} SMs x 128 FP32/INT32 lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz)",
+                     "work_per_bead_step": SLOTS_PER_BEAD_STEP,
+                     "avg_launch_ms": t_pair * 1000.0,
+                     "traffic": read_traffic(system.n)},
+        "roofline_step_hbm": {"bound": "hbm", "achieved": hbm_ach / 1e9, "peak": float(peaks["hbm_gbs"]),
+                              "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),
+                              "bytes_per_bead_step": ALG_BYTES_PER_BEAD_STEP["mixed"], "basis": peak_kind},
+        "kernel_share": kern_share,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_step, "d2h_bytes_per_step": d2h_step,
+                "call": f"upload_beads + upload_topology + step({E2E_PERIOD}) + observables + download, host pinned "
+                        f"buffers", "reps": len(e2e_times)},
+        "gpu_launches": mixed["launches"],
+        "clocks": clocks,
+        "status_bits": {k: v["status"] for k, v in results.items()},
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

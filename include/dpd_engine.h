@@ -1,0 +1,178 @@
+/* dpd_engine.h -- C ABI of the B200 DPD step engine (libospreydpd_cuda.so).
+ *
+ * The engine replaces the body of Osprey-DPD's per-timestep loop,
+ * CSimBox::Evolve (SimBox.cpp:977-1120), i.e.
+ *   CCNTCell::UpdatePos    (CNTCell.cpp:1598-2262)
+ *   CCNTCell::UpdateForce  (CNTCell.cpp:877-1572, DPD branch 1103-1572)
+ *   CSimBox::AddBondForces / CBond::AddForce            (SimBox.cpp:1382-1417, Bond.cpp:111-162)
+ *   CSimBox::AddBondPairForces / CBondPair::AddForce    (SimBox.cpp:1423-1439, BondPair.cpp:138-286)
+ *   CCNTCell::UpdateMom    (CNTCell.cpp:2280-2310)
+ *   CSimBox::CNTCellCheck  (SimBox.cpp:1365-1371, CNTCell.cpp:2628-2700)
+ * plus the single-bead sums of CMonitor::CalculateSingleBeadData
+ * (Monitor.cpp:790-1040) that the host needs on sample steps.
+ *
+ * Conventions: plain pointers and sizes, no CUDA or C++ types.  Every call
+ * returns 0 on success or a negative DPD_E* code; dpd_engine_last_error()
+ * gives the message.  Host arrays are in bead-upload order (the reference's
+ * bead-vector order, i.e. bead id order), xyz interleaved ("x3" = n*3).
+ * One CUDA stream per engine; calls on one engine are not re-entrant.
+ * The reference has no FFI of its own: the entry points below are the seam of
+ * the CSimBox/CCNTCell/CBond/CBondPair classes, one call per responsibility.
+ */
+#ifndef DPD_ENGINE_H
+#define DPD_ENGINE_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DPD_API __attribute__((visibility("default")))
+#else
+#define DPD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPD_OK                 0
+#define DPD_E_ARG             -1   /* invalid argument                       */
+#define DPD_E_CUDA            -2   /* CUDA runtime error                     */
+#define DPD_E_STATE           -3   /* call out of order (e.g. step before upload) */
+#define DPD_E_BOX             -4   /* bead outside the box at upload          */
+#define DPD_E_STATUS          -5   /* device status word reported a fatal condition */
+#define DPD_E_NOMEM           -6   /* host or device allocation failed       */
+
+#define DPD_PRECISION_MIXED    0   /* FP32 pair/bond forces, FP64 x, v and sums */
+#define DPD_PRECISION_FP64     1   /* everything FP64                          */
+
+/* Device status bits, OR-ed by the kernels (dpd_engine_status). */
+#define DPD_STATUS_CELL_SKIP      0x1u  /* a bead is filed in a cell other than floor(x/w):
+                                            it moved more than one cell in a step (the
+                                            reference logs CLogCNTBeadError, CNTCell.cpp:2650) */
+#define DPD_STATUS_NONFINITE      0x2u  /* a non-finite position, velocity or force       */
+#define DPD_STATUS_IMAGE_OVERFLOW 0x4u  /* a periodic image counter left +-511 box lengths */
+#define DPD_STATUS_FATAL_MASK     (DPD_STATUS_NONFINITE | DPD_STATUS_IMAGE_OVERFLOW)
+
+/* Kernel ids for dpd_engine_profile_read (the kernels of one step, in order). */
+#define DPD_KERNEL_UPDATE_POS   0   /* UpdatePos drift + cell move             */
+#define DPD_KERNEL_SCAN_CELLS   1   /* cell start offsets                      */
+#define DPD_KERNEL_PERMUTE      2   /* arrival slot -> new slot                */
+#define DPD_KERNEL_GATHER       3   /* cell-sorted state + force shadows       */
+#define DPD_KERNEL_PAIR_FORCES  4   /* DPD pair forces (UpdateForce)           */
+#define DPD_KERNEL_UPDATE_MOM   5   /* bonded forces + UpdateMom + sums        */
+#define DPD_KERNEL_REDUCE_OBS   6   /* final FP64 sums                         */
+#define DPD_KERNEL_DOWNLOAD     7   /* slot order -> bead order                */
+#define DPD_KERNEL_KINETIC      8   /* kinetic sums without a step             */
+#define DPD_NUM_KERNELS         9
+
+typedef struct dpd_engine dpd_engine;
+
+/* Parameters of CCNTCell::SetSimBoxLengths / SetTimeStepConstants /
+ * SetDPDBeadStructure / SetRNGSeed (CNTCell.cpp:134-203, SimState.cpp:69-95). */
+typedef struct dpd_params {
+    int32_t nx, ny, nz;       /* CNT cells per axis; each >= 3                      */
+    double  wx, wy, wz;       /* CNT cell widths; each >= 1 (the cut-off is 1)       */
+    double  dt, lambda, kT;   /* Step, Lambda, Temp                                  */
+    int32_t ntypes;           /* bead types, 1..32                                   */
+    const double* a;          /* ntypes*ntypes a_ij, row-major, symmetric            */
+    const double* gamma;      /* ntypes*ntypes gamma_ij                              */
+    uint64_t seed;            /* pair-noise seed (|RNGSeed|)                          */
+    int32_t precision;        /* DPD_PRECISION_*                                     */
+    int32_t device;           /* CUDA device ordinal, or -1 for the current device   */
+} dpd_params;
+
+/* Single-bead sums of CMonitor::CalculateSingleBeadData (Monitor.cpp:790-1040),
+ * accumulated in FP64 on the device at the end of the last dpd_engine_step. */
+typedef struct dpd_obs {
+    int64_t step;             /* m_SimTime of the state the sums describe             */
+    int64_t n;
+    double  sum_v[3];         /* sum of momenta (mass 1)                              */
+    double  sum_v2[3];        /* sum of squared momenta per axis                      */
+    double  virial[9];        /* sum of per-bead m_Stress (pair + bond), row-major    */
+    double  sum_x[3];         /* sum of positions                                     */
+    double  ang_mom[3];       /* sum of x cross v                                     */
+    double  kT;               /* (sum v^2)/(3N)                    Monitor.cpp:979     */
+    double  pressure;         /* (sum v^2 + trace virial)/(3V)     Monitor.cpp:981-982 */
+    int32_t has_virial;       /* 0 if no step has run since upload                    */
+    int32_t pad;
+} dpd_obs;
+
+/* Creates an engine for one box.  Replaces the CCNTCell statics set in
+ * CSimState::CSimState (SimState.cpp:55-110). */
+DPD_API int dpd_engine_create(const dpd_params* params, dpd_engine** out);
+
+/* Copies the beads in (ownership stays with the caller).  Replaces
+ * CSimBox::MakeCNTCells + AssignBeadstoCells (SimBox.cpp:715-877): beads are
+ * binned with the reference's (long)(x/w) rule.  movable may be NULL (all
+ * movable); unpbc3 may be NULL (= x3); f3 may be NULL (= 0). */
+DPD_API int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
+                            const uint8_t* movable, const double* x3, const double* unpbc3,
+                            const double* v3, const double* f3);
+
+/* Bonds (CBond: head id, tail id, k2, l0; Bond.h:45-52) and bond pairs
+ * (CBondPair: indices of its first and second bond in this bond list, k3,
+ * phi0 in radians; BondPair.h:23-30). */
+DPD_API int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_head_id,
+                               const int64_t* bond_tail_id, const double* k2, const double* l0,
+                               int64_t na, const int64_t* first_bond, const int64_t* second_bond,
+                               const double* k3, const double* phi0);
+
+/* Replaces the whole a_ij / gamma_ij tables (CCNTCell::SetDPDBeadConsInt /
+ * SetDPDBeadDissInt, CNTCell.cpp:434-456, and AddDPDBeadType, :498). */
+DPD_API int dpd_engine_set_pair_params(dpd_engine* e, int32_t ntypes, const double* a, const double* gamma);
+
+/* CCNTCell::ChangeTimeStepConstants (CNTCell.cpp:357): ignored unless dt > 0. */
+DPD_API int dpd_engine_set_dt(dpd_engine* e, double dt);
+
+/* CCNTCell::ToggleDPDBeadThermostat (CNTCell.cpp:318): on = 0 zeroes gamma
+ * (dissipative and random forces), on = 1 restores it. */
+DPD_API int dpd_engine_set_thermostat(dpd_engine* e, int32_t on);
+
+/* CCNTCell::ToggleDPDBeadConservativeForces (CNTCell.cpp:235). */
+DPD_API int dpd_engine_set_conservative(dpd_engine* e, int32_t on);
+
+/* Runs nsteps timesteps; first_step is the reference's m_SimTime of the first
+ * (it keys the pair noise).  Asynchronous: returns once the work is queued.
+ * The single-bead sums are taken at the end of the last step. */
+DPD_API int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps);
+
+/* Waits for queued work; returns the device status bits seen so far. */
+DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
+
+/* Copies the state out (synchronous); any pointer may be NULL.  stress9 is
+ * the per-bead virial of the last step (pair part split evenly between the
+ * two beads of a pair; bond part on the head bead as Bond.cpp:151-160). */
+DPD_API int dpd_engine_download(dpd_engine* e, double* x3, double* unpbc3, double* v3, double* f3,
+                        double* stress9);
+
+/* Index of the CNT cell each bead is filed in (nx*(ny*iz+iy)+ix). */
+DPD_API int dpd_engine_cells(dpd_engine* e, int32_t* cell);
+
+/* Single-bead sums of the last step (synchronous). */
+DPD_API int dpd_engine_observables(dpd_engine* e, dpd_obs* out);
+
+/* Queues all further work on the caller's CUDA stream (a cudaStream_t passed
+ * as a plain pointer; NULL returns to the engine's own stream).  The stream
+ * must belong to the engine's device and outlive its use. */
+DPD_API int dpd_engine_set_stream(dpd_engine* e, void* cuda_stream);
+
+/* on = 1 starts recording CUDA events around every kernel the engine queues
+ * (clearing earlier records); on = 0 stops.  Timing only, no extra sync. */
+DPD_API int dpd_engine_profile(dpd_engine* e, int32_t on);
+
+/* Waits for queued work and returns, per DPD_KERNEL_* id, the summed kernel
+ * time in ms and the number of timed launches since profiling was switched on.
+ * Both arrays hold DPD_NUM_KERNELS entries; either may be NULL. */
+DPD_API int dpd_engine_profile_read(dpd_engine* e, double* total_ms, int64_t* launches);
+
+/* Kernel launches the engine has queued since creation. */
+DPD_API int64_t dpd_engine_launch_count(const dpd_engine* e);
+
+DPD_API const char* dpd_engine_last_error(const dpd_engine* e);
+DPD_API void dpd_engine_destroy(dpd_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DPD_ENGINE_H */

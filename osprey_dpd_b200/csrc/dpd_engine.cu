@@ -1,0 +1,851 @@
+// dpd_engine.cu -- host runtime of the B200 DPD step engine and its C ABI
+// (include/dpd_engine.h).  It owns the device state, queues one timestep as a
+// fixed sequence of kernels on one CUDA stream, and translates between the
+// reference's bead-object view (bead-vector order, FP64 xyz triplets) and the
+// device's cell-sorted structure-of-arrays.
+#include "../../include/dpd_engine.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dpd_kernels.cuh"
+
+using namespace dpd;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPairThreads = 128;
+
+inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct dpd_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    dpd_params params{};
+    int precision = DPD_PRECISION_MIXED;
+    std::vector<double> a, gamma, gamma_backup, a_backup;   // host copies of the tables
+    bool thermostat_on = true, conservative_on = true;
+    int32_t ntypes = 0;
+    int64_t ncell = 0;
+    int nchunk = 0;
+    int64_t n = 0;
+    int64_t launches = 0;
+    bool uploaded = false;
+    bool stepped = false;
+    int64_t last_step = 0;      // m_SimTime of the state on the device
+    int cur = 0;                // which of the double buffers holds the state
+    std::string err;
+
+    // device state
+    StepConst* d_K = nullptr;
+    void* d_tab = nullptr;      // 3 * T*T of real: a, gamma, sigma
+    int64_t* d_step = nullptr;
+    unsigned* d_status = nullptr;
+    double* d_x[2] = {nullptr, nullptr};
+    double* d_v[2] = {nullptr, nullptr};
+    int* d_bid[2] = {nullptr, nullptr};
+    int* d_tf[2] = {nullptr, nullptr};
+    uint32_t* d_img[2] = {nullptr, nullptr};
+    int* d_cell[2] = {nullptr, nullptr};
+    void* d_F = nullptr;        // current force, slot order (real)
+    void* d_Fold = nullptr;     // previous force, slot order (real)
+    void* d_stress = nullptr;   // per-bead virial of the last sample step (real, 9 planes)
+    void* d_pos4 = nullptr;
+    void* d_vel4 = nullptr;
+    int* d_rank = nullptr;
+    int* d_perm = nullptr;
+    int* d_slot_of = nullptr;
+    int* d_pid_of = nullptr;
+    double* d_off = nullptr;
+    int* d_count = nullptr;
+    int* d_start = nullptr;
+    int* d_block_count = nullptr;
+    double* d_partials = nullptr;
+    double* d_obs = nullptr;
+    // download staging
+    double* d_out = nullptr;    // 3n x, 3n u, 3n v, 3n f, 9n stress
+    int* d_out_cell = nullptr;
+    // topology
+    int* d_csr_ptr = nullptr;
+    int* d_csr_term = nullptr;
+    int* d_bond_h = nullptr;
+    int* d_bond_t = nullptr;
+    double* d_bond_k2 = nullptr;
+    double* d_bond_l0 = nullptr;
+    int* d_ang[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* d_ang_k3 = nullptr;
+    double* d_ang_cos0 = nullptr;
+    double* d_ang_sin0 = nullptr;
+    // pinned host
+    int64_t* h_step = nullptr;
+    unsigned* h_status = nullptr;
+    double* h_obs = nullptr;
+    bool obs_valid = false;
+    bool obs_has_virial = false;
+
+    std::vector<void*> allocations;
+
+    // caller-provided stream (dpd_engine_set_stream) and kernel timing
+    cudaStream_t user_stream = nullptr;
+    bool profiling = false;
+    struct ProfRec { int kernel; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof;          // recorded since profiling was switched on
+    std::vector<cudaEvent_t> event_pool;
+
+    cudaStream_t s() const { return user_stream ? user_stream : stream; }
+};
+
+namespace {
+
+int fail(dpd_engine* e, int code, const std::string& msg)
+{
+    if (e) e->err = msg;
+    return code;
+}
+
+#define CU(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess)                                                              \
+            return fail(e, DPD_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+template <typename T>
+int dalloc(dpd_engine* e, T** p, size_t count)
+{
+    void* q = nullptr;
+    cudaError_t rc = cudaMalloc(&q, count ? count * sizeof(T) : sizeof(T));
+    if (rc != cudaSuccess) return fail(e, DPD_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(rc));
+    e->allocations.push_back(q);
+    *p = static_cast<T*>(q);
+    return DPD_OK;
+}
+
+void dfree(dpd_engine* e, void* p)
+{
+    if (!p) return;
+    auto it = std::find(e->allocations.begin(), e->allocations.end(), p);
+    if (it != e->allocations.end()) {
+        cudaFree(p);
+        e->allocations.erase(it);
+    }
+}
+
+size_t real_size(const dpd_engine* e) { return e->precision == DPD_PRECISION_FP64 ? sizeof(double) : sizeof(float); }
+
+int check_launch(dpd_engine* e, const char* what)
+{
+    ++e->launches;
+    cudaError_t rc = cudaGetLastError();
+    if (rc != cudaSuccess) return fail(e, DPD_E_CUDA, std::string(what) + ": " + cudaGetErrorString(rc));
+    return DPD_OK;
+}
+
+// Host mirror of StepConst and the pair tables (CCNTCell::SetTimeStepConstants,
+// CNTCell.cpp:180-203; sigma_ij = sqrt(gamma_ij) * sqrt(24 kT / dt), CNTCell.cpp:190,1220).
+int push_constants(dpd_engine* e)
+{
+    const dpd_params& p = e->params;
+    StepConst K{};
+    K.dt = p.dt;
+    K.halfdt = 0.5 * p.dt;
+    K.halfdt2 = 0.5 * p.dt * p.dt;
+    K.lamdt = p.lambda * p.dt;
+    K.invrootdt = std::sqrt(24.0 * p.kT / p.dt);
+    K.nc[0] = p.nx; K.nc[1] = p.ny; K.nc[2] = p.nz;
+    K.w[0] = p.wx; K.w[1] = p.wy; K.w[2] = p.wz;
+    for (int d = 0; d < 3; ++d) K.L[d] = (double)K.nc[d] * K.w[d];
+    K.ntypes = e->ntypes;
+    K.seed = p.seed;
+    const int m = e->ntypes * e->ntypes;
+    std::vector<double> tab(3 * (size_t)m);
+    for (int k = 0; k < m; ++k) {
+        const double a = e->conservative_on ? e->a[k] : 0.0;
+        const double g = e->thermostat_on ? e->gamma[k] : 0.0;
+        tab[k] = a;
+        tab[m + k] = g;
+        tab[2 * m + k] = std::sqrt(g) * K.invrootdt;
+    }
+    CU(cudaStreamSynchronize(e->s()));   // tables may be in use by queued work
+    CU(cudaMemcpy(e->d_K, &K, sizeof K, cudaMemcpyHostToDevice));
+    if (e->precision == DPD_PRECISION_FP64) {
+        CU(cudaMemcpy(e->d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> tf(tab.begin(), tab.end());
+        CU(cudaMemcpy(e->d_tab, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return DPD_OK;
+}
+
+cudaEvent_t take_event(dpd_engine* e)
+{
+    if (!e->event_pool.empty()) {
+        cudaEvent_t ev = e->event_pool.back();
+        e->event_pool.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    return ev;
+}
+
+// Brackets one kernel launch with events when profiling is on.
+struct Timed {
+    dpd_engine* e;
+    int kernel;
+    cudaEvent_t a = nullptr;
+    Timed(dpd_engine* eng, int k) : e(eng), kernel(k)
+    {
+        if (e->profiling && (a = take_event(e))) cudaEventRecord(a, e->s());
+    }
+    ~Timed()
+    {
+        if (!a) return;
+        cudaEvent_t b = take_event(e);
+        if (!b) { e->event_pool.push_back(a); return; }
+        cudaEventRecord(b, e->s());
+        e->prof.push_back({kernel, a, b});
+    }
+};
+
+template <typename real>
+int queue_step(dpd_engine* e, bool sample)
+{
+    typedef typename Vec4<real>::type V4;
+    const int n = (int)e->n;
+    const int a = e->cur, b = 1 - e->cur;
+    const int nb = blocks_for(n, kThreads);
+    const int npb = blocks_for(n, kPairThreads);
+    cudaStream_t st = e->s();
+    int rc;
+    {
+        Timed t(e, DPD_KERNEL_UPDATE_POS);
+        k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_x[a], e->d_v[a], (const real*)e->d_F,
+                                                    e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
+                                                    e->d_block_count, e->d_status);
+    }
+    if ((rc = check_launch(e, "k_update_pos"))) return rc;
+    {
+        Timed t(e, DPD_KERNEL_SCAN_CELLS);
+        k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, n, e->d_count, e->d_block_count,
+                                                          e->d_start);
+    }
+    if ((rc = check_launch(e, "k_scan_cells"))) return rc;
+    {
+        Timed t(e, DPD_KERNEL_PERMUTE);
+        k_permute<<<blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st>>>(
+            n, e->nchunk, e->d_cell[a], e->d_rank, e->d_start, e->d_perm, e->d_block_count);
+    }
+    if ((rc = check_launch(e, "k_permute"))) return rc;
+    {
+        Timed t(e, DPD_KERNEL_GATHER);
+        k_gather<real><<<nb, kThreads, 0, st>>>(
+            n, e->d_K, e->d_perm, e->d_start, e->d_x[a], e->d_v[a], (const real*)e->d_F, e->d_bid[a],
+            e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
+            e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_slot_of, e->d_pid_of, (V4*)e->d_pos4, (V4*)e->d_vel4);
+    }
+    if ((rc = check_launch(e, "k_gather"))) return rc;
+    {
+        Timed t(e, DPD_KERNEL_PAIR_FORCES);
+        auto kern = sample ? k_pair_forces_ref<real, true> : k_pair_forces_ref<real, false>;
+        kern<<<npb, kPairThreads, 0, st>>>(n, e->d_K, e->d_step, (const real*)e->d_tab, e->d_cell[b],
+                                            e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
+                                            (real*)e->d_F, (real*)e->d_stress);
+    }
+    if ((rc = check_launch(e, "k_pair_forces"))) return rc;
+    const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
+                        e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_ang_k3, e->d_ang_cos0,
+                        e->d_ang_sin0, e->d_off};
+    {
+        Timed t(e, DPD_KERNEL_UPDATE_MOM);
+        auto kern = sample ? k_update_mom<real, true> : k_update_mom<real, false>;
+        kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
+                                       (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_img[b],
+                                       e->d_slot_of, topo, (real*)e->d_stress, e->d_partials, e->d_status);
+    }
+    if ((rc = check_launch(e, "k_update_mom"))) return rc;
+    if (sample) {
+        {
+            Timed t(e, DPD_KERNEL_REDUCE_OBS);
+            k_reduce_obs<<<1, 256, 0, st>>>(nb, e->d_partials, e->d_obs);
+        }
+        if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
+    }
+    e->cur = b;
+    return DPD_OK;
+}
+
+void release_topology(dpd_engine* e)
+{
+    int** ip[] = {&e->d_csr_ptr, &e->d_csr_term, &e->d_bond_h, &e->d_bond_t,
+                  &e->d_ang[0], &e->d_ang[1], &e->d_ang[2], &e->d_ang[3]};
+    for (auto q : ip) { dfree(e, *q); *q = nullptr; }
+    double** dp[] = {&e->d_bond_k2, &e->d_bond_l0, &e->d_ang_k3, &e->d_ang_cos0, &e->d_ang_sin0};
+    for (auto q : dp) { dfree(e, *q); *q = nullptr; }
+}
+
+// Empty topology: csr_ptr all zero.
+int empty_topology(dpd_engine* e)
+{
+    release_topology(e);
+    int rc;
+    if ((rc = dalloc(e, &e->d_csr_ptr, (size_t)e->n + 1))) return rc;
+    CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
+    return DPD_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+
+extern "C" {
+
+int dpd_engine_create(const dpd_params* p, dpd_engine** out)
+{
+    dpd_engine* e = nullptr;
+    if (!out) return DPD_E_ARG;
+    *out = nullptr;
+    if (!p || p->nx < 3 || p->ny < 3 || p->nz < 3 || !(p->wx >= 1.0) || !(p->wy >= 1.0) || !(p->wz >= 1.0) ||
+        !(p->dt > 0.0) || p->lambda < 0.0 || p->kT < 0.0 || p->ntypes < 1 || p->ntypes > kMaxTypes || !p->a ||
+        !p->gamma || (p->precision != DPD_PRECISION_MIXED && p->precision != DPD_PRECISION_FP64))
+        return DPD_E_ARG;
+    const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+    if (ncell > (int64_t)1 << 30) return DPD_E_ARG;
+    e = new (std::nothrow) dpd_engine();
+    if (!e) return DPD_E_NOMEM;
+    e->params = *p;
+    e->params.a = nullptr;
+    e->params.gamma = nullptr;
+    e->precision = p->precision;
+    e->ntypes = p->ntypes;
+    const int m = p->ntypes * p->ntypes;
+    e->a.assign(p->a, p->a + m);
+    e->gamma.assign(p->gamma, p->gamma + m);
+    e->ncell = ncell;
+    e->nchunk = (int)((ncell + kScanChunk - 1) / kScanChunk);
+    int rc = DPD_OK;
+    do {
+        if (p->device >= 0) {
+            if (cudaSetDevice(p->device) != cudaSuccess) { rc = fail(e, DPD_E_CUDA, "cudaSetDevice failed"); break; }
+            e->device = p->device;
+        } else if (cudaGetDevice(&e->device) != cudaSuccess) {
+            rc = fail(e, DPD_E_CUDA, "no CUDA device");
+            break;
+        }
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = fail(e, DPD_E_CUDA, "cudaStreamCreate failed");
+            break;
+        }
+        if ((rc = dalloc(e, &e->d_K, 1))) break;
+        if ((rc = dalloc(e, (char**)&e->d_tab, 3 * (size_t)kMaxTypes * kMaxTypes * sizeof(double)))) break;
+        if ((rc = dalloc(e, &e->d_step, 1))) break;
+        if ((rc = dalloc(e, &e->d_status, 1))) break;
+        if ((rc = dalloc(e, &e->d_count, (size_t)ncell))) break;
+        if ((rc = dalloc(e, &e->d_start, (size_t)ncell + 1))) break;
+        if ((rc = dalloc(e, &e->d_block_count, (size_t)e->nchunk))) break;
+        if ((rc = dalloc(e, &e->d_obs, kObsTerms))) break;
+        if (cudaMallocHost(&e->h_step, sizeof(int64_t)) != cudaSuccess ||
+            cudaMallocHost(&e->h_status, sizeof(unsigned)) != cudaSuccess ||
+            cudaMallocHost(&e->h_obs, kObsTerms * sizeof(double)) != cudaSuccess) {
+            rc = fail(e, DPD_E_NOMEM, "cudaMallocHost failed");
+            break;
+        }
+        if (cudaMemset(e->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
+            cudaMemset(e->d_count, 0, sizeof(int) * ncell) != cudaSuccess ||
+            cudaMemset(e->d_block_count, 0, sizeof(int) * e->nchunk) != cudaSuccess ||
+            cudaMemset(e->d_step, 0, sizeof(int64_t)) != cudaSuccess) {
+            rc = fail(e, DPD_E_CUDA, "cudaMemset failed");
+            break;
+        }
+        if ((rc = push_constants(e))) break;
+    } while (0);
+    if (rc != DPD_OK) {
+        // keep the message readable through a half-built engine
+        fprintf(stderr, "dpd_engine_create: %s\n", e->err.c_str());
+        dpd_engine_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return DPD_OK;
+}
+
+void dpd_engine_destroy(dpd_engine* e)
+{
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->user_stream) cudaStreamSynchronize(e->user_stream);
+    for (auto& r : e->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
+    for (void* p : e->allocations) cudaFree(p);
+    e->allocations.clear();
+    if (e->h_step) cudaFreeHost(e->h_step);
+    if (e->h_status) cudaFreeHost(e->h_status);
+    if (e->h_obs) cudaFreeHost(e->h_obs);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* dpd_engine_last_error(const dpd_engine* e) { return e ? e->err.c_str() : "null engine"; }
+
+int dpd_engine_set_stream(dpd_engine* e, void* cuda_stream)
+{
+    if (!e) return DPD_E_ARG;
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));   // finish work queued on the old stream
+    e->user_stream = static_cast<cudaStream_t>(cuda_stream);
+    return DPD_OK;
+}
+
+int dpd_engine_profile(dpd_engine* e, int32_t on)
+{
+    if (!e) return DPD_E_ARG;
+    CU(cudaSetDevice(e->device));
+    if (on) {
+        CU(cudaStreamSynchronize(e->s()));
+        for (auto& r : e->prof) { e->event_pool.push_back(r.a); e->event_pool.push_back(r.b); }
+        e->prof.clear();
+    }
+    e->profiling = on != 0;
+    return DPD_OK;
+}
+
+int dpd_engine_profile_read(dpd_engine* e, double* total_ms, int64_t* launches)
+{
+    if (!e) return DPD_E_ARG;
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    double ms[DPD_NUM_KERNELS] = {0};
+    int64_t cnt[DPD_NUM_KERNELS] = {0};
+    for (auto& r : e->prof) {
+        float t = 0.f;
+        CU(cudaEventElapsedTime(&t, r.a, r.b));
+        if (r.kernel >= 0 && r.kernel < DPD_NUM_KERNELS) {
+            ms[r.kernel] += t;
+            cnt[r.kernel] += 1;
+        }
+    }
+    for (int k = 0; k < DPD_NUM_KERNELS; ++k) {
+        if (total_ms) total_ms[k] = ms[k];
+        if (launches) launches[k] = cnt[k];
+    }
+    return DPD_OK;
+}
+
+int64_t dpd_engine_launch_count(const dpd_engine* e) { return e ? e->launches : -1; }
+
+int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
+                            const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
+                            const double* f3)
+{
+    if (!e) return DPD_E_ARG;
+    if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    const dpd_params& p = e->params;
+    const double L[3] = {p.nx * p.wx, p.ny * p.wy, p.nz * p.wz};
+    const double w[3] = {p.wx, p.wy, p.wz};
+    const int nc[3] = {p.nx, p.ny, p.nz};
+    // CSimBox::AssignBeadstoCells (SimBox.cpp:715-762): ix = (long)(x/w)
+    std::vector<int> cell(n);
+    std::vector<double> off;
+    bool any_off = false;
+    std::vector<uint32_t> img(n);
+    for (int64_t b = 0; b < n; ++b) {
+        if (type[b] < 0 || type[b] >= e->ntypes) return fail(e, DPD_E_ARG, "bead type out of range");
+        if (id[b] < 1 || id[b] > 0x7fffffff) return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
+        int64_t ci[3];
+        for (int d = 0; d < 3; ++d) {
+            const double xv = x3[3 * b + d];
+            if (!std::isfinite(xv) || !std::isfinite(v3[3 * b + d])) return fail(e, DPD_E_BOX, "non-finite bead state");
+            ci[d] = (int64_t)(xv / w[d]);
+            if (xv < 0.0 || ci[d] < 0 || ci[d] >= nc[d]) {
+                char msg[160];
+                snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)b, (long long)id[b]);
+                return fail(e, DPD_E_BOX, msg);
+            }
+        }
+        cell[b] = (int)(ci[0] + (int64_t)nc[0] * (ci[1] + (int64_t)nc[1] * ci[2]));
+        int ii[3] = {0, 0, 0};
+        if (unpbc3) {
+            for (int d = 0; d < 3; ++d) {
+                const double du = unpbc3[3 * b + d] - x3[3 * b + d];
+                const double k = std::nearbyint(du / L[d]);
+                if (!(std::fabs(k) <= 511.0)) return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
+                ii[d] = (int)k;
+                const double r = du - k * L[d];
+                if (r != 0.0) any_off = true;
+            }
+        }
+        img[b] = img_pack(ii[0], ii[1], ii[2]);
+    }
+    if (any_off) {
+        off.assign(3 * (size_t)n, 0.0);
+        for (int64_t b = 0; b < n; ++b)
+            for (int d = 0; d < 3; ++d) {
+                const double du = unpbc3[3 * b + d] - x3[3 * b + d];
+                off[(size_t)d * n + b] = du - (double)img_get(img[b], d) * L[d];
+            }
+    }
+    // slot order: by cell, then by upload index (stable counting sort)
+    std::vector<int64_t> start(e->ncell + 1, 0);
+    for (int64_t b = 0; b < n; ++b) start[cell[b] + 1]++;
+    for (int64_t c = 0; c < e->ncell; ++c) start[c + 1] += start[c];
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    std::vector<int> slot_of(n), order(n);
+    for (int64_t b = 0; b < n; ++b) {
+        const int64_t s = fill[cell[b]]++;
+        slot_of[b] = (int)s;
+        order[s] = (int)b;
+    }
+    // (re)allocate per-bead buffers
+    if (e->n != n) {
+        void** bufs[] = {(void**)&e->d_x[0], (void**)&e->d_x[1], (void**)&e->d_v[0], (void**)&e->d_v[1],
+                         (void**)&e->d_bid[0], (void**)&e->d_bid[1], (void**)&e->d_tf[0], (void**)&e->d_tf[1],
+                         (void**)&e->d_img[0], (void**)&e->d_img[1], (void**)&e->d_cell[0], (void**)&e->d_cell[1],
+                         &e->d_F, &e->d_Fold, &e->d_stress, &e->d_pos4, &e->d_vel4, (void**)&e->d_rank,
+                         (void**)&e->d_perm, (void**)&e->d_slot_of, (void**)&e->d_pid_of, (void**)&e->d_partials,
+                         (void**)&e->d_out, (void**)&e->d_out_cell};
+        for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
+        const size_t rs = real_size(e);
+        int rc;
+        for (int k = 0; k < 2; ++k) {
+            if ((rc = dalloc(e, &e->d_x[k], 3 * (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_v[k], 3 * (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_bid[k], (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_tf[k], (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_img[k], (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_cell[k], (size_t)n))) return rc;
+        }
+        if ((rc = dalloc(e, (char**)&e->d_F, 3 * rs * (size_t)n))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_Fold, 3 * rs * (size_t)n))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_stress, 9 * rs * (size_t)n))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_pos4, 4 * rs * (size_t)n))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_vel4, 4 * rs * (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_rank, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_perm, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_slot_of, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_pid_of, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(n, kThreads) * kObsTerms))) return rc;
+        if ((rc = dalloc(e, &e->d_out, 21 * (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
+        e->n = n;
+    }
+    dfree(e, e->d_off);
+    e->d_off = nullptr;
+    if (any_off) {
+        int rc;
+        if ((rc = dalloc(e, &e->d_off, 3 * (size_t)n))) return rc;
+        CU(cudaMemcpy(e->d_off, off.data(), off.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // host staging in slot order
+    std::vector<double> hx(3 * n), hv(3 * n), hf(3 * n);
+    std::vector<int> hbid(n), htf(n), hcell(n), hpid(n);
+    std::vector<uint32_t> himg(n);
+    for (int64_t s = 0; s < n; ++s) {
+        const int b = order[s];
+        for (int d = 0; d < 3; ++d) {
+            hx[(size_t)d * n + s] = x3[3 * b + d];
+            hv[(size_t)d * n + s] = v3[3 * b + d];
+            hf[(size_t)d * n + s] = f3 ? f3[3 * b + d] : 0.0;
+        }
+        hbid[s] = b;
+        htf[s] = type[b] | ((movable && !movable[b]) ? (1 << 16) : 0);
+        hcell[s] = cell[b];
+        himg[s] = img[b];
+    }
+    for (int64_t b = 0; b < n; ++b) hpid[b] = (int)id[b];
+    const int c = e->cur;
+    CU(cudaMemcpy(e->d_x[c], hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_v[c], hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (e->precision == DPD_PRECISION_FP64) {
+        CU(cudaMemcpy(e->d_F, hf.data(), hf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> ff(hf.begin(), hf.end());
+        CU(cudaMemcpy(e->d_F, ff.data(), ff.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    CU(cudaMemcpy(e->d_bid[c], hbid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_tf[c], htf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_cell[c], hcell.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_img[c], himg.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_slot_of, slot_of.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_pid_of, hpid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    std::vector<int> st32(e->ncell + 1);
+    for (int64_t k = 0; k <= e->ncell; ++k) st32[k] = (int)start[k];
+    CU(cudaMemcpy(e->d_start, st32.data(), st32.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemset(e->d_stress, 0, 9 * real_size(e) * (size_t)n));
+    CU(cudaMemset(e->d_status, 0, sizeof(unsigned)));
+    int rc = empty_topology(e);
+    if (rc) return rc;
+    e->uploaded = true;
+    e->stepped = false;
+    e->obs_valid = false;
+    return DPD_OK;
+}
+
+int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_head_id, const int64_t* bond_tail_id,
+                               const double* k2, const double* l0, int64_t na, const int64_t* first_bond,
+                               const int64_t* second_bond, const double* k3, const double* phi0)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads before the topology");
+    if (nb < 0 || na < 0 || (nb && (!bond_head_id || !bond_tail_id || !k2 || !l0)) ||
+        (na && (!first_bond || !second_bond || !k3 || !phi0)))
+        return fail(e, DPD_E_ARG, "bad topology arrays");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    const int64_t n = e->n;
+    // bead id -> upload index
+    std::vector<int> hpid(n);
+    CU(cudaMemcpy(hpid.data(), e->d_pid_of, n * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> dense;
+    bool identity = true;
+    for (int64_t b = 0; b < n && identity; ++b) identity = (hpid[b] == b + 1);
+    auto index_of = [&](int64_t idv) -> int {
+        if (identity) return (idv >= 1 && idv <= n) ? (int)(idv - 1) : -1;
+        for (int64_t b = 0; b < n; ++b)
+            if (hpid[b] == idv) return (int)b;
+        return -1;
+    };
+    std::vector<int> bh(nb), bt(nb);
+    for (int64_t i = 0; i < nb; ++i) {
+        bh[i] = index_of(bond_head_id[i]);
+        bt[i] = index_of(bond_tail_id[i]);
+        if (bh[i] < 0 || bt[i] < 0) return fail(e, DPD_E_ARG, "bond refers to an unknown bead id");
+        if (bh[i] == bt[i]) return fail(e, DPD_E_ARG, "bond joins a bead to itself");
+    }
+    std::vector<int> a4[4];
+    for (auto& v : a4) v.resize(na);
+    std::vector<double> acos0(na), asin0(na);
+    for (int64_t i = 0; i < na; ++i) {
+        if (first_bond[i] < 0 || first_bond[i] >= nb || second_bond[i] < 0 || second_bond[i] >= nb)
+            return fail(e, DPD_E_ARG, "bond pair refers to an unknown bond");
+        a4[0][i] = bh[first_bond[i]];
+        a4[1][i] = bt[first_bond[i]];
+        a4[2][i] = bh[second_bond[i]];
+        a4[3][i] = bt[second_bond[i]];
+        // CBondPair ctor caches cos/sin of phi0; the phi0 > 0 branch of
+        // BondPair.cpp:178-188 is selected by sin0 != 0
+        acos0[i] = phi0[i] > 0.0 ? std::cos(phi0[i]) : 1.0;
+        asin0[i] = phi0[i] > 0.0 ? std::sin(phi0[i]) : 0.0;
+    }
+    // per-bead term lists (CSR by upload index); terms in bond order then pair order
+    std::vector<int> cnt(n + 1, 0);
+    for (int64_t i = 0; i < nb; ++i) { cnt[bh[i] + 1]++; cnt[bt[i] + 1]++; }
+    for (int64_t i = 0; i < na; ++i) { cnt[a4[1][i] + 1]++; cnt[a4[0][i] + 1]++; cnt[a4[2][i] + 1]++; }
+    for (int64_t b = 0; b < n; ++b) cnt[b + 1] += cnt[b];
+    std::vector<int> fillp(cnt.begin(), cnt.end() - 1), terms(cnt[n]);
+    if (nb * 2 + na * 3 > ((int64_t)1 << 28)) return fail(e, DPD_E_ARG, "topology too large");
+    for (int64_t i = 0; i < nb; ++i) {
+        terms[fillp[bh[i]]++] = (int)(i * 8 + kBondHead);
+        terms[fillp[bt[i]]++] = (int)(i * 8 + kBondTail);
+    }
+    for (int64_t i = 0; i < na; ++i) {
+        terms[fillp[a4[1][i]]++] = (int)(i * 8 + kAngle0);   // first bond's tail: force [0]
+        terms[fillp[a4[0][i]]++] = (int)(i * 8 + kAngle1);   // middle bead:       force [1]
+        terms[fillp[a4[2][i]]++] = (int)(i * 8 + kAngle2);   // second bond's head: force [2]
+    }
+    release_topology(e);
+    int rc;
+    if ((rc = dalloc(e, &e->d_csr_ptr, (size_t)n + 1))) return rc;
+    if ((rc = dalloc(e, &e->d_csr_term, terms.size()))) return rc;
+    CU(cudaMemcpy(e->d_csr_ptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!terms.empty()) CU(cudaMemcpy(e->d_csr_term, terms.data(), terms.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (nb) {
+        if ((rc = dalloc(e, &e->d_bond_h, nb)) || (rc = dalloc(e, &e->d_bond_t, nb)) ||
+            (rc = dalloc(e, &e->d_bond_k2, nb)) || (rc = dalloc(e, &e->d_bond_l0, nb)))
+            return rc;
+        CU(cudaMemcpy(e->d_bond_h, bh.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_bond_t, bt.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_bond_k2, k2, nb * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_bond_l0, l0, nb * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (na) {
+        for (int k = 0; k < 4; ++k) {
+            if ((rc = dalloc(e, &e->d_ang[k], na))) return rc;
+            CU(cudaMemcpy(e->d_ang[k], a4[k].data(), na * sizeof(int), cudaMemcpyHostToDevice));
+        }
+        if ((rc = dalloc(e, &e->d_ang_k3, na)) || (rc = dalloc(e, &e->d_ang_cos0, na)) ||
+            (rc = dalloc(e, &e->d_ang_sin0, na)))
+            return rc;
+        CU(cudaMemcpy(e->d_ang_k3, k3, na * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_ang_cos0, acos0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_ang_sin0, asin0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return DPD_OK;
+}
+
+int dpd_engine_set_pair_params(dpd_engine* e, int32_t ntypes, const double* a, const double* gamma)
+{
+    if (!e) return DPD_E_ARG;
+    if (ntypes < 1 || ntypes > kMaxTypes || !a || !gamma) return fail(e, DPD_E_ARG, "bad pair tables");
+    if (ntypes < e->ntypes) return fail(e, DPD_E_ARG, "bead types cannot be removed");
+    const int m = ntypes * ntypes;
+    for (int i = 0; i < ntypes; ++i)
+        for (int j = 0; j < ntypes; ++j)
+            if (a[i * ntypes + j] != a[j * ntypes + i] || gamma[i * ntypes + j] != gamma[j * ntypes + i])
+                return fail(e, DPD_E_ARG, "pair tables must be symmetric");
+    e->ntypes = ntypes;
+    e->a.assign(a, a + m);
+    e->gamma.assign(gamma, gamma + m);
+    CU(cudaSetDevice(e->device));
+    return push_constants(e);
+}
+
+int dpd_engine_set_dt(dpd_engine* e, double dt)
+{
+    if (!e) return DPD_E_ARG;
+    if (!(dt > 0.0)) return DPD_OK;   // ChangeTimeStepConstants ignores dt <= 0 (CNTCell.cpp:359)
+    e->params.dt = dt;
+    CU(cudaSetDevice(e->device));
+    return push_constants(e);
+}
+
+int dpd_engine_set_thermostat(dpd_engine* e, int32_t on)
+{
+    if (!e) return DPD_E_ARG;
+    e->thermostat_on = on != 0;
+    CU(cudaSetDevice(e->device));
+    return push_constants(e);
+}
+
+int dpd_engine_set_conservative(dpd_engine* e, int32_t on)
+{
+    if (!e) return DPD_E_ARG;
+    e->conservative_on = on != 0;
+    CU(cudaSetDevice(e->device));
+    return push_constants(e);
+}
+
+int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    if (nsteps < 0) return fail(e, DPD_E_ARG, "negative step count");
+    if (nsteps == 0) return DPD_OK;
+    CU(cudaSetDevice(e->device));
+    // the step counter keys the pair noise; it is advanced on the device
+    // by the last kernel of every step
+    CU(cudaStreamSynchronize(e->s()));
+    *e->h_step = first_step;
+    CU(cudaMemcpyAsync(e->d_step, e->h_step, sizeof(int64_t), cudaMemcpyHostToDevice, e->s()));
+    for (int32_t k = 0; k < nsteps; ++k) {
+        const bool sample = (k == nsteps - 1);
+        const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, sample)
+                                                             : queue_step<float>(e, sample);
+        if (rc) return rc;
+    }
+    e->stepped = true;
+    e->obs_valid = false;
+    e->obs_has_virial = true;
+    e->last_step = first_step + nsteps - 1;
+    return DPD_OK;
+}
+
+int dpd_engine_status(dpd_engine* e, uint32_t* bits)
+{
+    if (!e) return DPD_E_ARG;
+    CU(cudaSetDevice(e->device));
+    CU(cudaMemcpyAsync(e->h_status, e->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    if (bits) *bits = *e->h_status;
+    return DPD_OK;
+}
+
+static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, double* f3, double* st9, int32_t* cell)
+{
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    CU(cudaSetDevice(e->device));
+    const int n = (int)e->n;
+    double* o = e->d_out;
+    double *ox = x3 ? o : nullptr, *ou = u3 ? o + 3 * (size_t)n : nullptr, *ov = v3 ? o + 6 * (size_t)n : nullptr,
+           *of = f3 ? o + 9 * (size_t)n : nullptr, *ost = st9 ? o + 12 * (size_t)n : nullptr;
+    const int c = e->cur;
+    if (e->precision == DPD_PRECISION_FP64)
+        k_download<double><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
+            n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->d_off,
+            e->stepped ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
+            cell ? e->d_out_cell : nullptr);
+    else
+        k_download<float><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
+            n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->d_off,
+            e->stepped ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
+            cell ? e->d_out_cell : nullptr);
+    int rc = check_launch(e, "k_download");
+    if (rc) return rc;
+    if (x3) CU(cudaMemcpyAsync(x3, ox, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, e->s()));
+    if (u3) CU(cudaMemcpyAsync(u3, ou, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, e->s()));
+    if (v3) CU(cudaMemcpyAsync(v3, ov, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, e->s()));
+    if (f3) CU(cudaMemcpyAsync(f3, of, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, e->s()));
+    if (st9) CU(cudaMemcpyAsync(st9, ost, 9 * sizeof(double) * n, cudaMemcpyDeviceToHost, e->s()));
+    if (cell) CU(cudaMemcpyAsync(cell, e->d_out_cell, sizeof(int) * n, cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    return DPD_OK;
+}
+
+int dpd_engine_download(dpd_engine* e, double* x3, double* unpbc3, double* v3, double* f3, double* stress9)
+{
+    if (!e) return DPD_E_ARG;
+    return run_download(e, x3, unpbc3, v3, f3, stress9, nullptr);
+}
+
+int dpd_engine_cells(dpd_engine* e, int32_t* cell)
+{
+    if (!e) return DPD_E_ARG;
+    if (!cell) return fail(e, DPD_E_ARG, "null cell array");
+    return run_download(e, nullptr, nullptr, nullptr, nullptr, nullptr, cell);
+}
+
+int dpd_engine_observables(dpd_engine* e, dpd_obs* out)
+{
+    if (!e) return DPD_E_ARG;
+    if (!out) return fail(e, DPD_E_ARG, "null output");
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    CU(cudaSetDevice(e->device));
+    const int n = (int)e->n;
+    if (!e->stepped) {
+        const int nb = blocks_for(n, kThreads);
+        k_kinetic_partials<<<nb, kThreads, 0, e->s()>>>(n, e->d_x[e->cur], e->d_v[e->cur], e->d_partials);
+        int rc = check_launch(e, "k_kinetic_partials");
+        if (rc) return rc;
+        k_reduce_obs<<<1, 256, 0, e->s()>>>(nb, e->d_partials, e->d_obs);
+        if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
+    }
+    CU(cudaMemcpyAsync(e->h_obs, e->d_obs, kObsTerms * sizeof(double), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    const double* h = e->h_obs;
+    memset(out, 0, sizeof *out);
+    out->step = e->stepped ? e->last_step : 0;
+    out->n = e->n;
+    for (int d = 0; d < 3; ++d) {
+        out->sum_v[d] = h[d];
+        out->sum_v2[d] = h[3 + d];
+        out->sum_x[d] = h[15 + d];
+        out->ang_mom[d] = h[18 + d];
+    }
+    out->has_virial = e->stepped ? 1 : 0;
+    for (int q = 0; q < 9; ++q) out->virial[q] = e->stepped ? h[6 + q] : 0.0;
+    const dpd_params& p = e->params;
+    const double V = (p.nx * p.wx) * (p.ny * p.wy) * (p.nz * p.wz);
+    const double v2 = out->sum_v2[0] + out->sum_v2[1] + out->sum_v2[2];
+    out->kT = v2 / (3.0 * (double)e->n);
+    out->pressure = 0.3333333333 * (1.0 / V) * (v2 + out->virial[0] + out->virial[4] + out->virial[8]);
+    return DPD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,652 @@
+// dpd_kernels.cuh -- sm_100a kernels of one DPD timestep.
+//
+// Device layout ("slot order"): beads sorted by CNT cell, cells in the
+// reference's index order nx*(ny*iz+iy)+ix (SimBox.cpp:888-920), and inside a
+// cell by their slot in the previous step (a stable counting sort), so the
+// order -- and every floating-point sum -- is deterministic.  Per-bead arrays
+// are structure-of-arrays; 3-vectors are three planes of n values.
+//
+// One step, in the reference's order (CSimBox::Evolve, SimBox.cpp:977-1120):
+//   k_update_pos   UpdatePos: drift, incremental cell move + PBC wrap,
+//                  per-cell counts                 (CNTCell.cpp:1634-2262)
+//   k_scan_cells   cell start offsets (exclusive prefix sum of the counts)
+//   k_permute      arrival slot -> new slot map
+//   k_gather       stable per-cell order, permutes the state, writes the
+//                  cell-relative FP32/FP64 shadows the force kernel reads
+//   k_pair_forces  conservative + dissipative + random pair forces over the
+//                  27 neighbour cells                (CNTCell.cpp:1103-1572)
+//   k_update_mom   bond and bond-pair forces, UpdateMom, FP64 sums on
+//                  sample steps                      (Bond.cpp:111-162,
+//                  BondPair.cpp:138-286, CNTCell.cpp:2280-2310,
+//                  Monitor.cpp:790-1040)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "philox.cuh"
+
+namespace dpd {
+
+constexpr int kMaxTypes = 32;
+constexpr int kScanThreads = 256;
+constexpr int kScanPerThread = 8;
+constexpr int kScanChunk = kScanThreads * kScanPerThread;   // cells per scan block
+constexpr int kObsTerms = 21;   // sum_v[3] sum_v2[3] virial[9] sum_x[3] angmom[3]
+
+// Image counters: three signed 10-bit fields (bias 512) in one word.
+__host__ __device__ __forceinline__ uint32_t img_pack(int ix, int iy, int iz)
+{
+    return (uint32_t)(ix + 512) | ((uint32_t)(iy + 512) << 10) | ((uint32_t)(iz + 512) << 20);
+}
+__host__ __device__ __forceinline__ int img_get(uint32_t w, int d)
+{
+    return (int)((w >> (10 * d)) & 1023u) - 512;
+}
+
+// Time-step and box constants; lives in device memory so that a parameter
+// change needs no relaunch configuration (CCNTCell statics, CNTCell.cpp:42-75).
+struct StepConst {
+    double dt, halfdt, halfdt2, lamdt, invrootdt;
+    double L[3], w[3];
+    int nc[3];
+    int ntypes;
+    uint64_t seed;
+};
+
+// Bead flags word: type in bits 0..15, frozen (never moves) in bit 16.
+__device__ __forceinline__ int flag_type(int tf) { return tf & 0xFFFF; }
+__device__ __forceinline__ bool flag_frozen(int tf) { return (tf >> 16) & 1; }
+
+template <typename real> struct Vec4;
+template <> struct Vec4<float> { typedef float4 type; };
+template <> struct Vec4<double> { typedef double4 type; };
+
+__device__ __forceinline__ float as_real_bits(int v, float) { return __int_as_float(v); }
+__device__ __forceinline__ double as_real_bits(int v, double) { return __longlong_as_double((long long)v); }
+__device__ __forceinline__ int real_bits(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int real_bits(double v) { return (int)__double_as_longlong(v); }
+
+// ------------------------------------------------------------- UpdatePos
+
+// Drift and cell migration of every bead (CCNTCell::UpdatePos).  The
+// reference's 27-way decision tree moves a bead by one cell along each axis
+// where x > TR (+1) or x < BL (-1), TR = BL + w with BL = ix*w
+// (CNTCell.cpp:598-604, 1768-2254), wrapping the moved coordinates only when
+// both cells lie on the box boundary.  Frozen beads keep their cell.
+template <typename real>
+__global__ void __launch_bounds__(256) k_update_pos(
+    int n, const StepConst* __restrict__ K, double* __restrict__ x, const double* __restrict__ v,
+    const real* __restrict__ F, const int* __restrict__ tf, uint32_t* __restrict__ img,
+    int* __restrict__ cell, int* __restrict__ rank, int* __restrict__ count,
+    int* __restrict__ block_count, unsigned* __restrict__ status)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = s < n;
+    int cnew = 0;
+    unsigned bad = 0;
+    if (live) {
+        const int c = cell[s];
+        cnew = c;
+        if (!flag_frozen(tf[s])) {
+            const double dt = K->dt, h2 = K->halfdt2;
+            const int nx = K->nc[0], ny = K->nc[1], nz = K->nc[2];
+            int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
+            const bool ext = ci[0] == 0 || ci[0] == nx - 1 || ci[1] == 0 || ci[1] == ny - 1 ||
+                             ci[2] == 0 || ci[2] == nz - 1;
+            double xn[3];
+            int mv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                // x += dt*v + dt^2/2*F with the reference's rounding (no fused multiply-add)
+                const double dx = __dadd_rn(__dmul_rn(dt, v[d * n + s]), __dmul_rn(h2, (double)F[d * n + s]));
+                xn[d] = __dadd_rn(x[d * n + s], dx);
+                const double BL = __dmul_rn((double)ci[d], K->w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
+                const double TR = __dadd_rn(BL, K->w[d]);
+                mv[d] = (xn[d] > TR) ? 1 : ((xn[d] < BL) ? -1 : 0);
+            }
+            uint32_t im = img[s];
+            if (mv[0] | mv[1] | mv[2]) {
+                int nci[3];
+                for (int d = 0; d < 3; ++d) {
+                    nci[d] = ci[d] + mv[d];
+                    if (nci[d] < 0) nci[d] += K->nc[d];
+                    else if (nci[d] >= K->nc[d]) nci[d] -= K->nc[d];
+                }
+                const bool next = nci[0] == 0 || nci[0] == nx - 1 || nci[1] == 0 || nci[1] == ny - 1 ||
+                                  nci[2] == 0 || nci[2] == nz - 1;
+                if (ext && next) {
+                    int ii[3] = {img_get(im, 0), img_get(im, 1), img_get(im, 2)};
+                    for (int d = 0; d < 3; ++d) {
+                        if (mv[d] > 0 && xn[d] > K->L[d]) { xn[d] -= K->L[d]; ++ii[d]; }
+                        else if (mv[d] < 0 && xn[d] < 0.0) { xn[d] += K->L[d]; --ii[d]; }
+                        if (ii[d] < -511 || ii[d] > 511) bad |= 0x4u;
+                    }
+                    im = img_pack(ii[0], ii[1], ii[2]);
+                }
+                cnew = nci[0] + nx * (nci[1] + ny * nci[2]);
+            }
+            // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650)
+            const long long ax = (long long)(xn[0] / K->w[0]);
+            const long long ay = (long long)(xn[1] / K->w[1]);
+            const long long az = (long long)(xn[2] / K->w[2]);
+            if ((long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (!isfinite(xn[d])) bad |= 0x2u;
+                x[d * n + s] = xn[d];
+            }
+            img[s] = im;
+            cell[s] = cnew;
+        }
+        rank[s] = atomicAdd(&count[cnew], 1);
+    }
+    // one atomic per scan chunk per warp
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (live) {
+        const int chunk = cnew / kScanChunk;
+        const unsigned peers = __match_any_sync(act, chunk);
+        const int leader = __ffs(peers) - 1;
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&block_count[chunk], __popc(peers));
+    }
+    if (bad) atomicOr(status, bad);
+}
+
+// ------------------------------------------------------------------ scan
+
+// start[c] = sum of count[0..c); one block per chunk of kScanChunk cells.  The
+// chunk's base is the sum of the per-chunk totals counted by k_update_pos.
+// Counts are cleared for the next step.
+__global__ void __launch_bounds__(kScanThreads) k_scan_cells(
+    int ncell, int n, int* __restrict__ count, const int* __restrict__ block_count,
+    int* __restrict__ start)
+{
+    __shared__ int warp_sum[kScanThreads / 32];
+    __shared__ int base_s;
+    const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    int acc = 0;
+    for (int k = t; k < b; k += kScanThreads) acc += block_count[k];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) warp_sum[wid] = acc;
+    __syncthreads();
+    if (t == 0) {
+        int s = 0;
+        for (int w = 0; w < kScanThreads / 32; ++w) s += warp_sum[w];
+        base_s = s;
+    }
+    __syncthreads();
+    const int base = base_s;
+    const int c0 = b * kScanChunk + t * kScanPerThread;
+    int vals[kScanPerThread];
+    int tot = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPerThread; ++k) {
+        const int c = c0 + k;
+        vals[k] = (c < ncell) ? count[c] : 0;
+        tot += vals[k];
+    }
+    // exclusive scan of per-thread totals across the block
+    int inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    __syncthreads();
+    if (lane == 31) warp_sum[wid] = inc;
+    __syncthreads();
+    int wbase = 0;
+    for (int w = 0; w < wid; ++w) wbase += warp_sum[w];
+    int run = base + wbase + inc - tot;
+#pragma unroll
+    for (int k = 0; k < kScanPerThread; ++k) {
+        const int c = c0 + k;
+        if (c < ncell) {
+            start[c] = run;
+            count[c] = 0;
+        }
+        run += vals[k];
+    }
+    if (b == gridDim.x - 1 && t == 0) start[ncell] = n;
+}
+
+// new arrival slot -> old slot; also clears the per-chunk totals.
+__global__ void __launch_bounds__(256) k_permute(
+    int n, int nchunk, const int* __restrict__ cell, const int* __restrict__ rank,
+    const int* __restrict__ start, int* __restrict__ perm, int* __restrict__ block_count)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nchunk) block_count[s] = 0;
+    if (s < n) perm[start[cell[s]] + rank[s]] = s;
+}
+
+// Stable order inside each cell (by previous slot), state permutation, and
+// the force kernel's shadows: position relative to the bead's own cell origin
+// and intermediate velocity v~ = v + lambda*dt*F_old (CNTCell.cpp:1743-1747),
+// with the bead type and the noise id in the fourth component.
+template <typename real>
+__global__ void __launch_bounds__(256) k_gather(
+    int n, const StepConst* __restrict__ K, const int* __restrict__ perm, const int* __restrict__ start,
+    const double* __restrict__ x_in, const double* __restrict__ v_in, const real* __restrict__ F_in,
+    const int* __restrict__ bid_in, const int* __restrict__ tf_in, const uint32_t* __restrict__ img_in,
+    const int* __restrict__ cell_in, double* __restrict__ x_out, double* __restrict__ v_out,
+    real* __restrict__ Fold_out, int* __restrict__ bid_out, int* __restrict__ tf_out,
+    uint32_t* __restrict__ img_out, int* __restrict__ cell_out, int* __restrict__ slot_of,
+    const int* __restrict__ pid_of, typename Vec4<real>::type* __restrict__ pos4,
+    typename Vec4<real>::type* __restrict__ vel4)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int s = perm[d];
+    const int c = cell_in[s];
+    const int beg = start[c], end = start[c + 1];
+    int k = 0;
+    for (int e = beg; e < end; ++e) k += (perm[e] < s);
+    const int o = beg + k;
+    const int b = bid_in[s];
+    const int tfl = tf_in[s];
+    const int nx = K->nc[0], ny = K->nc[1];
+    const int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
+    const bool frozen = flag_frozen(tfl);
+    real rel[3], vt[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double xv = x_in[q * n + s];
+        const double vv = v_in[q * n + s];
+        const real fv = F_in[q * n + s];
+        x_out[q * n + o] = xv;
+        v_out[q * n + o] = vv;
+        Fold_out[q * n + o] = fv;
+        rel[q] = (real)__dadd_rn(xv, -__dmul_rn((double)ci[q], K->w[q]));
+        vt[q] = frozen ? (real)vv : (real)__dadd_rn(vv, __dmul_rn(K->lamdt, (double)fv));
+    }
+    bid_out[o] = b;
+    tf_out[o] = tfl;
+    img_out[o] = img_in[s];
+    cell_out[o] = c;
+    slot_of[b] = o;
+    typedef typename Vec4<real>::type V4;
+    V4 p, w;
+    p.x = rel[0]; p.y = rel[1]; p.z = rel[2]; p.w = as_real_bits(flag_type(tfl), real(0));
+    w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid_of[b], real(0));
+    pos4[o] = p;
+    vel4[o] = w;
+}
+
+// ------------------------------------------------------------ pair forces
+
+// Pair-parameter tables staged per block: a_ij, gamma_ij and
+// sigma_ij = sqrt(gamma_ij) * sqrt(24 kT / dt).
+template <typename real>
+struct PairTables {
+    real a[kMaxTypes * kMaxTypes];
+    real g[kMaxTypes * kMaxTypes];
+    real sig[kMaxTypes * kMaxTypes];
+};
+
+template <typename real>
+__device__ __forceinline__ void load_tables(PairTables<real>& T, const real* __restrict__ tab, int nt)
+{
+    const int m = nt * nt;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        T.a[k] = tab[k];
+        T.g[k] = tab[m + k];
+        T.sig[k] = tab[2 * m + k];
+    }
+}
+
+__device__ __forceinline__ float noise_centered(uint32_t r, float)
+{
+    // 0.5 - r * 2^-32, formed exactly in integers before the conversion
+    return (float)(int)(0x80000000u - r) * 2.3283064365386963e-10f;
+}
+__device__ __forceinline__ double noise_centered(uint32_t r, double)
+{
+    return 0.5 - (double)r * 2.3283064365386963e-10;
+}
+
+// Reference force kernel: one thread per bead, full 27-cell shell, every
+// pair evaluated from both sides (no atomics, deterministic).  The DPD force
+// of CNTCell.cpp:1192-1220 with rc = 1:
+//   w = 1 - r; F = (a_ij w - gamma_ij w^2 (r.v)/r + sigma_ij w (0.5 - U)) r_vec / r
+template <typename real, bool VIRIAL>
+__global__ void __launch_bounds__(128) k_pair_forces_ref(
+    int n, const StepConst* __restrict__ K, const int64_t* __restrict__ step_ptr,
+    const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
+    const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
+    real* __restrict__ F, real* __restrict__ stress)
+{
+    __shared__ PairTables<real> T;
+    const int nt = K->ntypes;
+    load_tables(T, tab, nt);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t key = philox_step_key(K->seed, *step_ptr);
+    const int nx = K->nc[0], ny = K->nc[1], nz = K->nc[2];
+    const int c = cell[i];
+    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    const typename Vec4<real>::type pi = pos4[i], vi = vel4[i];
+    const int ti = real_bits(pi.w) & 0xFFFF;
+    const uint32_t idi = (uint32_t)real_bits(vi.w);
+    real fx = 0, fy = 0, fz = 0;
+    real s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int oz = -1; oz <= 1; ++oz) {
+        int z2 = cz + oz;
+        z2 += (z2 < 0) ? nz : ((z2 >= nz) ? -nz : 0);
+        for (int oy = -1; oy <= 1; ++oy) {
+            int y2 = cy + oy;
+            y2 += (y2 < 0) ? ny : ((y2 >= ny) ? -ny : 0);
+            for (int ox = -1; ox <= 1; ++ox) {
+                int x2 = cx + ox;
+                x2 += (x2 < 0) ? nx : ((x2 >= nx) ? -nx : 0);
+                const int c2 = x2 + nx * (y2 + ny * z2);
+                const real sx = (real)(ox * K->w[0]), sy = (real)(oy * K->w[1]), sz = (real)(oz * K->w[2]);
+                const int jb = start[c2], je = start[c2 + 1];
+                for (int j = jb; j < je; ++j) {
+                    if (j == i) continue;
+                    const typename Vec4<real>::type pj = pos4[j];
+                    const real dx = (pi.x - pj.x) - sx;
+                    const real dy = (pi.y - pj.y) - sy;
+                    const real dz = (pi.z - pj.z) - sz;
+                    const real r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 < real(1) && r2 > real(1e-18)) {
+                        const typename Vec4<real>::type vj = vel4[j];
+                        const real r = sqrt(r2);
+                        const real inv = real(1) / r;
+                        const real wr = real(1) - r;
+                        const int tj = real_bits(pj.w) & 0xFFFF;
+                        const int tt = ti * nt + tj;
+                        const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
+                        const uint32_t idj = (uint32_t)real_bits(vj.w);
+                        const uint32_t u = philox2x32_10(min(idi, idj), max(idi, idj), key);
+                        const real mag = T.a[tt] * wr - T.g[tt] * wr * wr * rdotv +
+                                         T.sig[tt] * wr * noise_centered(u, real(0));
+                        const real m = mag * inv;
+                        const real gx = m * dx, gy = m * dy, gz = m * dz;
+                        fx += gx; fy += gy; fz += gz;
+                        if (VIRIAL) {
+                            s[0] += dx * gx; s[1] += dy * gx; s[2] += dz * gx;
+                            s[3] += dx * gy; s[4] += dy * gy; s[5] += dz * gy;
+                            s[6] += dx * gz; s[7] += dy * gz; s[8] += dz * gz;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    F[i] = fx;
+    F[n + i] = fy;
+    F[2 * n + i] = fz;
+    if (VIRIAL) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) stress[q * n + i] = real(0.5) * s[q];
+    }
+}
+
+// -------------------------------------------------------------- UpdateMom
+
+struct Topology {
+    const int* csr_ptr;     // per bead (upload index): first term
+    const int* csr_term;    // term = index * 8 + code
+    const int* bond_h;      // bond head / tail bead (upload index)
+    const int* bond_t;
+    const double* bond_k2;
+    const double* bond_l0;
+    const int* ang_b1h;     // first bond head (middle bead), first bond tail,
+    const int* ang_b1t;     // second bond head, second bond tail
+    const int* ang_b2h;
+    const int* ang_b2t;
+    const double* ang_k3;
+    const double* ang_cos0; // cos(phi0); 1 when phi0 <= 0
+    const double* ang_sin0; // sin(phi0); exactly 0 when phi0 <= 0 (the k3/|b1||b2| branch)
+    const double* off;      // unPBC - (x + img*L) at upload, 3 planes by upload index, or null
+};
+
+enum TermCode { kBondHead = 0, kBondTail = 1, kAngle0 = 2, kAngle1 = 3, kAngle2 = 4 };
+
+__device__ __forceinline__ void unwrapped(const StepConst* __restrict__ K, const double* __restrict__ x,
+                                          const uint32_t* __restrict__ img, const double* __restrict__ off,
+                                          int n, int nb_total, int slot, int b, double u[3])
+{
+    const uint32_t im = img[slot];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        u[d] = x[d * n + slot] + (double)img_get(im, d) * K->L[d];
+        if (off) u[d] += off[d * nb_total + b];
+    }
+}
+
+// Bond and bond-pair forces gathered per bead (each bond is evaluated by both
+// of its beads and each bond pair by its three beads, so no atomics), then the
+// velocity update of CCNTCell::UpdateMom: v = v_old + dt/2 (F + F_old) for
+// movable beads.  Non-movable beads keep v and, as in the reference (whose
+// UpdatePos skips them), keep accumulating force.  On sample steps the FP64
+// single-bead sums are reduced per block.
+template <typename real, bool SAMPLE>
+__global__ void __launch_bounds__(256) k_update_mom(
+    int n, const StepConst* __restrict__ K, int64_t* __restrict__ step_ptr,
+    const double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
+    const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
+    const uint32_t* __restrict__ img, const int* __restrict__ slot_of, Topology topo,
+    real* __restrict__ stress, double* __restrict__ partials, unsigned* __restrict__ status)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[kObsTerms];
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
+    if (s < n) {
+        const int b = bid[s];
+        const int tfl = tf[s];
+        const bool frozen = flag_frozen(tfl);
+        real f[3] = {F[s], F[n + s], F[2 * n + s]};
+        real fo[3] = {Fold[s], Fold[n + s], Fold[2 * n + s]};
+        if (frozen) { f[0] += fo[0]; f[1] += fo[1]; f[2] += fo[2]; }
+        real bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int t0 = topo.csr_ptr[b], t1 = topo.csr_ptr[b + 1];
+        for (int t = t0; t < t1; ++t) {
+            const int term = topo.csr_term[t];
+            const int code = term & 7, idx = term >> 3;
+            if (code <= kBondTail) {
+                // CBond::AddForce, Bond.cpp:123-160 (serial build: unPBC coordinates)
+                const int h = topo.bond_h[idx], tl = topo.bond_t[idx];
+                double uh[3], ut[3];
+                unwrapped(K, x, img, topo.off, n, n, slot_of[h], h, uh);
+                unwrapped(K, x, img, topo.off, n, n, slot_of[tl], tl, ut);
+                const real bx = (real)(uh[0] - ut[0]), by = (real)(uh[1] - ut[1]), bz = (real)(uh[2] - ut[2]);
+                const real len = sqrt(bx * bx + by * by + bz * bz);
+                const real m = (real)topo.bond_k2[idx] * ((real)topo.bond_l0[idx] - len) / len;
+                const real gx = m * bx, gy = m * by, gz = m * bz;
+                if (code == kBondHead) {
+                    f[0] += gx; f[1] += gy; f[2] += gz;
+                    if (SAMPLE) {
+                        bs[0] += bx * gx; bs[1] += by * gx; bs[2] += bz * gx;
+                        bs[3] += bx * gy; bs[4] += by * gy; bs[5] += bz * gy;
+                        bs[6] += bx * gz; bs[7] += by * gz; bs[8] += bz * gz;
+                    }
+                } else {
+                    f[0] -= gx; f[1] -= gy; f[2] -= gz;
+                }
+            } else {
+                // CBondPair::AddForce, BondPair.cpp:140-285
+                double u1h[3], u1t[3], u2h[3], u2t[3];
+                const int a1h = topo.ang_b1h[idx], a1t = topo.ang_b1t[idx];
+                const int a2h = topo.ang_b2h[idx], a2t = topo.ang_b2t[idx];
+                unwrapped(K, x, img, topo.off, n, n, slot_of[a1h], a1h, u1h);
+                unwrapped(K, x, img, topo.off, n, n, slot_of[a1t], a1t, u1t);
+                unwrapped(K, x, img, topo.off, n, n, slot_of[a2h], a2h, u2h);
+                unwrapped(K, x, img, topo.off, n, n, slot_of[a2t], a2t, u2t);
+                real b1[3], b2[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    b1[d] = (real)(u1h[d] - u1t[d]);
+                    b2[d] = (real)(u2h[d] - u2t[d]);
+                }
+                const real l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
+                const real l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
+                const real mag = l1 * l2;
+                if (mag > real(0.0001)) {
+                    const real dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
+                    const real o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
+                    real fm = (real)topo.ang_k3[idx] / mag;
+                    const double s0 = topo.ang_sin0[idx];
+                    if (s0 != 0.0 && fabs((double)dot) > 0.000001) {
+                        const real pre = sqrt(real(1) / (o1 * o2) - real(1));
+                        fm = (real)topo.ang_k3[idx] * ((real)topo.ang_cos0[idx] - (real)s0 / pre) / mag;
+                    }
+                    real g0[3], g2[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        g0[d] = fm * (o1 * b1[d] - b2[d]);
+                        g2[d] = fm * (b1[d] - o2 * b2[d]);
+                    }
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (code == kAngle0) f[d] += g0[d];
+                        else if (code == kAngle2) f[d] += g2[d];
+                        else f[d] += -g0[d] - g2[d];
+                    }
+                }
+            }
+        }
+        F[s] = f[0];
+        F[n + s] = f[1];
+        F[2 * n + s] = f[2];
+        if (!isfinite((double)f[0]) || !isfinite((double)f[1]) || !isfinite((double)f[2]))
+            atomicOr(status, 0x2u);
+        double vn[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            vn[d] = v[d * n + s];
+            if (!frozen) {
+                vn[d] = __dadd_rn(vn[d], __dmul_rn(K->halfdt, __dadd_rn((double)f[d], (double)fo[d])));
+                v[d * n + s] = vn[d];
+            }
+        }
+        if (SAMPLE) {
+            const double xs[3] = {x[s], x[n + s], x[2 * n + s]};
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const real st = stress[q * n + s] + bs[q];
+                stress[q * n + s] = st;
+                acc[6 + q] = (double)st;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                acc[d] = vn[d];
+                acc[3 + d] = vn[d] * vn[d];
+                acc[15 + d] = xs[d];
+            }
+            acc[18] = xs[1] * vn[2] - xs[2] * vn[1];
+            acc[19] = -xs[0] * vn[2] + xs[2] * vn[0];
+            acc[20] = xs[0] * vn[1] - xs[1] * vn[0];
+        }
+    }
+    if (SAMPLE) {
+        __shared__ double red[256 / 32][kObsTerms];
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+        for (int q = 0; q < kObsTerms; ++q) {
+            double a = acc[q];
+#pragma unroll
+            for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == 0) red[wid][q] = a;
+        }
+        __syncthreads();
+        if (threadIdx.x < kObsTerms) {
+            double a = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w][threadIdx.x];
+            partials[blockIdx.x * kObsTerms + threadIdx.x] = a;
+        }
+    }
+    if (s == 0) *step_ptr += 1;
+}
+
+// Fixed-order sum of the per-block partials (deterministic).
+__global__ void __launch_bounds__(256) k_reduce_obs(int nblocks, const double* __restrict__ partials,
+                                                     double* __restrict__ out)
+{
+    __shared__ double red[256 / 32];
+    for (int q = 0; q < kObsTerms; ++q) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) a += partials[b * kObsTerms + q];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            out[q] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Kinetic sums without a force evaluation (state just uploaded).
+__global__ void __launch_bounds__(256) k_kinetic_partials(int n, const double* __restrict__ x,
+                                                           const double* __restrict__ v,
+                                                           double* __restrict__ partials)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[kObsTerms];
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
+    if (s < n) {
+        const double xs[3] = {x[s], x[n + s], x[2 * n + s]};
+        const double vs[3] = {v[s], v[n + s], v[2 * n + s]};
+        for (int d = 0; d < 3; ++d) {
+            acc[d] = vs[d];
+            acc[3 + d] = vs[d] * vs[d];
+            acc[15 + d] = xs[d];
+        }
+        acc[18] = xs[1] * vs[2] - xs[2] * vs[1];
+        acc[19] = -xs[0] * vs[2] + xs[2] * vs[0];
+        acc[20] = xs[0] * vs[1] - xs[1] * vs[0];
+    }
+    __shared__ double red[256 / 32][kObsTerms];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int q = 0; q < kObsTerms; ++q) {
+        double a = acc[q];
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) red[wid][q] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsTerms) {
+        double a = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w][threadIdx.x];
+        partials[blockIdx.x * kObsTerms + threadIdx.x] = a;
+    }
+}
+
+// ---------------------------------------------------------------- download
+
+// Slot order -> upload order, FP64, xyz interleaved; unPBC = x + img*L + off.
+template <typename real>
+__global__ void __launch_bounds__(256) k_download(
+    int n, const StepConst* __restrict__ K, const int* __restrict__ slot_of, const double* __restrict__ x,
+    const double* __restrict__ v, const real* __restrict__ F, const uint32_t* __restrict__ img,
+    const double* __restrict__ off, const real* __restrict__ stress, const int* __restrict__ cell,
+    double* __restrict__ ox, double* __restrict__ ou, double* __restrict__ ov, double* __restrict__ of,
+    double* __restrict__ ost, int* __restrict__ ocell)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const int s = slot_of[b];
+    const uint32_t im = img[s];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double xv = x[d * n + s];
+        if (ox) ox[3 * b + d] = xv;
+        if (ou) ou[3 * b + d] = xv + (double)img_get(im, d) * K->L[d] + (off ? off[d * n + b] : 0.0);
+        if (ov) ov[3 * b + d] = v[d * n + s];
+        if (of) of[3 * b + d] = (double)F[d * n + s];
+    }
+    if (ost) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ost[9 * b + q] = stress ? (double)stress[q * n + s] : 0.0;
+    }
+    if (ocell) ocell[b] = cell[s];
+}
+
+}  // namespace dpd

@@ -1,0 +1,231 @@
+"""Python binding of the C ABI in include/dpd_engine.h (ctypes).
+
+This is a thin host-side mirror of the reference's per-step seam: create the
+engine for a box (the CCNTCell statics), upload the beads and the bond/bond-pair
+topology, step, and read back bead state and single-bead sums.  All work runs
+in libospreydpd_cuda.so on the GPU; there is no CPU path, and loading fails
+loudly when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+MIXED = 0
+FP64 = 1
+
+STATUS_CELL_SKIP = 0x1
+STATUS_NONFINITE = 0x2
+STATUS_IMAGE_OVERFLOW = 0x4
+
+EXPORTED = [
+    "dpd_engine_create", "dpd_engine_upload_beads", "dpd_engine_upload_topology",
+    "dpd_engine_set_pair_params", "dpd_engine_set_dt", "dpd_engine_set_thermostat",
+    "dpd_engine_set_conservative", "dpd_engine_step", "dpd_engine_status", "dpd_engine_download",
+    "dpd_engine_cells", "dpd_engine_observables", "dpd_engine_launch_count",
+    "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
+    "dpd_engine_profile_read",
+]
+
+KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
+                "reduce_obs", "download", "kinetic"]
+
+
+class DpdParams(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("wx", C.c_double), ("wy", C.c_double), ("wz", C.c_double),
+                ("dt", C.c_double), ("lam", C.c_double), ("kT", C.c_double),
+                ("ntypes", C.c_int32), ("a", C.POINTER(C.c_double)), ("gamma", C.POINTER(C.c_double)),
+                ("seed", C.c_uint64), ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+class DpdObs(C.Structure):
+    _fields_ = [("step", C.c_int64), ("n", C.c_int64), ("sum_v", C.c_double * 3), ("sum_v2", C.c_double * 3),
+                ("virial", C.c_double * 9), ("sum_x", C.c_double * 3), ("ang_mom", C.c_double * 3),
+                ("kT", C.c_double), ("pressure", C.c_double), ("has_virial", C.c_int32), ("pad", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"step": self.step, "n": self.n, "sum_v": list(self.sum_v), "sum_v2": list(self.sum_v2),
+                "virial": list(self.virial), "sum_x": list(self.sum_x), "ang_mom": list(self.ang_mom),
+                "kT": self.kT, "pressure": self.pressure, "has_virial": bool(self.has_virial)}
+
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def load(path: Optional[str] = None) -> C.CDLL:
+    """Loads libospreydpd_cuda.so; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise EngineError(f"{path} is missing: run `python -m osprey_dpd_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.dpd_engine_create.argtypes = [C.POINTER(DpdParams), C.POINTER(vp)]
+    L.dpd_engine_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 7
+    L.dpd_engine_upload_topology.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
+    L.dpd_engine_set_pair_params.argtypes = [vp, C.c_int32, vp, vp]
+    L.dpd_engine_set_dt.argtypes = [vp, C.c_double]
+    L.dpd_engine_set_thermostat.argtypes = [vp, C.c_int32]
+    L.dpd_engine_set_conservative.argtypes = [vp, C.c_int32]
+    L.dpd_engine_step.argtypes = [vp, C.c_int64, C.c_int32]
+    L.dpd_engine_status.argtypes = [vp, C.POINTER(C.c_uint32)]
+    L.dpd_engine_download.argtypes = [vp] + [vp] * 5
+    L.dpd_engine_cells.argtypes = [vp, vp]
+    L.dpd_engine_observables.argtypes = [vp, C.POINTER(DpdObs)]
+    L.dpd_engine_launch_count.argtypes = [vp]
+    L.dpd_engine_launch_count.restype = C.c_int64
+    L.dpd_engine_last_error.argtypes = [vp]
+    L.dpd_engine_last_error.restype = C.c_char_p
+    L.dpd_engine_set_stream.argtypes = [vp, vp]
+    L.dpd_engine_profile.argtypes = [vp, C.c_int32]
+    L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
+    L.dpd_engine_destroy.argtypes = [vp]
+    L.dpd_engine_destroy.restype = None
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class DpdEngine:
+    """One engine instance: a box, its beads and topology, on one GPU."""
+
+    def __init__(self, cells, widths, dt: float, lam: float, kT: float, a, gamma, seed: int,
+                 precision: int = MIXED, device: int = -1):
+        L = load()
+        self._a = np.ascontiguousarray(a, dtype=np.float64)
+        self._g = np.ascontiguousarray(gamma, dtype=np.float64)
+        T = self._a.shape[0]
+        p = DpdParams(int(cells[0]), int(cells[1]), int(cells[2]), float(widths[0]), float(widths[1]),
+                      float(widths[2]), float(dt), float(lam), float(kT), T,
+                      self._a.ctypes.data_as(C.POINTER(C.c_double)), self._g.ctypes.data_as(C.POINTER(C.c_double)),
+                      int(seed) & 0xFFFFFFFFFFFFFFFF, int(precision), int(device))
+        h = C.c_void_p()
+        rc = L.dpd_engine_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise EngineError(f"dpd_engine_create failed ({rc})")
+        self.h = h
+        self.n = 0
+        self.precision = precision
+
+    @classmethod
+    def from_system(cls, system, precision: int = MIXED, device: int = -1, kT: float = None,
+                    gamma_scale: float = 1.0, seed: int = None, topology: bool = True) -> "DpdEngine":
+        eng = cls(system.cells, system.widths, system.dt, system.lam, system.kT if kT is None else kT,
+                  system.a, system.gamma * gamma_scale, abs(int(system.seed if seed is None else seed)),
+                  precision, device)
+        eng.upload_beads(system.ids, system.types, system.movable, system.x, system.unpbc, system.v, system.f)
+        if topology:
+            eng.upload_topology(system.bond_head, system.bond_tail, system.bond_k2, system.bond_l0,
+                                system.angle_first, system.angle_second, system.angle_k3, system.angle_phi0)
+        return eng
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            msg = load().dpd_engine_last_error(self.h)
+            raise EngineError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def upload_beads(self, ids, types, movable, x, unpbc, v, f=None) -> None:
+        n = len(ids)
+        arrs = [np.ascontiguousarray(ids, np.int64), np.ascontiguousarray(types, np.int32),
+                None if movable is None else np.ascontiguousarray(movable, np.uint8),
+                np.ascontiguousarray(x, np.float64), None if unpbc is None else np.ascontiguousarray(unpbc, np.float64),
+                np.ascontiguousarray(v, np.float64), None if f is None else np.ascontiguousarray(f, np.float64)]
+        self._check(load().dpd_engine_upload_beads(self.h, n, *[_p(a) for a in arrs]), "upload_beads")
+        self.n = n
+
+    def upload_topology(self, head, tail, k2, l0, first, second, k3, phi0) -> None:
+        t = [np.ascontiguousarray(head, np.int64), np.ascontiguousarray(tail, np.int64),
+             np.ascontiguousarray(k2, np.float64), np.ascontiguousarray(l0, np.float64),
+             np.ascontiguousarray(first, np.int64), np.ascontiguousarray(second, np.int64),
+             np.ascontiguousarray(k3, np.float64), np.ascontiguousarray(phi0, np.float64)]
+        self._check(load().dpd_engine_upload_topology(self.h, len(t[0]), _p(t[0]), _p(t[1]), _p(t[2]), _p(t[3]),
+                                                      len(t[4]), _p(t[4]), _p(t[5]), _p(t[6]), _p(t[7])),
+                    "upload_topology")
+
+    def set_pair_params(self, a, gamma) -> None:
+        a = np.ascontiguousarray(a, np.float64)
+        g = np.ascontiguousarray(gamma, np.float64)
+        self._check(load().dpd_engine_set_pair_params(self.h, a.shape[0], _p(a), _p(g)), "set_pair_params")
+
+    def set_dt(self, dt: float) -> None:
+        self._check(load().dpd_engine_set_dt(self.h, float(dt)), "set_dt")
+
+    def set_thermostat(self, on: bool) -> None:
+        self._check(load().dpd_engine_set_thermostat(self.h, int(bool(on))), "set_thermostat")
+
+    def set_conservative(self, on: bool) -> None:
+        self._check(load().dpd_engine_set_conservative(self.h, int(bool(on))), "set_conservative")
+
+    def step(self, first_step: int, nsteps: int) -> None:
+        self._check(load().dpd_engine_step(self.h, int(first_step), int(nsteps)), "step")
+
+    def status(self) -> int:
+        bits = C.c_uint32(0)
+        self._check(load().dpd_engine_status(self.h, C.byref(bits)), "status")
+        return int(bits.value)
+
+    def download(self, stress: bool = True) -> dict:
+        n = self.n
+        out = {k: np.zeros((n, 3)) for k in ("x", "unpbc", "v", "f")}
+        out["stress"] = np.zeros((n, 9)) if stress else None
+        self._check(load().dpd_engine_download(self.h, _p(out["x"]), _p(out["unpbc"]), _p(out["v"]), _p(out["f"]),
+                                               _p(out["stress"])), "download")
+        return out
+
+    def download_into(self, x=None, unpbc=None, v=None, f=None, stress=None) -> None:
+        self._check(load().dpd_engine_download(self.h, _p(x), _p(unpbc), _p(v), _p(f), _p(stress)), "download")
+
+    def cells(self) -> np.ndarray:
+        c = np.zeros(self.n, dtype=np.int32)
+        self._check(load().dpd_engine_cells(self.h, _p(c)), "cells")
+        return c
+
+    def observables(self) -> dict:
+        o = DpdObs()
+        self._check(load().dpd_engine_observables(self.h, C.byref(o)), "observables")
+        return o.as_dict()
+
+    def set_stream(self, stream_handle: int) -> None:
+        """Queue on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""
+        self._check(load().dpd_engine_set_stream(self.h, C.c_void_p(int(stream_handle) or None)), "set_stream")
+
+    def profile(self, on: bool) -> None:
+        self._check(load().dpd_engine_profile(self.h, int(bool(on))), "profile")
+
+    def profile_read(self) -> dict:
+        ms = np.zeros(len(KERNEL_NAMES))
+        cnt = np.zeros(len(KERNEL_NAMES), dtype=np.int64)
+        self._check(load().dpd_engine_profile_read(self.h, _p(ms), _p(cnt)), "profile_read")
+        return {k: {"ms": float(ms[i]), "launches": int(cnt[i])} for i, k in enumerate(KERNEL_NAMES)}
+
+    def launch_count(self) -> int:
+        return int(load().dpd_engine_launch_count(self.h))
+
+    def close(self) -> None:
+        h = getattr(self, "h", None)
+        if h:
+            load().dpd_engine_destroy(h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
