@@ -41,6 +41,7 @@ extern "C" {
 #define DPD_E_BOX             -4   /* bead outside the box at upload          */
 #define DPD_E_STATUS          -5   /* device status word reported a fatal condition */
 #define DPD_E_NOMEM           -6   /* host or device allocation failed       */
+#define DPD_E_LIMIT           -7   /* system larger than a fixed-size buffer allows */
 
 #define DPD_PRECISION_MIXED    0   /* FP32 pair/bond forces, FP64 x, v and sums */
 #define DPD_PRECISION_FP64     1   /* everything FP64                          */
@@ -170,6 +171,42 @@ DPD_API int64_t dpd_engine_launch_count(const dpd_engine* e);
 
 DPD_API const char* dpd_engine_last_error(const dpd_engine* e);
 DPD_API void dpd_engine_destroy(dpd_engine* e);
+
+/* ---- Pair forces without any allocation ---------------------------------
+ * This entry point has no counterpart in the reference.  It is for callers
+ * that may not allocate device memory at the moment they need forces: a host
+ * program whose memory pool owns the whole GPU, a capture-sensitive or
+ * real-time loop where cudaMalloc would synchronise or stall the device, or a
+ * plug-in whose host forbids library-side allocations.  Such a caller owns
+ * its bead and force buffers but cannot give the engine the cell-list
+ * scratch it would otherwise cudaMalloc (dpd_engine_create/upload).
+ *
+ * It computes the DPD pair forces of CCNTCell::UpdateForce (conservative,
+ * dissipative and random; FP32 arithmetic, the engine's pair kernel) for
+ * beads at positions x3 with the velocities v3 the forces should see (the
+ * intermediate v~ of the step), types and noise ids, at timestep `step` (which
+ * keys the pair noise), and writes them as FP64 to f3 in the caller's bead
+ * order.  x3, v3, f3 (n*3 doubles, xyz interleaved), type and id (n int32)
+ * are DEVICE pointers.  params->precision is ignored; params->device selects
+ * the GPU (-1: current).  The work is queued on cuda_stream (NULL: the legacy
+ * default stream) and the call returns after it has finished.
+ *
+ * Scratch: one fixed file-scope device array of about 4.5 MB, held by every
+ * GPU that loads the library until the process exits.  Limits:
+ * n <= DPD_NOALLOC_MAX_BEADS and nx*ny*nz <= DPD_NOALLOC_MAX_CELLS, otherwise
+ * DPD_E_LIMIT with nothing launched.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the one array and each call clears the
+ * parts that must start at zero, so calls that overlap on the GPU (other
+ * threads or streams on the same device) race and must be serialised by the
+ * caller.  Returns DPD_E_BOX if a position lies outside the box (forces are
+ * then not meaningful), DPD_E_ARG for bad arguments, DPD_E_CUDA on a CUDA
+ * error.  No cudaMalloc, cudaFree or other allocating routine is called. */
+#define DPD_NOALLOC_MAX_BEADS   65536
+#define DPD_NOALLOC_MAX_CELLS   32768
+DPD_API int dpd_pair_forces_noalloc(const dpd_params* params, int64_t step, int64_t n,
+                                    const double* x3, const double* v3, const int32_t* type,
+                                    const int32_t* id, double* f3, void* cuda_stream);
 
 #ifdef __cplusplus
 }

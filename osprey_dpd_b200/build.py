@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libospreydpd_cuda.so")
-SOURCES = [os.path.join(HERE, "csrc", "dpd_engine.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "dpd_engine.cu"), os.path.join(HERE, "csrc", "dpd_noalloc.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "dpd_engine.h")]
 

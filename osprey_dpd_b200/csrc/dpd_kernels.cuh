@@ -19,6 +19,8 @@
 //                  sample steps                      (Bond.cpp:111-162,
 //                  BondPair.cpp:138-286, CNTCell.cpp:2280-2310,
 //                  Monitor.cpp:790-1040)
+// Non-template kernels have internal linkage so that more than one
+// translation unit of the library can include this header.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(256) k_update_pos(
 // start[c] = sum of count[0..c); one block per chunk of kScanChunk cells.  The
 // chunk's base is the sum of the per-chunk totals counted by k_update_pos.
 // Counts are cleared for the next step.
-__global__ void __launch_bounds__(kScanThreads) k_scan_cells(
+static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     int ncell, int n, int* __restrict__ count, const int* __restrict__ block_count,
     int* __restrict__ start)
 {
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
 }
 
 // new arrival slot -> old slot; also clears the per-chunk totals.
-__global__ void __launch_bounds__(256) k_permute(
+static __global__ void __launch_bounds__(256) k_permute(
     int n, int nchunk, const int* __restrict__ cell, const int* __restrict__ rank,
     const int* __restrict__ start, int* __restrict__ perm, int* __restrict__ block_count)
 {
@@ -563,7 +565,7 @@ __global__ void __launch_bounds__(256) k_update_mom(
 }
 
 // Fixed-order sum of the per-block partials (deterministic).
-__global__ void __launch_bounds__(256) k_reduce_obs(int nblocks, const double* __restrict__ partials,
+static __global__ void __launch_bounds__(256) k_reduce_obs(int nblocks, const double* __restrict__ partials,
                                                      double* __restrict__ out)
 {
     __shared__ double red[256 / 32];
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(256) k_reduce_obs(int nblocks, const double* _
 }
 
 // Kinetic sums without a force evaluation (state just uploaded).
-__global__ void __launch_bounds__(256) k_kinetic_partials(int n, const double* __restrict__ x,
+static __global__ void __launch_bounds__(256) k_kinetic_partials(int n, const double* __restrict__ x,
                                                            const double* __restrict__ v,
                                                            double* __restrict__ partials)
 {
