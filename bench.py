@@ -9,9 +9,10 @@ dt = 0.02.  Synthetic, seeded (osprey_dpd_b200/workloads.py).
 A step is one full DPD timestep (UpdatePos, cell re-binning, pair forces,
 bond + bond-pair forces, UpdateMom).  `value` is the mixed-precision
 (FP32 forces, FP64 positions/velocities/sums) throughput with the state
-resident in HBM; the all-FP64 form is timed the same way.  L2 is flushed (a
-256 MiB write) before every timed step, each step is timed with CUDA events on
-the engine's stream, and the max over ranks is reported.  `e2e` is the same
+resident in HBM; the all-FP64 form is timed the same way.  L2 is flushed before
+every timed step (a 256 MiB write, then a 256 MiB read of another buffer so
+that the write's dirty lines are back in HBM), each step is timed with CUDA
+events on the engine's stream, and the max over ranks is reported.  `e2e` is the same
 metric through the C ABI with host buffers: upload the bead state, run one
 reference sample period (100 steps), read back the single-bead sums and the
 full bead state.
@@ -41,7 +42,8 @@ import numpy as np  # noqa: E402
 
 METRIC = "bead-steps/s, 393k-bead bilayer: FP32/FP64-mixed vs all-FP64, 1 B200"
 UNIT = "bead-steps/s"
-E2E_PERIOD = 100          # SamplePeriod of the reference's bilayer example (examples/dmpci.bilayer)
+SAMPLE_PERIOD = 100       # SamplePeriod of the reference's bilayer example (examples/dmpci.bilayer)
+E2E_PERIOD = SAMPLE_PERIOD
 L2_FLUSH_BYTES = 256 << 20
 SLOTS_PER_BEAD_STEP = 755.0   # pair-force issue work per bead-step (half shell, rho = 3)
 ALG_BYTES_PER_BEAD_STEP = {"mixed": 124.0, "fp64": 148.0}   # whole-step algorithmic HBM bytes
@@ -177,13 +179,22 @@ def run_reference_arm(args):
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool):
     """Per-step device time (ms) with L2 flushed before each step."""
     eng = engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
+    eng.set_sample_period(SAMPLE_PERIOD)
     stream = torch.cuda.Stream(device=dev)
     eng.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    clean = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def flush_l2():
+        # evict the state by writing a buffer larger than L2, then read a second
+        # one so the dirty lines of the first are written back before the step
+        flush.zero_()
+        return clean.sum()
+
     t = 1
     for _ in range(warmup):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            flush_l2()
         eng.step(t, 1)
         t += 1
     torch.cuda.synchronize(dev)
@@ -193,7 +204,7 @@ def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev
     launches0 = eng.launch_count()
     for k in range(steps):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            flush_l2()
             evs[k][0].record(stream)
         eng.step(t, 1)
         with torch.cuda.stream(stream):
@@ -254,13 +265,15 @@ def read_traffic(n_beads: int):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", default="bilayer", choices=["bilayer", "water", "binary", "polymer"])
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=12, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -298,7 +311,10 @@ def main():
 
     results = {}
     clocks = None
-    for prec_name, prec in (("mixed", E.MIXED), ("fp64", E.FP64)):
+    precs = [("mixed", E.MIXED), ("fp64", E.FP64)]
+    if args.precision != "both":
+        precs = [p for p in precs if p[0] == args.precision]
+    for prec_name, prec in precs:
         barrier()
         sampler = ClockSampler(local) if prec_name == "mixed" else None
         if sampler:
@@ -314,9 +330,12 @@ def main():
                               "status": status,
                               "value": ws * system.n * args.steps / (total_ms / 1000.0)}
 
-    e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch)
-    e2e_t = max_over_ranks(sum(e2e_times))
-    e2e_value = ws * system.n * E2E_PERIOD * len(e2e_times) / e2e_t
+    e2e_value = h2d_step = d2h_step = None
+    e2e_times = []
+    if not args.no_e2e:
+        e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch)
+        e2e_t = max_over_ranks(sum(e2e_times))
+        e2e_value = ws * system.n * E2E_PERIOD * len(e2e_times) / e2e_t
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -332,7 +351,7 @@ def main():
             dist.destroy_process_group()
         return 0
 
-    mixed = results["mixed"]
+    mixed = results.get("mixed") or results["fp64"]
     pair = mixed["prof"]["pair_forces"]
     t_pair = pair["ms"] / max(pair["launches"], 1) / 1000.0
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -348,10 +367,11 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 state",
         "data": "synthetic (seeded generator, reference workload shapes)",
         "config": {"workload": desc, "n_beads": system.n, "cells": list(system.cells), "dt": system.dt,
-                   "precision": "mixed", "l2": "flushed (256 MiB write) before every timed step",
+                   "precision": "mixed", "l2": "flushed before every timed step (256 MiB write, then 256 MiB read so no dirty lines remain)",
+                   "sample_period": SAMPLE_PERIOD,
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
-        "fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
-                 "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]},
+        "fp64": ({"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
+                  "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]} if "fp64" in results else None),
         "roofline": {"bound": "issue", "kernel": "pair_forces (mixed)",
                      "achieved": achieved / 1e9, "peak": issue_peak / 1e9, "unit": "Gslot/s",
                      "frac": achieved / issue_peak,

@@ -52,7 +52,8 @@ extern "C" {
                                             reference logs CLogCNTBeadError, CNTCell.cpp:2650) */
 #define DPD_STATUS_NONFINITE      0x2u  /* a non-finite position, velocity or force       */
 #define DPD_STATUS_IMAGE_OVERFLOW 0x4u  /* a periodic image counter left +-511 box lengths */
-#define DPD_STATUS_FATAL_MASK     (DPD_STATUS_NONFINITE | DPD_STATUS_IMAGE_OVERFLOW)
+#define DPD_STATUS_INTERNAL       0x8u  /* an internal capacity check tripped (a bug): results invalid */
+#define DPD_STATUS_FATAL_MASK     (DPD_STATUS_NONFINITE | DPD_STATUS_IMAGE_OVERFLOW | DPD_STATUS_INTERNAL)
 
 /* Kernel ids for dpd_engine_profile_read (the kernels of one step, in order). */
 #define DPD_KERNEL_UPDATE_POS   0   /* UpdatePos drift + cell move             */
@@ -137,19 +138,29 @@ DPD_API int dpd_engine_set_conservative(dpd_engine* e, int32_t on);
  * The single-bead sums are taken at the end of the last step. */
 DPD_API int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps);
 
+/* Steps at which the single-bead sums and the per-bead virial are taken:
+ * period > 0 samples every step with m_SimTime % period == 0, the rule of
+ * ISimState::TimeToSample (ISimState.cpp:468-471); period = 0 (the default)
+ * samples at the last step of every dpd_engine_step call.  The virial costs
+ * extra work, so other steps skip it as the reference's monitor does. */
+DPD_API int dpd_engine_set_sample_period(dpd_engine* e, int64_t period);
+
 /* Waits for queued work; returns the device status bits seen so far. */
 DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
 
 /* Copies the state out (synchronous); any pointer may be NULL.  stress9 is
- * the per-bead virial of the last step (pair part split evenly between the
- * two beads of a pair; bond part on the head bead as Bond.cpp:151-160). */
+ * the per-bead virial of the latest sample step (pair part split evenly
+ * between the two beads of a pair; bond part on the head bead as
+ * Bond.cpp:151-160), zero before any sample step. */
 DPD_API int dpd_engine_download(dpd_engine* e, double* x3, double* unpbc3, double* v3, double* f3,
                         double* stress9);
 
 /* Index of the CNT cell each bead is filed in (nx*(ny*iz+iy)+ix). */
 DPD_API int dpd_engine_cells(dpd_engine* e, int32_t* cell);
 
-/* Single-bead sums of the last step (synchronous). */
+/* Single-bead sums of the latest sample step (synchronous); before any sample
+ * step since the upload, the kinetic sums of the current state without a
+ * virial (has_virial = 0). */
 DPD_API int dpd_engine_observables(dpd_engine* e, dpd_obs* out);
 
 /* Queues all further work on the caller's CUDA stream (a cudaStream_t passed

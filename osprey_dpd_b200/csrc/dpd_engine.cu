@@ -10,12 +10,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "dpd_kernels.cuh"
+#include "pair_forces.cuh"
 
 using namespace dpd;
 
@@ -97,6 +99,9 @@ struct dpd_engine {
     double* h_obs = nullptr;
     bool obs_valid = false;
     bool obs_has_virial = false;
+    int64_t sample_period = 0;      // 0: sample at the last step of every call
+    bool sampled = false;           // a sample step has run since the last upload
+    int64_t last_sample_step = 0;
 
     std::vector<void*> allocations;
 
@@ -108,6 +113,13 @@ struct dpd_engine {
     std::vector<cudaEvent_t> event_pool;
 
     cudaStream_t s() const { return user_stream ? user_stream : stream; }
+
+    // pair-kernel launch shape (DPD_TUNE="hitcap=32,bps=8,carveout=50"; 0 = automatic)
+    int sms = 148;
+    int pair_hitcap = 32;
+    int pair_bps = 0;          // resident blocks per SM for the persistent grid
+    int pair_carveout = -1;    // preferred shared-memory carveout in percent, -1 = driver default
+    bool pair_attr_set[2][2] = {{false, false}, {false, false}};
 };
 
 namespace {
@@ -230,7 +242,6 @@ int queue_step(dpd_engine* e, bool sample)
     const int n = (int)e->n;
     const int a = e->cur, b = 1 - e->cur;
     const int nb = blocks_for(n, kThreads);
-    const int npb = blocks_for(n, kPairThreads);
     cudaStream_t st = e->s();
     int rc;
     {
@@ -261,11 +272,24 @@ int queue_step(dpd_engine* e, bool sample)
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
     {
+        auto kern = sample ? k_pair_forces<real, true> : k_pair_forces<real, false>;
+        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap);
+        const int pv = sizeof(real) == 8 ? 1 : 0, sv = sample ? 1 : 0;
+        if (!e->pair_attr_set[pv][sv]) {
+            CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            if (e->pair_carveout >= 0)
+                CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, e->pair_carveout));
+            e->pair_attr_set[pv][sv] = true;
+        }
+        // one tile per block by default; bps > 0 selects a persistent grid of
+        // sms * bps blocks walking contiguous tiles
+        const int tiles = blocks_for(n, kPairBlock);
+        const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
-        auto kern = sample ? k_pair_forces_ref<real, true> : k_pair_forces_ref<real, false>;
-        kern<<<npb, kPairThreads, 0, st>>>(n, e->d_K, e->d_step, (const real*)e->d_tab, e->d_cell[b],
-                                            e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
-                                            (real*)e->d_F, (real*)e->d_stress);
+        kern<<<blocks_for(tiles, tpb), kPairBlock, dyn, st>>>(n, e->d_K, e->d_step, (const real*)e->d_tab,
+                                                               e->d_cell[b], e->d_start, (const V4*)e->d_pos4,
+                                                               (const V4*)e->d_vel4, (real*)e->d_F,
+                                                               (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status);
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
     const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
@@ -282,12 +306,34 @@ int queue_step(dpd_engine* e, bool sample)
     if (sample) {
         {
             Timed t(e, DPD_KERNEL_REDUCE_OBS);
-            k_reduce_obs<<<1, 256, 0, st>>>(nb, e->d_partials, e->d_obs);
+            k_reduce_obs<<<1, 32 * kObsTerms, 0, st>>>(nb, e->d_partials, e->d_obs);
         }
         if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
     }
     e->cur = b;
     return DPD_OK;
+}
+
+// "hitcap=32,bps=8,carveout=50": pair-kernel hit-list capacity (8..64), resident
+// blocks per SM for its persistent grid, preferred shared-memory carveout (%).
+void parse_tuning(dpd_engine* e, const char* spec)
+{
+    std::string str(spec);
+    size_t pos = 0;
+    while (pos < str.size()) {
+        size_t end = str.find(',', pos);
+        if (end == std::string::npos) end = str.size();
+        const std::string item = str.substr(pos, end - pos);
+        const size_t eq = item.find('=');
+        if (eq != std::string::npos) {
+            const std::string key = item.substr(0, eq);
+            const int val = atoi(item.c_str() + eq + 1);
+            if (key == "hitcap") e->pair_hitcap = std::min(std::max(val, 8), (int)kHitCapMax);
+            else if (key == "bps") e->pair_bps = std::max(val, 0);
+            else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
+        }
+        pos = end + 1;
+    }
 }
 
 void release_topology(dpd_engine* e)
@@ -347,6 +393,8 @@ int dpd_engine_create(const dpd_params* p, dpd_engine** out)
             rc = fail(e, DPD_E_CUDA, "no CUDA device");
             break;
         }
+        cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);
+        if (const char* tune = getenv("DPD_TUNE")) parse_tuning(e, tune);
         if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
             rc = fail(e, DPD_E_CUDA, "cudaStreamCreate failed");
             break;
@@ -402,6 +450,14 @@ void dpd_engine_destroy(dpd_engine* e)
 }
 
 const char* dpd_engine_last_error(const dpd_engine* e) { return e ? e->err.c_str() : "null engine"; }
+
+int dpd_engine_set_sample_period(dpd_engine* e, int64_t period)
+{
+    if (!e) return DPD_E_ARG;
+    if (period < 0) return fail(e, DPD_E_ARG, "negative sample period");
+    e->sample_period = period;
+    return DPD_OK;
+}
 
 int dpd_engine_set_stream(dpd_engine* e, void* cuda_stream)
 {
@@ -565,7 +621,7 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
             hf[(size_t)d * n + s] = f3 ? f3[3 * b + d] : 0.0;
         }
         hbid[s] = b;
-        htf[s] = type[b] | ((movable && !movable[b]) ? (1 << 16) : 0);
+        htf[s] = type[b] | ((movable && !movable[b]) ? kFlagFrozen : 0);
         hcell[s] = cell[b];
         himg[s] = img[b];
     }
@@ -594,6 +650,7 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
     if (rc) return rc;
     e->uploaded = true;
     e->stepped = false;
+    e->sampled = false;
     e->obs_valid = false;
     return DPD_OK;
 }
@@ -659,6 +716,19 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         terms[fillp[a4[1][i]]++] = (int)(i * 8 + kAngle0);   // first bond's tail: force [0]
         terms[fillp[a4[0][i]]++] = (int)(i * 8 + kAngle1);   // middle bead:       force [1]
         terms[fillp[a4[2][i]]++] = (int)(i * 8 + kAngle2);   // second bond's head: force [2]
+    }
+    // mark the beads that have terms (flag bit 17) so k_update_mom skips the
+    // topology lookup for all others
+    {
+        std::vector<int> tf(n), bid(n);
+        const int c = e->cur;
+        CU(cudaMemcpy(tf.data(), e->d_tf[c], n * sizeof(int), cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(bid.data(), e->d_bid[c], n * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int64_t sl = 0; sl < n; ++sl) {
+            const int b = bid[sl];
+            tf[sl] = (tf[sl] & ~kFlagBonded) | (cnt[b + 1] > cnt[b] ? kFlagBonded : 0);
+        }
+        CU(cudaMemcpy(e->d_tf[c], tf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     }
     release_topology(e);
     int rc;
@@ -745,10 +815,16 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     *e->h_step = first_step;
     CU(cudaMemcpyAsync(e->d_step, e->h_step, sizeof(int64_t), cudaMemcpyHostToDevice, e->s()));
     for (int32_t k = 0; k < nsteps; ++k) {
-        const bool sample = (k == nsteps - 1);
+        const int64_t t = first_step + k;
+        // ISimState::TimeToSample (ISimState.cpp:468-471): m_SimTime % SamplePeriod == 0
+        const bool sample = e->sample_period > 0 ? (t % e->sample_period == 0) : (k == nsteps - 1);
         const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, sample)
                                                              : queue_step<float>(e, sample);
         if (rc) return rc;
+        if (sample) {
+            e->sampled = true;
+            e->last_sample_step = t;
+        }
     }
     e->stepped = true;
     e->obs_valid = false;
@@ -779,12 +855,12 @@ static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, doubl
     if (e->precision == DPD_PRECISION_FP64)
         k_download<double><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
             n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->d_off,
-            e->stepped ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
+            e->sampled ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     else
         k_download<float><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
             n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->d_off,
-            e->stepped ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
+            e->sampled ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     int rc = check_launch(e, "k_download");
     if (rc) return rc;
@@ -818,19 +894,19 @@ int dpd_engine_observables(dpd_engine* e, dpd_obs* out)
     if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
     CU(cudaSetDevice(e->device));
     const int n = (int)e->n;
-    if (!e->stepped) {
+    if (!e->sampled) {
         const int nb = blocks_for(n, kThreads);
         k_kinetic_partials<<<nb, kThreads, 0, e->s()>>>(n, e->d_x[e->cur], e->d_v[e->cur], e->d_partials);
         int rc = check_launch(e, "k_kinetic_partials");
         if (rc) return rc;
-        k_reduce_obs<<<1, 256, 0, e->s()>>>(nb, e->d_partials, e->d_obs);
+        k_reduce_obs<<<1, 32 * kObsTerms, 0, e->s()>>>(nb, e->d_partials, e->d_obs);
         if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
     }
     CU(cudaMemcpyAsync(e->h_obs, e->d_obs, kObsTerms * sizeof(double), cudaMemcpyDeviceToHost, e->s()));
     CU(cudaStreamSynchronize(e->s()));
     const double* h = e->h_obs;
     memset(out, 0, sizeof *out);
-    out->step = e->stepped ? e->last_step : 0;
+    out->step = e->sampled ? e->last_sample_step : (e->stepped ? e->last_step : 0);
     out->n = e->n;
     for (int d = 0; d < 3; ++d) {
         out->sum_v[d] = h[d];
@@ -838,8 +914,8 @@ int dpd_engine_observables(dpd_engine* e, dpd_obs* out)
         out->sum_x[d] = h[15 + d];
         out->ang_mom[d] = h[18 + d];
     }
-    out->has_virial = e->stepped ? 1 : 0;
-    for (int q = 0; q < 9; ++q) out->virial[q] = e->stepped ? h[6 + q] : 0.0;
+    out->has_virial = e->sampled ? 1 : 0;
+    for (int q = 0; q < 9; ++q) out->virial[q] = e->sampled ? h[6 + q] : 0.0;
     const dpd_params& p = e->params;
     const double V = (p.nx * p.wx) * (p.ny * p.wy) * (p.nz * p.wz);
     const double v2 = out->sum_v2[0] + out->sum_v2[1] + out->sum_v2[2];

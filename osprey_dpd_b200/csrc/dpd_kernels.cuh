@@ -31,7 +31,7 @@ namespace dpd {
 
 constexpr int kMaxTypes = 32;
 constexpr int kScanThreads = 256;
-constexpr int kScanPerThread = 8;
+constexpr int kScanPerThread = 4;
 constexpr int kScanChunk = kScanThreads * kScanPerThread;   // cells per scan block
 constexpr int kObsTerms = 21;   // sum_v[3] sum_v2[3] virial[9] sum_x[3] angmom[3]
 
@@ -55,9 +55,13 @@ struct StepConst {
     uint64_t seed;
 };
 
-// Bead flags word: type in bits 0..15, frozen (never moves) in bit 16.
+// Bead flags word: type in bits 0..15, frozen (never moves) in bit 16,
+// has bond or bond-pair terms in bit 17.
 __device__ __forceinline__ int flag_type(int tf) { return tf & 0xFFFF; }
 __device__ __forceinline__ bool flag_frozen(int tf) { return (tf >> 16) & 1; }
+__device__ __forceinline__ bool flag_bonded(int tf) { return (tf >> 17) & 1; }
+constexpr int kFlagFrozen = 1 << 16;
+constexpr int kFlagBonded = 1 << 17;
 
 template <typename real> struct Vec4;
 template <> struct Vec4<float> { typedef float4 type; };
@@ -76,7 +80,7 @@ __device__ __forceinline__ int real_bits(double v) { return (int)__double_as_lon
 // (CNTCell.cpp:598-604, 1768-2254), wrapping the moved coordinates only when
 // both cells lie on the box boundary.  Frozen beads keep their cell.
 template <typename real>
-__global__ void __launch_bounds__(256) k_update_pos(
+__global__ void __launch_bounds__(256, 6) k_update_pos(
     int n, const StepConst* __restrict__ K, double* __restrict__ x, const double* __restrict__ v,
     const real* __restrict__ F, const int* __restrict__ tf, uint32_t* __restrict__ img,
     int* __restrict__ cell, int* __restrict__ rank, int* __restrict__ count,
@@ -87,9 +91,19 @@ __global__ void __launch_bounds__(256) k_update_pos(
     int cnew = 0;
     unsigned bad = 0;
     if (live) {
+        // every load first, so one memory round trip covers them all
         const int c = cell[s];
+        const int tfl = tf[s];
+        double x0[3], v0[3], f0[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x0[d] = x[d * n + s];
+            v0[d] = v[d * n + s];
+            f0[d] = (double)F[d * n + s];
+        }
+        const uint32_t im0 = img[s];
         cnew = c;
-        if (!flag_frozen(tf[s])) {
+        if (!flag_frozen(tfl)) {
             const double dt = K->dt, h2 = K->halfdt2;
             const int nx = K->nc[0], ny = K->nc[1], nz = K->nc[2];
             int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
@@ -100,13 +114,13 @@ __global__ void __launch_bounds__(256) k_update_pos(
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 // x += dt*v + dt^2/2*F with the reference's rounding (no fused multiply-add)
-                const double dx = __dadd_rn(__dmul_rn(dt, v[d * n + s]), __dmul_rn(h2, (double)F[d * n + s]));
-                xn[d] = __dadd_rn(x[d * n + s], dx);
+                const double dx = __dadd_rn(__dmul_rn(dt, v0[d]), __dmul_rn(h2, f0[d]));
+                xn[d] = __dadd_rn(x0[d], dx);
                 const double BL = __dmul_rn((double)ci[d], K->w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
                 const double TR = __dadd_rn(BL, K->w[d]);
                 mv[d] = (xn[d] > TR) ? 1 : ((xn[d] < BL) ? -1 : 0);
             }
-            uint32_t im = img[s];
+            uint32_t im = im0;
             if (mv[0] | mv[1] | mv[2]) {
                 int nci[3];
                 for (int d = 0; d < 3; ++d) {
@@ -140,15 +154,22 @@ __global__ void __launch_bounds__(256) k_update_pos(
             img[s] = im;
             cell[s] = cnew;
         }
-        rank[s] = atomicAdd(&count[cnew], 1);
     }
-    // one atomic per scan chunk per warp
+    // Warp-aggregated counting: lanes bound for the same cell take one atomic
+    // (beads are cell-sorted, so a warp spans ~11 cells) and ranks follow lane
+    // order inside the group; one atomic per scan chunk per warp as well.
     const unsigned act = __ballot_sync(0xffffffffu, live);
     if (live) {
-        const int chunk = cnew / kScanChunk;
-        const unsigned peers = __match_any_sync(act, chunk);
+        const int lane = threadIdx.x & 31;
+        const unsigned peers = __match_any_sync(act, cnew);
         const int leader = __ffs(peers) - 1;
-        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&block_count[chunk], __popc(peers));
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&count[cnew], __popc(peers));
+        base = __shfl_sync(act, base, leader);
+        rank[s] = base + __popc(peers & ((1u << lane) - 1u));
+        const int chunk = cnew / kScanChunk;
+        const unsigned cpeers = __match_any_sync(act, chunk);
+        if (lane == __ffs(cpeers) - 1) atomicAdd(&block_count[chunk], __popc(cpeers));   // result unused: a reduction
     }
     if (bad) atomicOr(status, bad);
 }
@@ -227,7 +248,7 @@ static __global__ void __launch_bounds__(256) k_permute(
 // and intermediate velocity v~ = v + lambda*dt*F_old (CNTCell.cpp:1743-1747),
 // with the bead type and the noise id in the fourth component.
 template <typename real>
-__global__ void __launch_bounds__(256) k_gather(
+__global__ void __launch_bounds__(256, 6) k_gather(
     int n, const StepConst* __restrict__ K, const int* __restrict__ perm, const int* __restrict__ start,
     const double* __restrict__ x_in, const double* __restrict__ v_in, const real* __restrict__ F_in,
     const int* __restrict__ bid_in, const int* __restrict__ tf_in, const uint32_t* __restrict__ img_in,
@@ -240,22 +261,33 @@ __global__ void __launch_bounds__(256) k_gather(
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
     const int s = perm[d];
+    // the bead's state is independent of its final slot: load it before the
+    // rank scan so both memory round trips overlap
     const int c = cell_in[s];
+    const int b = bid_in[s];
+    const int tfl = tf_in[s];
+    const uint32_t im = img_in[s];
+    double xs[3], vs[3];
+    real fs[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        xs[q] = x_in[q * n + s];
+        vs[q] = v_in[q * n + s];
+        fs[q] = F_in[q * n + s];
+    }
     const int beg = start[c], end = start[c + 1];
     int k = 0;
     for (int e = beg; e < end; ++e) k += (perm[e] < s);
     const int o = beg + k;
-    const int b = bid_in[s];
-    const int tfl = tf_in[s];
     const int nx = K->nc[0], ny = K->nc[1];
     const int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
     const bool frozen = flag_frozen(tfl);
     real rel[3], vt[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        const double xv = x_in[q * n + s];
-        const double vv = v_in[q * n + s];
-        const real fv = F_in[q * n + s];
+        const double xv = xs[q];
+        const double vv = vs[q];
+        const real fv = fs[q];
         x_out[q * n + o] = xv;
         v_out[q * n + o] = vv;
         Fold_out[q * n + o] = fv;
@@ -264,7 +296,7 @@ __global__ void __launch_bounds__(256) k_gather(
     }
     bid_out[o] = b;
     tf_out[o] = tfl;
-    img_out[o] = img_in[s];
+    img_out[o] = im;
     cell_out[o] = c;
     slot_of[b] = o;
     typedef typename Vec4<real>::type V4;
@@ -426,7 +458,7 @@ __device__ __forceinline__ void unwrapped(const StepConst* __restrict__ K, const
 // UpdatePos skips them), keep accumulating force.  On sample steps the FP64
 // single-bead sums are reduced per block.
 template <typename real, bool SAMPLE>
-__global__ void __launch_bounds__(256) k_update_mom(
+__global__ void __launch_bounds__(256, 4) k_update_mom(
     int n, const StepConst* __restrict__ K, int64_t* __restrict__ step_ptr,
     const double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
     const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
@@ -443,9 +475,11 @@ __global__ void __launch_bounds__(256) k_update_mom(
         const bool frozen = flag_frozen(tfl);
         real f[3] = {F[s], F[n + s], F[2 * n + s]};
         real fo[3] = {Fold[s], Fold[n + s], Fold[2 * n + s]};
+        const double v0[3] = {v[s], v[n + s], v[2 * n + s]};
         if (frozen) { f[0] += fo[0]; f[1] += fo[1]; f[2] += fo[2]; }
         real bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const int t0 = topo.csr_ptr[b], t1 = topo.csr_ptr[b + 1];
+        const bool bonded = flag_bonded(tfl);
+        const int t0 = bonded ? topo.csr_ptr[b] : 0, t1 = bonded ? topo.csr_ptr[b + 1] : 0;
         for (int t = t0; t < t1; ++t) {
             const int term = topo.csr_term[t];
             const int code = term & 7, idx = term >> 3;
@@ -519,7 +553,7 @@ __global__ void __launch_bounds__(256) k_update_mom(
         double vn[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            vn[d] = v[d * n + s];
+            vn[d] = v0[d];
             if (!frozen) {
                 vn[d] = __dadd_rn(vn[d], __dmul_rn(K->halfdt, __dadd_rn((double)f[d], (double)fo[d])));
                 v[d * n + s] = vn[d];
@@ -564,25 +598,17 @@ __global__ void __launch_bounds__(256) k_update_mom(
     if (s == 0) *step_ptr += 1;
 }
 
-// Fixed-order sum of the per-block partials (deterministic).
-static __global__ void __launch_bounds__(256) k_reduce_obs(int nblocks, const double* __restrict__ partials,
-                                                     double* __restrict__ out)
+// Fixed-order sum of the per-block partials (deterministic): one warp per
+// term, a fixed strided split and a fixed shuffle tree.
+static __global__ void __launch_bounds__(32 * kObsTerms) k_reduce_obs(int nblocks, const double* __restrict__ partials,
+                                                                       double* __restrict__ out)
 {
-    __shared__ double red[256 / 32];
-    for (int q = 0; q < kObsTerms; ++q) {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) a += partials[b * kObsTerms + q];
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double a = 0.0;
+    for (int b = lane; b < nblocks; b += 32) a += partials[b * kObsTerms + q];
 #pragma unroll
-        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            out[q] = t;
-        }
-        __syncthreads();
-    }
+    for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) out[q] = a;
 }
 
 // Kinetic sums without a force evaluation (state just uploaded).

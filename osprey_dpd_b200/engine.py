@@ -31,7 +31,7 @@ EXPORTED = [
     "dpd_engine_set_conservative", "dpd_engine_step", "dpd_engine_status", "dpd_engine_download",
     "dpd_engine_cells", "dpd_engine_observables", "dpd_engine_launch_count",
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
-    "dpd_engine_profile_read",
+    "dpd_engine_profile_read", "dpd_engine_set_sample_period",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -91,6 +91,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_last_error.argtypes = [vp]
     L.dpd_engine_last_error.restype = C.c_char_p
     L.dpd_engine_set_stream.argtypes = [vp, vp]
+    L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
     L.dpd_engine_destroy.argtypes = [vp]
@@ -201,6 +202,9 @@ class DpdEngine:
         o = DpdObs()
         self._check(load().dpd_engine_observables(self.h, C.byref(o)), "observables")
         return o.as_dict()
+
+    def set_sample_period(self, period: int) -> None:
+        self._check(load().dpd_engine_set_sample_period(self.h, int(period)), "set_sample_period")
 
     def set_stream(self, stream_handle: int) -> None:
         """Queue on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""

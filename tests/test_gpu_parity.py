@@ -113,3 +113,53 @@ def test_bitwise_deterministic(engine_mod, precision):
         eng.close()
     for k in ("x", "v", "f", "stress"):
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_sample_period_takes_sums_at_sample_steps(engine_mod, oracle_mod, precision):
+    """With a sample period the sums describe the latest step t with
+    t % period == 0 (ISimState::TimeToSample), not the last step run."""
+    s = SYSTEMS["bilayer"]()
+    eng, orc = _pair(engine_mod, oracle_mod, s, precision)
+    eng.set_sample_period(4)
+    eng.step(1, 6)
+    obs = eng.observables()
+    assert obs["step"] == 4 and obs["has_virial"]
+    orc.step(1, 4)
+    o = orc.state()
+    v2 = float(np.sum(o["v"] ** 2))
+    tol = 2e-5 if precision == 0 else 1e-10
+    assert abs(obs["kT"] - v2 / (3 * s.n)) < tol * (v2 / (3 * s.n))
+    vir = o["stress"].sum(axis=0)
+    assert np.allclose(obs["virial"], vir, rtol=0, atol=tol * float(np.max(np.abs(vir))))
+
+
+def _dense_cluster_system():
+    """Water with 60 extra beads packed inside one cell: neighbour rows far
+    longer than any per-lane hit list, and many overlapping pairs."""
+    s = W.water(8)
+    rng = np.random.default_rng(7)
+    extra = 60
+    c = np.array([3.5, 4.5, 2.5])
+    pts = c + (rng.random((extra, 3)) - 0.5) * 0.9
+    s2 = W._assemble("water", s.cells, s.widths, s.density, s.dt, s.lam, s.kT, s.seed, s.type_names, s.a,
+                     s.gamma, [W.PolymerSpec("Water", ("W",), s.n + extra)], [], [],
+                     np.zeros(s.n + extra, np.int32), np.concatenate([s.unpbc, pts]),
+                     np.concatenate([s.v, np.zeros((extra, 3))]))
+    return s2
+
+
+@pytest.mark.parametrize("tune", ["", "hitcap=8", "hitcap=64,bps=1"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precision, tune, monkeypatch):
+    """A cell with 60+ beads, under the default and extreme pair-kernel
+    launch shapes (DPD_TUNE): forces still match the oracle."""
+    monkeypatch.setenv("DPD_TUNE", tune)
+    s = _dense_cluster_system()
+    eng, orc = _pair(engine_mod, oracle_mod, s, precision)
+    eng.step(1, 2)
+    orc.step(1, 2)
+    g, o = eng.download(), orc.state()
+    ftol = 1e-4 if precision == 0 else 1e-10
+    assert rel_err(g["f"], o["f"]) < ftol
+    assert eng.status() == 0
