@@ -477,7 +477,12 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
         real fo[3] = {Fold[s], Fold[n + s], Fold[2 * n + s]};
         const double v0[3] = {v[s], v[n + s], v[2 * n + s]};
         if (frozen) { f[0] += fo[0]; f[1] += fo[1]; f[2] += fo[2]; }
-        real bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        // Bonded terms in FP64 in both precision modes: only bonded beads pay
+        // for it, and the bond-pair force with phi0 > 0 divides by
+        // sqrt(1/cos^2 - 1), which FP32 cannot resolve for nearly straight
+        // chains.  The sum is rounded once into the force accumulator.
+        double bf[3] = {0.0, 0.0, 0.0};
+        double bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         const bool bonded = flag_bonded(tfl);
         const int t0 = bonded ? topo.csr_ptr[b] : 0, t1 = bonded ? topo.csr_ptr[b + 1] : 0;
         for (int t = t0; t < t1; ++t) {
@@ -489,19 +494,21 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 double uh[3], ut[3];
                 unwrapped(K, x, img, topo.off, n, n, slot_of[h], h, uh);
                 unwrapped(K, x, img, topo.off, n, n, slot_of[tl], tl, ut);
-                const real bx = (real)(uh[0] - ut[0]), by = (real)(uh[1] - ut[1]), bz = (real)(uh[2] - ut[2]);
-                const real len = sqrt(bx * bx + by * by + bz * bz);
-                const real m = (real)topo.bond_k2[idx] * ((real)topo.bond_l0[idx] - len) / len;
-                const real gx = m * bx, gy = m * by, gz = m * bz;
+                const double bx = uh[0] - ut[0], by = uh[1] - ut[1], bz = uh[2] - ut[2];
+                const double len = sqrt(bx * bx + by * by + bz * bz);
+                const double k2 = topo.bond_k2[idx], l0 = topo.bond_l0[idx];
+                const double gx = k2 * (l0 - len) * bx / len;
+                const double gy = k2 * (l0 - len) * by / len;
+                const double gz = k2 * (l0 - len) * bz / len;
                 if (code == kBondHead) {
-                    f[0] += gx; f[1] += gy; f[2] += gz;
+                    bf[0] += gx; bf[1] += gy; bf[2] += gz;
                     if (SAMPLE) {
                         bs[0] += bx * gx; bs[1] += by * gx; bs[2] += bz * gx;
                         bs[3] += bx * gy; bs[4] += by * gy; bs[5] += bz * gy;
                         bs[6] += bx * gz; bs[7] += by * gz; bs[8] += bz * gz;
                     }
                 } else {
-                    f[0] -= gx; f[1] -= gy; f[2] -= gz;
+                    bf[0] -= gx; bf[1] -= gy; bf[2] -= gz;
                 }
             } else {
                 // CBondPair::AddForce, BondPair.cpp:140-285
@@ -512,38 +519,39 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 unwrapped(K, x, img, topo.off, n, n, slot_of[a1t], a1t, u1t);
                 unwrapped(K, x, img, topo.off, n, n, slot_of[a2h], a2h, u2h);
                 unwrapped(K, x, img, topo.off, n, n, slot_of[a2t], a2t, u2t);
-                real b1[3], b2[3];
+                double b1[3], b2[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    b1[d] = (real)(u1h[d] - u1t[d]);
-                    b2[d] = (real)(u2h[d] - u2t[d]);
+                    b1[d] = u1h[d] - u1t[d];
+                    b2[d] = u2h[d] - u2t[d];
                 }
-                const real l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
-                const real l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
-                const real mag = l1 * l2;
-                if (mag > real(0.0001)) {
-                    const real dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
-                    const real o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
-                    real fm = (real)topo.ang_k3[idx] / mag;
+                const double l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
+                const double l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
+                const double mag = l1 * l2;
+                if (mag > 0.0001) {
+                    const double dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
+                    const double o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
+                    const double k3 = topo.ang_k3[idx];
+                    double fm = k3 / mag;
                     const double s0 = topo.ang_sin0[idx];
-                    if (s0 != 0.0 && fabs((double)dot) > 0.000001) {
-                        const real pre = sqrt(real(1) / (o1 * o2) - real(1));
-                        fm = (real)topo.ang_k3[idx] * ((real)topo.ang_cos0[idx] - (real)s0 / pre) / mag;
-                    }
-                    real g0[3], g2[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        g0[d] = fm * (o1 * b1[d] - b2[d]);
-                        g2[d] = fm * (b1[d] - o2 * b2[d]);
+                    if (s0 != 0.0 && fabs(dot) > 0.000001) {
+                        const double pre = sqrt(1.0 / (o1 * o2) - 1.0);
+                        fm = k3 * (topo.ang_cos0[idx] - s0 / pre) / mag;
                     }
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
-                        if (code == kAngle0) f[d] += g0[d];
-                        else if (code == kAngle2) f[d] += g2[d];
-                        else f[d] += -g0[d] - g2[d];
+                        const double g0 = fm * (o1 * b1[d] - b2[d]);
+                        const double g2 = fm * (b1[d] - o2 * b2[d]);
+                        if (code == kAngle0) bf[d] += g0;
+                        else if (code == kAngle2) bf[d] += g2;
+                        else bf[d] += -g0 - g2;
                     }
                 }
             }
+        }
+        if (bonded) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) f[d] = (real)((double)f[d] + bf[d]);
         }
         F[s] = f[0];
         F[n + s] = f[1];
@@ -563,7 +571,7 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
             const double xs[3] = {x[s], x[n + s], x[2 * n + s]};
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
-                const real st = stress[q * n + s] + bs[q];
+                const real st = (real)((double)stress[q * n + s] + bs[q]);
                 stress[q * n + s] = st;
                 acc[6 + q] = (double)st;
             }

@@ -245,7 +245,7 @@ def binary_mixture(n: int = 32, density: float = 3.0, seed: int = BASE_SEED + 2,
 
 def bilayer(cells: Tuple[int, int, int] = (64, 64, 32), nlipids: int = 6000, density: float = 3.0,
             seed: int = BASE_SEED + 3, dt: float = 0.02, kT: float = 1.0, gamma: float = 4.5,
-            k3: float = 20.0, with_htt: bool = False) -> DpdSystem:
+            k3: float = 20.0, with_htt: bool = False, phi0_deg: float = 0.0) -> DpdSystem:
     """H3T6 lipids in two leaflets about the box mid-plane (heads outward),
     chains along z with 0.5 spacing on a jittered lateral lattice; water fills
     the box outside the bilayer slab.  Lipids are declared first (ids 1..9*nlipids)."""
@@ -295,9 +295,9 @@ def bilayer(cells: Tuple[int, int, int] = (64, 64, 32), nlipids: int = 6000, den
     types = np.concatenate([np.tile(np.array([tmap[s] for s in shape], np.int32), nlipids),
                             np.full(nw, 2, np.int32)])
     bonds = [BondSpec("H", "H", 128.0, 0.5), BondSpec("H", "T", 128.0, 0.5), BondSpec("T", "T", 128.0, 0.5)]
-    bps = [BondPairSpec("T", "T", "T", k3, 0.0)]
+    bps = [BondPairSpec("T", "T", "T", k3, phi0_deg)]
     if with_htt:
-        bps.append(BondPairSpec("H", "T", "T", k3, 0.0))
+        bps.append(BondPairSpec("H", "T", "T", k3, phi0_deg))
     return _assemble("bilayer", cells, (1.0, 1.0, 1.0), density, dt, 0.5, kT, seed, names, am, gm,
                      [PolymerSpec("Lipid", shape, nlipids), PolymerSpec("Water", ("W",), nw)],
                      bonds, bps, types, u, v)
