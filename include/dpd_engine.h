@@ -99,6 +99,16 @@ typedef struct dpd_obs {
     int32_t pad;
 } dpd_obs;
 
+/* One box of a replica batch: its CNT cells, widths, pair tables (ntypes of
+ * the shared parameters) and pair-noise seed. */
+typedef struct dpd_box {
+    int32_t nx, ny, nz;
+    double  wx, wy, wz;
+    const double* a;
+    const double* gamma;
+    uint64_t seed;
+} dpd_box;
+
 /* Creates an engine for one box.  Replaces the CCNTCell statics set in
  * CSimState::CSimState (SimState.cpp:55-110). */
 DPD_API int dpd_engine_create(const dpd_params* params, dpd_engine** out);
@@ -182,6 +192,27 @@ DPD_API int64_t dpd_engine_launch_count(const dpd_engine* e);
 
 DPD_API const char* dpd_engine_last_error(const dpd_engine* e);
 DPD_API void dpd_engine_destroy(dpd_engine* e);
+
+/* ---- Replica batches ---------------------------------------------------
+ * A batch advances many independent boxes (replicas of different size, a_ij
+ * and seed) with the same kernel launches: the boxes are packed into one
+ * cell-sorted state and a box table, so a step costs one set of launches for
+ * all of them.  The reference runs one box per process; each box of a batch
+ * evolves exactly as the same box in its own engine.  dt, lambda, kT,
+ * ntypes, precision and device come from `shared` (its box fields are
+ * ignored).  Bonds are not supported in batches.  All dpd_engine_* calls
+ * apply to a batch; positions in and out are box-local and dpd_engine_cells
+ * reports box-local cell indices. */
+DPD_API int dpd_batch_create(const dpd_params* shared, int32_t nboxes, const dpd_box* boxes, dpd_engine** out);
+
+/* Beads of all boxes at once; box[i] is the box of bead i (ids may repeat
+ * across boxes: each box has its own noise stream). */
+DPD_API int dpd_batch_upload_beads(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id,
+                                   const int32_t* type, const uint8_t* movable, const double* x3,
+                                   const double* unpbc3, const double* v3, const double* f3);
+
+/* Single-bead sums of one box (the virial from its latest sample step). */
+DPD_API int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out);
 
 /* ---- Pair forces without any allocation ---------------------------------
  * This entry point has no counterpart in the reference.  It is for callers

@@ -24,7 +24,6 @@ using namespace dpd;
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPairThreads = 128;
 
 inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
 
@@ -52,6 +51,13 @@ struct dpd_engine {
     int64_t last_step = 0;      // m_SimTime of the state on the device
     int cur = 0;                // which of the double buffers holds the state
     std::string err;
+
+    // boxes: one for a single simulation, one per replica for a batch
+    std::vector<Box> hboxes;
+    std::vector<double> box_a, box_g;   // nboxes * ntypes^2 each
+    Box* d_boxes = nullptr;
+    double* d_box_obs = nullptr;        // nboxes * kObsTerms, filled on demand
+    bool box_obs_valid = false;
 
     // device state
     StepConst* d_K = nullptr;
@@ -114,12 +120,22 @@ struct dpd_engine {
 
     cudaStream_t s() const { return user_stream ? user_stream : stream; }
 
+    // captured multi-step sequences (DPD_GRAPHS=0 disables)
+    struct Graph {
+        int nsteps, parity;
+        std::vector<char> samples;
+        cudaStream_t stream;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    bool graphs_enabled = true;
+
     // pair-kernel launch shape (DPD_TUNE="hitcap=32,bps=8,carveout=50"; 0 = automatic)
     int sms = 148;
     int pair_hitcap = 32;
     int pair_bps = 0;          // resident blocks per SM for the persistent grid
     int pair_carveout = -1;    // preferred shared-memory carveout in percent, -1 = driver default
-    bool pair_attr_set[2][2] = {{false, false}, {false, false}};
+    bool pair_attr_set[2][2] = {{false, false}, {false, false}};   // [fp64][sample]; one box kind per engine
 };
 
 namespace {
@@ -168,8 +184,9 @@ int check_launch(dpd_engine* e, const char* what)
     return DPD_OK;
 }
 
-// Host mirror of StepConst and the pair tables (CCNTCell::SetTimeStepConstants,
-// CNTCell.cpp:180-203; sigma_ij = sqrt(gamma_ij) * sqrt(24 kT / dt), CNTCell.cpp:190,1220).
+// Host mirror of StepConst, the box table and the pair tables
+// (CCNTCell::SetTimeStepConstants, CNTCell.cpp:180-203;
+// sigma_ij = sqrt(gamma_ij) * sqrt(24 kT / dt), CNTCell.cpp:190,1220).
 int push_constants(dpd_engine* e)
 {
     const dpd_params& p = e->params;
@@ -179,22 +196,31 @@ int push_constants(dpd_engine* e)
     K.halfdt2 = 0.5 * p.dt * p.dt;
     K.lamdt = p.lambda * p.dt;
     K.invrootdt = std::sqrt(24.0 * p.kT / p.dt);
-    K.nc[0] = p.nx; K.nc[1] = p.ny; K.nc[2] = p.nz;
-    K.w[0] = p.wx; K.w[1] = p.wy; K.w[2] = p.wz;
-    for (int d = 0; d < 3; ++d) K.L[d] = (double)K.nc[d] * K.w[d];
+    const Box& b0 = e->hboxes[0];
+    for (int d = 0; d < 3; ++d) {
+        K.nc[d] = b0.nc[d];
+        K.w[d] = b0.w[d];
+        K.L[d] = b0.L[d];
+    }
     K.ntypes = e->ntypes;
-    K.seed = p.seed;
+    K.seed = b0.seed;
     const int m = e->ntypes * e->ntypes;
-    std::vector<double> tab(3 * (size_t)m);
-    for (int k = 0; k < m; ++k) {
-        const double a = e->conservative_on ? e->a[k] : 0.0;
-        const double g = e->thermostat_on ? e->gamma[k] : 0.0;
-        tab[k] = a;
-        tab[m + k] = g;
-        tab[2 * m + k] = std::sqrt(g) * K.invrootdt;
+    const size_t nb = e->hboxes.size();
+    std::vector<double> tab(3 * (size_t)m * nb);
+    for (size_t bx = 0; bx < nb; ++bx) {
+        double* t = tab.data() + 3 * (size_t)m * bx;
+        e->hboxes[bx].tab = (int)(3 * (size_t)m * bx);
+        for (int k = 0; k < m; ++k) {
+            const double a = e->conservative_on ? e->box_a[bx * m + k] : 0.0;
+            const double g = e->thermostat_on ? e->box_g[bx * m + k] : 0.0;
+            t[k] = a;
+            t[m + k] = g;
+            t[2 * m + k] = std::sqrt(g) * K.invrootdt;
+        }
     }
     CU(cudaStreamSynchronize(e->s()));   // tables may be in use by queued work
     CU(cudaMemcpy(e->d_K, &K, sizeof K, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_boxes, e->hboxes.data(), nb * sizeof(Box), cudaMemcpyHostToDevice));
     if (e->precision == DPD_PRECISION_FP64) {
         CU(cudaMemcpy(e->d_tab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
@@ -202,6 +228,53 @@ int push_constants(dpd_engine* e)
         CU(cudaMemcpy(e->d_tab, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     return DPD_OK;
+}
+
+// Single-bead sums of every box: one block per box over its contiguous slot
+// range, fixed order (deterministic).  The virial is the per-bead stress of the
+// latest sample step.
+template <typename real>
+__global__ void __launch_bounds__(256) k_box_sums(const Box* __restrict__ boxes, const int* __restrict__ start,
+                                                  int n, const double* __restrict__ x, const double* __restrict__ v,
+                                                  const real* __restrict__ stress, double* __restrict__ out)
+{
+    const Box& B = boxes[blockIdx.x];
+    const int s0 = start[B.cell_base], s1 = start[B.cell_base + B.nc[0] * B.nc[1] * B.nc[2]];
+    double acc[kObsTerms];
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const double xs[3] = {x[s], x[n + s], x[2 * n + s]};
+        const double vs[3] = {v[s], v[n + s], v[2 * n + s]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            acc[d] += vs[d];
+            acc[3 + d] += vs[d] * vs[d];
+            acc[15 + d] += xs[d];
+        }
+        if (stress) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[6 + q] += (double)stress[q * n + s];
+        }
+        acc[18] += xs[1] * vs[2] - xs[2] * vs[1];
+        acc[19] += -xs[0] * vs[2] + xs[2] * vs[0];
+        acc[20] += xs[0] * vs[1] - xs[1] * vs[0];
+    }
+    __shared__ double red[8][kObsTerms];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) {
+        double a = acc[q];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) red[wid][q] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsTerms) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += red[w][threadIdx.x];
+        out[blockIdx.x * kObsTerms + threadIdx.x] = a;
+    }
 }
 
 cudaEvent_t take_event(dpd_engine* e)
@@ -235,6 +308,26 @@ struct Timed {
     }
 };
 
+// Dynamic shared memory and carveout of the pair kernel's variants (outside
+// any stream capture).
+template <typename real>
+int set_pair_attributes(dpd_engine* e)
+{
+    const bool multi = e->hboxes.size() > 1;
+    const int pv = sizeof(real) == 8 ? 1 : 0;
+    for (int sv = 0; sv < 2; ++sv) {
+        if (e->pair_attr_set[pv][sv]) continue;
+        auto kern = multi ? (sv ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
+                          : (sv ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+        CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        if (e->pair_carveout >= 0)
+            CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, e->pair_carveout));
+        e->pair_attr_set[pv][sv] = true;
+    }
+    return DPD_OK;
+}
+
 template <typename real>
 int queue_step(dpd_engine* e, bool sample)
 {
@@ -246,7 +339,7 @@ int queue_step(dpd_engine* e, bool sample)
     int rc;
     {
         Timed t(e, DPD_KERNEL_UPDATE_POS);
-        k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_x[a], e->d_v[a], (const real*)e->d_F,
+        k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a], (const real*)e->d_F,
                                                     e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
                                                     e->d_block_count, e->d_status);
     }
@@ -266,27 +359,23 @@ int queue_step(dpd_engine* e, bool sample)
     {
         Timed t(e, DPD_KERNEL_GATHER);
         k_gather<real><<<nb, kThreads, 0, st>>>(
-            n, e->d_K, e->d_perm, e->d_start, e->d_x[a], e->d_v[a], (const real*)e->d_F, e->d_bid[a],
+            n, e->d_K, e->d_boxes, e->d_perm, e->d_start, e->d_x[a], e->d_v[a], (const real*)e->d_F, e->d_bid[a],
             e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
             e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_slot_of, e->d_pid_of, (V4*)e->d_pos4, (V4*)e->d_vel4);
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
     {
-        auto kern = sample ? k_pair_forces<real, true> : k_pair_forces<real, false>;
-        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap);
-        const int pv = sizeof(real) == 8 ? 1 : 0, sv = sample ? 1 : 0;
-        if (!e->pair_attr_set[pv][sv]) {
-            CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-            if (e->pair_carveout >= 0)
-                CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, e->pair_carveout));
-            e->pair_attr_set[pv][sv] = true;
-        }
+        const bool multi = e->hboxes.size() > 1;
+        auto kern = multi ? (sample ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
+                          : (sample ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+        if ((rc = set_pair_attributes<real>(e))) return rc;
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
         const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
-        kern<<<blocks_for(tiles, tpb), kPairBlock, dyn, st>>>(n, e->d_K, e->d_step, (const real*)e->d_tab,
+        kern<<<blocks_for(tiles, tpb), kPairBlock, dyn, st>>>(n, e->d_K, e->d_boxes, e->d_step, (const real*)e->d_tab,
                                                                e->d_cell[b], e->d_start, (const V4*)e->d_pos4,
                                                                (const V4*)e->d_vel4, (real*)e->d_F,
                                                                (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status);
@@ -298,7 +387,7 @@ int queue_step(dpd_engine* e, bool sample)
     {
         Timed t(e, DPD_KERNEL_UPDATE_MOM);
         auto kern = sample ? k_update_mom<real, true> : k_update_mom<real, false>;
-        kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
+        kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
                                        (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_img[b],
                                        e->d_slot_of, topo, (real*)e->d_stress, e->d_partials, e->d_status);
     }
@@ -336,6 +425,12 @@ void parse_tuning(dpd_engine* e, const char* spec)
     }
 }
 
+void drop_graphs(dpd_engine* e)
+{
+    for (auto& g : e->graphs) cudaGraphExecDestroy(g.exec);
+    e->graphs.clear();
+}
+
 void release_topology(dpd_engine* e)
 {
     int** ip[] = {&e->d_csr_ptr, &e->d_csr_term, &e->d_bond_h, &e->d_bond_t,
@@ -361,27 +456,54 @@ int empty_topology(dpd_engine* e)
 
 extern "C" {
 
-int dpd_engine_create(const dpd_params* p, dpd_engine** out)
+static bool box_ok(int32_t nx, int32_t ny, int32_t nz, double wx, double wy, double wz)
+{
+    return nx >= 3 && ny >= 3 && nz >= 3 && wx >= 1.0 && wy >= 1.0 && wz >= 1.0;
+}
+
+// Shared by the single-box and the batch constructors.
+static int create_impl(const dpd_params* p, int32_t nboxes, const dpd_box* bx, dpd_engine** out)
 {
     dpd_engine* e = nullptr;
     if (!out) return DPD_E_ARG;
     *out = nullptr;
-    if (!p || p->nx < 3 || p->ny < 3 || p->nz < 3 || !(p->wx >= 1.0) || !(p->wy >= 1.0) || !(p->wz >= 1.0) ||
-        !(p->dt > 0.0) || p->lambda < 0.0 || p->kT < 0.0 || p->ntypes < 1 || p->ntypes > kMaxTypes || !p->a ||
-        !p->gamma || (p->precision != DPD_PRECISION_MIXED && p->precision != DPD_PRECISION_FP64))
+    if (!p || !(p->dt > 0.0) || p->lambda < 0.0 || p->kT < 0.0 || p->ntypes < 1 || p->ntypes > kMaxTypes ||
+        (p->precision != DPD_PRECISION_MIXED && p->precision != DPD_PRECISION_FP64) || nboxes < 1 ||
+        nboxes > kMaxBoxes || !bx)
         return DPD_E_ARG;
-    const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+    int64_t ncell = 0;
+    for (int32_t k = 0; k < nboxes; ++k) {
+        if (!box_ok(bx[k].nx, bx[k].ny, bx[k].nz, bx[k].wx, bx[k].wy, bx[k].wz) || !bx[k].a || !bx[k].gamma)
+            return DPD_E_ARG;
+        ncell += (int64_t)bx[k].nx * bx[k].ny * bx[k].nz;
+    }
     if (ncell > (int64_t)1 << 30) return DPD_E_ARG;
     e = new (std::nothrow) dpd_engine();
     if (!e) return DPD_E_NOMEM;
     e->params = *p;
     e->params.a = nullptr;
     e->params.gamma = nullptr;
+    e->params.nx = bx[0].nx; e->params.ny = bx[0].ny; e->params.nz = bx[0].nz;
+    e->params.wx = bx[0].wx; e->params.wy = bx[0].wy; e->params.wz = bx[0].wz;
+    e->params.seed = bx[0].seed;
     e->precision = p->precision;
     e->ntypes = p->ntypes;
     const int m = p->ntypes * p->ntypes;
-    e->a.assign(p->a, p->a + m);
-    e->gamma.assign(p->gamma, p->gamma + m);
+    int64_t base = 0;
+    for (int32_t k = 0; k < nboxes; ++k) {
+        Box b{};
+        b.nc[0] = bx[k].nx; b.nc[1] = bx[k].ny; b.nc[2] = bx[k].nz;
+        b.w[0] = bx[k].wx; b.w[1] = bx[k].wy; b.w[2] = bx[k].wz;
+        for (int d = 0; d < 3; ++d) b.L[d] = (double)b.nc[d] * b.w[d];
+        b.cell_base = (int)base;
+        b.seed = bx[k].seed;
+        base += (int64_t)b.nc[0] * b.nc[1] * b.nc[2];
+        e->hboxes.push_back(b);
+        e->box_a.insert(e->box_a.end(), bx[k].a, bx[k].a + m);
+        e->box_g.insert(e->box_g.end(), bx[k].gamma, bx[k].gamma + m);
+    }
+    e->a.assign(bx[0].a, bx[0].a + m);
+    e->gamma.assign(bx[0].gamma, bx[0].gamma + m);
     e->ncell = ncell;
     e->nchunk = (int)((ncell + kScanChunk - 1) / kScanChunk);
     int rc = DPD_OK;
@@ -395,12 +517,17 @@ int dpd_engine_create(const dpd_params* p, dpd_engine** out)
         }
         cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);
         if (const char* tune = getenv("DPD_TUNE")) parse_tuning(e, tune);
+        if (const char* g = getenv("DPD_GRAPHS")) e->graphs_enabled = atoi(g) != 0;
         if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
             rc = fail(e, DPD_E_CUDA, "cudaStreamCreate failed");
             break;
         }
         if ((rc = dalloc(e, &e->d_K, 1))) break;
-        if ((rc = dalloc(e, (char**)&e->d_tab, 3 * (size_t)kMaxTypes * kMaxTypes * sizeof(double)))) break;
+        if ((rc = dalloc(e, &e->d_boxes, (size_t)nboxes))) break;
+        if ((rc = dalloc(e, &e->d_box_obs, (size_t)nboxes * kObsTerms))) break;
+        // a single box may later grow its type table (AddDPDBeadType); a batch keeps its types
+        const size_t tab_m = nboxes == 1 ? (size_t)kMaxTypes * kMaxTypes : (size_t)m;
+        if ((rc = dalloc(e, (char**)&e->d_tab, 3 * tab_m * nboxes * sizeof(double)))) break;
         if ((rc = dalloc(e, &e->d_step, 1))) break;
         if ((rc = dalloc(e, &e->d_status, 1))) break;
         if ((rc = dalloc(e, &e->d_count, (size_t)ncell))) break;
@@ -432,12 +559,27 @@ int dpd_engine_create(const dpd_params* p, dpd_engine** out)
     return DPD_OK;
 }
 
+int dpd_engine_create(const dpd_params* p, dpd_engine** out)
+{
+    if (!out) return DPD_E_ARG;
+    *out = nullptr;
+    if (!p || !p->a || !p->gamma) return DPD_E_ARG;
+    const dpd_box b{p->nx, p->ny, p->nz, p->wx, p->wy, p->wz, p->a, p->gamma, p->seed};
+    return create_impl(p, 1, &b, out);
+}
+
+int dpd_batch_create(const dpd_params* shared, int32_t nboxes, const dpd_box* boxes, dpd_engine** out)
+{
+    return create_impl(shared, nboxes, boxes, out);
+}
+
 void dpd_engine_destroy(dpd_engine* e)
 {
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->user_stream) cudaStreamSynchronize(e->user_stream);
+    drop_graphs(e);
     for (auto& r : e->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
     for (void* p : e->allocations) cudaFree(p);
@@ -465,6 +607,7 @@ int dpd_engine_set_stream(dpd_engine* e, void* cuda_stream)
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));   // finish work queued on the old stream
     e->user_stream = static_cast<cudaStream_t>(cuda_stream);
+    drop_graphs(e);
     return DPD_OK;
 }
 
@@ -505,19 +648,17 @@ int dpd_engine_profile_read(dpd_engine* e, double* total_ms, int64_t* launches)
 
 int64_t dpd_engine_launch_count(const dpd_engine* e) { return e ? e->launches : -1; }
 
-int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
-                            const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
-                            const double* f3)
+static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                       const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
+                       const double* f3)
 {
     if (!e) return DPD_E_ARG;
+    drop_graphs(e);
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
+    if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
-    const dpd_params& p = e->params;
-    const double L[3] = {p.nx * p.wx, p.ny * p.wy, p.nz * p.wz};
-    const double w[3] = {p.wx, p.wy, p.wz};
-    const int nc[3] = {p.nx, p.ny, p.nz};
-    // CSimBox::AssignBeadstoCells (SimBox.cpp:715-762): ix = (long)(x/w)
+    // CSimBox::AssignBeadstoCells (SimBox.cpp:715-762): ix = (long)(x/w), box-local coordinates
     std::vector<int> cell(n);
     std::vector<double> off;
     bool any_off = false;
@@ -525,6 +666,12 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
     for (int64_t b = 0; b < n; ++b) {
         if (type[b] < 0 || type[b] >= e->ntypes) return fail(e, DPD_E_ARG, "bead type out of range");
         if (id[b] < 1 || id[b] > 0x7fffffff) return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
+        const int bxi = box ? box[b] : 0;
+        if (bxi < 0 || bxi >= (int)e->hboxes.size()) return fail(e, DPD_E_ARG, "bead box index out of range");
+        const Box& B = e->hboxes[bxi];
+        const double* L = B.L;
+        const double* w = B.w;
+        const int* nc = B.nc;
         int64_t ci[3];
         for (int d = 0; d < 3; ++d) {
             const double xv = x3[3 * b + d];
@@ -536,7 +683,7 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
                 return fail(e, DPD_E_BOX, msg);
             }
         }
-        cell[b] = (int)(ci[0] + (int64_t)nc[0] * (ci[1] + (int64_t)nc[1] * ci[2]));
+        cell[b] = (int)(B.cell_base + ci[0] + (int64_t)nc[0] * (ci[1] + (int64_t)nc[1] * ci[2]));
         int ii[3] = {0, 0, 0};
         if (unpbc3) {
             for (int d = 0; d < 3; ++d) {
@@ -552,11 +699,13 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
     }
     if (any_off) {
         off.assign(3 * (size_t)n, 0.0);
-        for (int64_t b = 0; b < n; ++b)
+        for (int64_t b = 0; b < n; ++b) {
+            const double* L = e->hboxes[box ? box[b] : 0].L;
             for (int d = 0; d < 3; ++d) {
                 const double du = unpbc3[3 * b + d] - x3[3 * b + d];
                 off[(size_t)d * n + b] = du - (double)img_get(img[b], d) * L[d];
             }
+        }
     }
     // slot order: by cell, then by upload index (stable counting sort)
     std::vector<int64_t> start(e->ncell + 1, 0);
@@ -621,7 +770,7 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
             hf[(size_t)d * n + s] = f3 ? f3[3 * b + d] : 0.0;
         }
         hbid[s] = b;
-        htf[s] = type[b] | ((movable && !movable[b]) ? kFlagFrozen : 0);
+        htf[s] = type[b] | ((box ? box[b] : 0) << 8) | ((movable && !movable[b]) ? kFlagFrozen : 0);
         hcell[s] = cell[b];
         himg[s] = img[b];
     }
@@ -652,7 +801,23 @@ int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const i
     e->stepped = false;
     e->sampled = false;
     e->obs_valid = false;
+    e->box_obs_valid = false;
     return DPD_OK;
+}
+
+int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
+                            const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
+                            const double* f3)
+{
+    return upload_impl(e, n, nullptr, id, type, movable, x3, unpbc3, v3, f3);
+}
+
+int dpd_batch_upload_beads(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                           const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
+                           const double* f3)
+{
+    if (!box) return fail(e, DPD_E_ARG, "null box array");
+    return upload_impl(e, n, box, id, type, movable, x3, unpbc3, v3, f3);
 }
 
 int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_head_id, const int64_t* bond_tail_id,
@@ -661,6 +826,9 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
 {
     if (!e) return DPD_E_ARG;
     if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads before the topology");
+    if (e->hboxes.size() > 1 && (nb > 0 || na > 0))
+        return fail(e, DPD_E_STATE, "bonds are not supported in a replica batch");
+    drop_graphs(e);
     if (nb < 0 || na < 0 || (nb && (!bond_head_id || !bond_tail_id || !k2 || !l0)) ||
         (na && (!first_bond || !second_bond || !k3 || !phi0)))
         return fail(e, DPD_E_ARG, "bad topology arrays");
@@ -770,9 +938,26 @@ int dpd_engine_set_pair_params(dpd_engine* e, int32_t ntypes, const double* a, c
         for (int j = 0; j < ntypes; ++j)
             if (a[i * ntypes + j] != a[j * ntypes + i] || gamma[i * ntypes + j] != gamma[j * ntypes + i])
                 return fail(e, DPD_E_ARG, "pair tables must be symmetric");
+    if (ntypes != e->ntypes && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch keeps its bead types");
+    if (ntypes != e->ntypes) {
+        // the pair kernel's shared-memory size and the captured graphs depend on ntypes
+        memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
+        CU(cudaSetDevice(e->device));
+        CU(cudaStreamSynchronize(e->s()));
+        drop_graphs(e);
+    }
     e->ntypes = ntypes;
     e->a.assign(a, a + m);
     e->gamma.assign(gamma, gamma + m);
+    if (e->hboxes.size() == 1) {
+        e->box_a = e->a;
+        e->box_g = e->gamma;
+    } else {
+        for (size_t k = 0; k < e->hboxes.size(); ++k) {
+            std::copy(a, a + m, e->box_a.begin() + k * m);
+            std::copy(gamma, gamma + m, e->box_g.begin() + k * m);
+        }
+    }
     CU(cudaSetDevice(e->device));
     return push_constants(e);
 }
@@ -814,20 +999,71 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     CU(cudaStreamSynchronize(e->s()));
     *e->h_step = first_step;
     CU(cudaMemcpyAsync(e->d_step, e->h_step, sizeof(int64_t), cudaMemcpyHostToDevice, e->s()));
+    std::vector<char> samples(nsteps);
     for (int32_t k = 0; k < nsteps; ++k) {
         const int64_t t = first_step + k;
         // ISimState::TimeToSample (ISimState.cpp:468-471): m_SimTime % SamplePeriod == 0
-        const bool sample = e->sample_period > 0 ? (t % e->sample_period == 0) : (k == nsteps - 1);
-        const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, sample)
-                                                             : queue_step<float>(e, sample);
-        if (rc) return rc;
-        if (sample) {
-            e->sampled = true;
-            e->last_sample_step = t;
-        }
+        samples[k] = e->sample_period > 0 ? (t % e->sample_period == 0) : (k == nsteps - 1);
     }
+    auto queue_all = [&](void) -> int {
+        for (int32_t k = 0; k < nsteps; ++k) {
+            const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, samples[k])
+                                                                 : queue_step<float>(e, samples[k]);
+            if (rc) return rc;
+        }
+        return DPD_OK;
+    };
+    const int parity = e->cur;
+    if (e->graphs_enabled && !e->profiling && nsteps >= 2) {
+        // one captured graph per (step count, buffer parity, sample pattern, stream)
+        dpd_engine::Graph* g = nullptr;
+        for (auto& cand : e->graphs)
+            if (cand.nsteps == nsteps && cand.parity == parity && cand.samples == samples && cand.stream == e->s())
+                g = &cand;
+        if (!g) {
+            if (e->graphs.size() >= 16) drop_graphs(e);
+            // kernel attributes are set outside the capture
+            const int rc0 = (e->precision == DPD_PRECISION_FP64) ? set_pair_attributes<double>(e)
+                                                                  : set_pair_attributes<float>(e);
+            if (rc0) return rc0;
+            cudaGraph_t graph = nullptr;
+            CU(cudaStreamBeginCapture(e->s(), cudaStreamCaptureModeThreadLocal));
+            const int64_t launches0 = e->launches;
+            const int rc = queue_all();
+            cudaError_t ce = cudaStreamEndCapture(e->s(), &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                e->cur = parity;
+                return rc;
+            }
+            if (ce != cudaSuccess) return fail(e, DPD_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            cudaGraphExec_t exec = nullptr;
+            ce = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) return fail(e, DPD_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            e->graphs.push_back({nsteps, parity, samples, e->s(), exec});
+            g = &e->graphs.back();
+            e->launches = launches0;   // counted per replay below
+            e->cur = parity;
+        }
+        CU(cudaGraphLaunch(g->exec, e->s()));
+        int64_t nsample = 0;
+        for (char c : samples) nsample += c;
+        e->launches += 6 * (int64_t)nsteps + nsample;   // six kernels a step, plus the sum on sample steps
+        e->cur = (nsteps % 2) ? 1 - parity : parity;
+    } else {
+        const int rc = queue_all();
+        if (rc) return rc;
+    }
+    for (int32_t k = nsteps - 1; k >= 0; --k)
+        if (samples[k]) {
+            e->sampled = true;
+            e->last_sample_step = first_step + k;
+            break;
+        }
     e->stepped = true;
     e->obs_valid = false;
+    e->box_obs_valid = false;
     e->obs_has_virial = true;
     e->last_step = first_step + nsteps - 1;
     return DPD_OK;
@@ -854,12 +1090,12 @@ static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, doubl
     const int c = e->cur;
     if (e->precision == DPD_PRECISION_FP64)
         k_download<double><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->d_off,
+            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->d_off,
             e->sampled ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     else
         k_download<float><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_K, e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->d_off,
+            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->d_off,
             e->sampled ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     int rc = check_launch(e, "k_download");
@@ -920,6 +1156,59 @@ int dpd_engine_observables(dpd_engine* e, dpd_obs* out)
     const double V = (p.nx * p.wx) * (p.ny * p.wy) * (p.nz * p.wz);
     const double v2 = out->sum_v2[0] + out->sum_v2[1] + out->sum_v2[2];
     out->kT = v2 / (3.0 * (double)e->n);
+    out->pressure = 0.3333333333 * (1.0 / V) * (v2 + out->virial[0] + out->virial[4] + out->virial[8]);
+    return DPD_OK;
+}
+
+int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out)
+{
+    if (!e) return DPD_E_ARG;
+    if (!out) return fail(e, DPD_E_ARG, "null output");
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    if (box < 0 || box >= (int32_t)e->hboxes.size()) return fail(e, DPD_E_ARG, "box index out of range");
+    CU(cudaSetDevice(e->device));
+    const int nb = (int)e->hboxes.size();
+    if (!e->box_obs_valid) {
+        const int c = e->cur;
+        if (e->precision == DPD_PRECISION_FP64)
+            k_box_sums<double><<<nb, 256, 0, e->s()>>>(e->d_boxes, e->d_start, (int)e->n, e->d_x[c], e->d_v[c],
+                                                       e->sampled ? (const double*)e->d_stress : nullptr,
+                                                       e->d_box_obs);
+        else
+            k_box_sums<float><<<nb, 256, 0, e->s()>>>(e->d_boxes, e->d_start, (int)e->n, e->d_x[c], e->d_v[c],
+                                                      e->sampled ? (const float*)e->d_stress : nullptr,
+                                                      e->d_box_obs);
+        int rc = check_launch(e, "k_box_sums");
+        if (rc) return rc;
+        e->box_obs_valid = true;
+    }
+    double h[kObsTerms];
+    CU(cudaMemcpyAsync(h, e->d_box_obs + (size_t)box * kObsTerms, sizeof h, cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    int64_t nbox = 0;
+    {
+        int se[2];
+        const Box& B = e->hboxes[box];
+        CU(cudaMemcpy(&se[0], e->d_start + B.cell_base, sizeof(int), cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(&se[1], e->d_start + B.cell_base + B.nc[0] * B.nc[1] * B.nc[2], sizeof(int),
+                      cudaMemcpyDeviceToHost));
+        nbox = se[1] - se[0];
+    }
+    memset(out, 0, sizeof *out);
+    out->step = e->sampled ? e->last_sample_step : (e->stepped ? e->last_step : 0);
+    out->n = nbox;
+    for (int d = 0; d < 3; ++d) {
+        out->sum_v[d] = h[d];
+        out->sum_v2[d] = h[3 + d];
+        out->sum_x[d] = h[15 + d];
+        out->ang_mom[d] = h[18 + d];
+    }
+    out->has_virial = e->sampled ? 1 : 0;
+    for (int q = 0; q < 9; ++q) out->virial[q] = h[6 + q];
+    const Box& B = e->hboxes[box];
+    const double V = B.L[0] * B.L[1] * B.L[2];
+    const double v2 = out->sum_v2[0] + out->sum_v2[1] + out->sum_v2[2];
+    out->kT = nbox > 0 ? v2 / (3.0 * (double)nbox) : 0.0;
     out->pressure = 0.3333333333 * (1.0 / V) * (v2 + out->virial[0] + out->virial[4] + out->virial[8]);
     return DPD_OK;
 }

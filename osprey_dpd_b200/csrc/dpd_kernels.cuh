@@ -45,8 +45,9 @@ __host__ __device__ __forceinline__ int img_get(uint32_t w, int d)
     return (int)((w >> (10 * d)) & 1023u) - 512;
 }
 
-// Time-step and box constants; lives in device memory so that a parameter
-// change needs no relaunch configuration (CCNTCell statics, CNTCell.cpp:42-75).
+// Time-step constants and the first box; lives in device memory so that a
+// parameter change needs no relaunch configuration (CCNTCell statics,
+// CNTCell.cpp:42-75).
 struct StepConst {
     double dt, halfdt, halfdt2, lamdt, invrootdt;
     double L[3], w[3];
@@ -55,13 +56,30 @@ struct StepConst {
     uint64_t seed;
 };
 
-// Bead flags word: type in bits 0..15, frozen (never moves) in bit 16,
-// has bond or bond-pair terms in bit 17.
-__device__ __forceinline__ int flag_type(int tf) { return tf & 0xFFFF; }
-__device__ __forceinline__ bool flag_frozen(int tf) { return (tf >> 16) & 1; }
-__device__ __forceinline__ bool flag_bonded(int tf) { return (tf >> 17) & 1; }
-constexpr int kFlagFrozen = 1 << 16;
-constexpr int kFlagBonded = 1 << 17;
+// One simulation box (CCNTCell::SetSimBoxLengths, CNTCell.cpp:143-158).  An
+// engine holds a packed table of them: one for a single simulation, one per
+// replica for a batch.  Global cell index = cell_base + nx*(ny*iz+iy)+ix.
+struct Box {
+    int nc[3];
+    int cell_base;
+    double w[3];
+    double L[3];
+    uint64_t seed;     // pair-noise seed of this box
+    int tab;           // offset of this box's pair tables (3 * ntypes^2 reals)
+    int pad;
+};
+
+// Bead flags word: type in bits 0..7, box in bits 8..23, frozen (never
+// moves) in bit 24, has bond or bond-pair terms in bit 25.  The force
+// kernel's position shadow carries bits 0..23.
+__host__ __device__ __forceinline__ int flag_type(int tf) { return tf & 0xFF; }
+__host__ __device__ __forceinline__ int flag_box(int tf) { return (tf >> 8) & 0xFFFF; }
+__device__ __forceinline__ bool flag_frozen(int tf) { return (tf >> 24) & 1; }
+__device__ __forceinline__ bool flag_bonded(int tf) { return (tf >> 25) & 1; }
+constexpr int kFlagFrozen = 1 << 24;
+constexpr int kFlagBonded = 1 << 25;
+constexpr int kShadowMask = 0x00FFFFFF;
+constexpr int kMaxBoxes = 1 << 16;
 
 template <typename real> struct Vec4;
 template <> struct Vec4<float> { typedef float4 type; };
@@ -81,7 +99,8 @@ __device__ __forceinline__ int real_bits(double v) { return (int)__double_as_lon
 // both cells lie on the box boundary.  Frozen beads keep their cell.
 template <typename real>
 __global__ void __launch_bounds__(256, 6) k_update_pos(
-    int n, const StepConst* __restrict__ K, double* __restrict__ x, const double* __restrict__ v,
+    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, double* __restrict__ x,
+    const double* __restrict__ v,
     const real* __restrict__ F, const int* __restrict__ tf, uint32_t* __restrict__ img,
     int* __restrict__ cell, int* __restrict__ rank, int* __restrict__ count,
     int* __restrict__ block_count, unsigned* __restrict__ status)
@@ -105,8 +124,10 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
         cnew = c;
         if (!flag_frozen(tfl)) {
             const double dt = K->dt, h2 = K->halfdt2;
-            const int nx = K->nc[0], ny = K->nc[1], nz = K->nc[2];
-            int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
+            const Box& B = boxes[flag_box(tfl)];
+            const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
+            const int cl = c - B.cell_base;
+            int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
             const bool ext = ci[0] == 0 || ci[0] == nx - 1 || ci[1] == 0 || ci[1] == ny - 1 ||
                              ci[2] == 0 || ci[2] == nz - 1;
             double xn[3];
@@ -116,8 +137,8 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
                 // x += dt*v + dt^2/2*F with the reference's rounding (no fused multiply-add)
                 const double dx = __dadd_rn(__dmul_rn(dt, v0[d]), __dmul_rn(h2, f0[d]));
                 xn[d] = __dadd_rn(x0[d], dx);
-                const double BL = __dmul_rn((double)ci[d], K->w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
-                const double TR = __dadd_rn(BL, K->w[d]);
+                const double BL = __dmul_rn((double)ci[d], B.w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
+                const double TR = __dadd_rn(BL, B.w[d]);
                 mv[d] = (xn[d] > TR) ? 1 : ((xn[d] < BL) ? -1 : 0);
             }
             uint32_t im = im0;
@@ -125,27 +146,27 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
                 int nci[3];
                 for (int d = 0; d < 3; ++d) {
                     nci[d] = ci[d] + mv[d];
-                    if (nci[d] < 0) nci[d] += K->nc[d];
-                    else if (nci[d] >= K->nc[d]) nci[d] -= K->nc[d];
+                    if (nci[d] < 0) nci[d] += B.nc[d];
+                    else if (nci[d] >= B.nc[d]) nci[d] -= B.nc[d];
                 }
                 const bool next = nci[0] == 0 || nci[0] == nx - 1 || nci[1] == 0 || nci[1] == ny - 1 ||
                                   nci[2] == 0 || nci[2] == nz - 1;
                 if (ext && next) {
                     int ii[3] = {img_get(im, 0), img_get(im, 1), img_get(im, 2)};
                     for (int d = 0; d < 3; ++d) {
-                        if (mv[d] > 0 && xn[d] > K->L[d]) { xn[d] -= K->L[d]; ++ii[d]; }
-                        else if (mv[d] < 0 && xn[d] < 0.0) { xn[d] += K->L[d]; --ii[d]; }
+                        if (mv[d] > 0 && xn[d] > B.L[d]) { xn[d] -= B.L[d]; ++ii[d]; }
+                        else if (mv[d] < 0 && xn[d] < 0.0) { xn[d] += B.L[d]; --ii[d]; }
                         if (ii[d] < -511 || ii[d] > 511) bad |= 0x4u;
                     }
                     im = img_pack(ii[0], ii[1], ii[2]);
                 }
-                cnew = nci[0] + nx * (nci[1] + ny * nci[2]);
+                cnew = B.cell_base + nci[0] + nx * (nci[1] + ny * nci[2]);
             }
             // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650)
-            const long long ax = (long long)(xn[0] / K->w[0]);
-            const long long ay = (long long)(xn[1] / K->w[1]);
-            const long long az = (long long)(xn[2] / K->w[2]);
-            if ((long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
+            const long long ax = (long long)(xn[0] / B.w[0]);
+            const long long ay = (long long)(xn[1] / B.w[1]);
+            const long long az = (long long)(xn[2] / B.w[2]);
+            if (B.cell_base + (long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 if (!isfinite(xn[d])) bad |= 0x2u;
@@ -249,7 +270,8 @@ static __global__ void __launch_bounds__(256) k_permute(
 // with the bead type and the noise id in the fourth component.
 template <typename real>
 __global__ void __launch_bounds__(256, 6) k_gather(
-    int n, const StepConst* __restrict__ K, const int* __restrict__ perm, const int* __restrict__ start,
+    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int* __restrict__ perm,
+    const int* __restrict__ start,
     const double* __restrict__ x_in, const double* __restrict__ v_in, const real* __restrict__ F_in,
     const int* __restrict__ bid_in, const int* __restrict__ tf_in, const uint32_t* __restrict__ img_in,
     const int* __restrict__ cell_in, double* __restrict__ x_out, double* __restrict__ v_out,
@@ -279,8 +301,10 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     int k = 0;
     for (int e = beg; e < end; ++e) k += (perm[e] < s);
     const int o = beg + k;
-    const int nx = K->nc[0], ny = K->nc[1];
-    const int ci[3] = {c % nx, (c / nx) % ny, c / (nx * ny)};
+    const Box& B = boxes[flag_box(tfl)];
+    const int nx = B.nc[0], ny = B.nc[1];
+    const int cl = c - B.cell_base;
+    const int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
     const bool frozen = flag_frozen(tfl);
     real rel[3], vt[3];
 #pragma unroll
@@ -291,7 +315,7 @@ __global__ void __launch_bounds__(256, 6) k_gather(
         x_out[q * n + o] = xv;
         v_out[q * n + o] = vv;
         Fold_out[q * n + o] = fv;
-        rel[q] = (real)__dadd_rn(xv, -__dmul_rn((double)ci[q], K->w[q]));
+        rel[q] = (real)__dadd_rn(xv, -__dmul_rn((double)ci[q], B.w[q]));
         vt[q] = frozen ? (real)vv : (real)__dadd_rn(vv, __dmul_rn(K->lamdt, (double)fv));
     }
     bid_out[o] = b;
@@ -301,7 +325,7 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     slot_of[b] = o;
     typedef typename Vec4<real>::type V4;
     V4 p, w;
-    p.x = rel[0]; p.y = rel[1]; p.z = rel[2]; p.w = as_real_bits(flag_type(tfl), real(0));
+    p.x = rel[0]; p.y = rel[1]; p.z = rel[2]; p.w = as_real_bits(tfl & kShadowMask, real(0));
     w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid_of[b], real(0));
     pos4[o] = p;
     vel4[o] = w;
@@ -361,7 +385,7 @@ __global__ void __launch_bounds__(128) k_pair_forces_ref(
     const int c = cell[i];
     const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
     const typename Vec4<real>::type pi = pos4[i], vi = vel4[i];
-    const int ti = real_bits(pi.w) & 0xFFFF;
+    const int ti = real_bits(pi.w) & 0xFF;
     const uint32_t idi = (uint32_t)real_bits(vi.w);
     real fx = 0, fy = 0, fz = 0;
     real s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -389,7 +413,7 @@ __global__ void __launch_bounds__(128) k_pair_forces_ref(
                         const real r = sqrt(r2);
                         const real inv = real(1) / r;
                         const real wr = real(1) - r;
-                        const int tj = real_bits(pj.w) & 0xFFFF;
+                        const int tj = real_bits(pj.w) & 0xFF;
                         const int tt = ti * nt + tj;
                         const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
                         const uint32_t idj = (uint32_t)real_bits(vj.w);
@@ -439,14 +463,14 @@ struct Topology {
 
 enum TermCode { kBondHead = 0, kBondTail = 1, kAngle0 = 2, kAngle1 = 3, kAngle2 = 4 };
 
-__device__ __forceinline__ void unwrapped(const StepConst* __restrict__ K, const double* __restrict__ x,
+__device__ __forceinline__ void unwrapped(const Box& B, const double* __restrict__ x,
                                           const uint32_t* __restrict__ img, const double* __restrict__ off,
                                           int n, int nb_total, int slot, int b, double u[3])
 {
     const uint32_t im = img[slot];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        u[d] = x[d * n + slot] + (double)img_get(im, d) * K->L[d];
+        u[d] = x[d * n + slot] + (double)img_get(im, d) * B.L[d];
         if (off) u[d] += off[d * nb_total + b];
     }
 }
@@ -459,7 +483,7 @@ __device__ __forceinline__ void unwrapped(const StepConst* __restrict__ K, const
 // single-bead sums are reduced per block.
 template <typename real, bool SAMPLE>
 __global__ void __launch_bounds__(256, 4) k_update_mom(
-    int n, const StepConst* __restrict__ K, int64_t* __restrict__ step_ptr,
+    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, int64_t* __restrict__ step_ptr,
     const double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
     const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
     const uint32_t* __restrict__ img, const int* __restrict__ slot_of, Topology topo,
@@ -484,6 +508,7 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
         double bf[3] = {0.0, 0.0, 0.0};
         double bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         const bool bonded = flag_bonded(tfl);
+        const Box& B = boxes[flag_box(tfl)];
         const int t0 = bonded ? topo.csr_ptr[b] : 0, t1 = bonded ? topo.csr_ptr[b + 1] : 0;
         for (int t = t0; t < t1; ++t) {
             const int term = topo.csr_term[t];
@@ -492,8 +517,8 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 // CBond::AddForce, Bond.cpp:123-160 (serial build: unPBC coordinates)
                 const int h = topo.bond_h[idx], tl = topo.bond_t[idx];
                 double uh[3], ut[3];
-                unwrapped(K, x, img, topo.off, n, n, slot_of[h], h, uh);
-                unwrapped(K, x, img, topo.off, n, n, slot_of[tl], tl, ut);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[h], h, uh);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[tl], tl, ut);
                 const double bx = uh[0] - ut[0], by = uh[1] - ut[1], bz = uh[2] - ut[2];
                 const double len = sqrt(bx * bx + by * by + bz * bz);
                 const double k2 = topo.bond_k2[idx], l0 = topo.bond_l0[idx];
@@ -515,10 +540,10 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 double u1h[3], u1t[3], u2h[3], u2t[3];
                 const int a1h = topo.ang_b1h[idx], a1t = topo.ang_b1t[idx];
                 const int a2h = topo.ang_b2h[idx], a2t = topo.ang_b2t[idx];
-                unwrapped(K, x, img, topo.off, n, n, slot_of[a1h], a1h, u1h);
-                unwrapped(K, x, img, topo.off, n, n, slot_of[a1t], a1t, u1t);
-                unwrapped(K, x, img, topo.off, n, n, slot_of[a2h], a2h, u2h);
-                unwrapped(K, x, img, topo.off, n, n, slot_of[a2t], a2t, u2t);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[a1h], a1h, u1h);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[a1t], a1t, u1t);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[a2h], a2h, u2h);
+                unwrapped(B, x, img, topo.off, n, n, slot_of[a2t], a2t, u2t);
                 double b1[3], b2[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -660,7 +685,8 @@ static __global__ void __launch_bounds__(256) k_kinetic_partials(int n, const do
 // Slot order -> upload order, FP64, xyz interleaved; unPBC = x + img*L + off.
 template <typename real>
 __global__ void __launch_bounds__(256) k_download(
-    int n, const StepConst* __restrict__ K, const int* __restrict__ slot_of, const double* __restrict__ x,
+    int n, const Box* __restrict__ boxes, const int* __restrict__ tf, const int* __restrict__ slot_of,
+    const double* __restrict__ x,
     const double* __restrict__ v, const real* __restrict__ F, const uint32_t* __restrict__ img,
     const double* __restrict__ off, const real* __restrict__ stress, const int* __restrict__ cell,
     double* __restrict__ ox, double* __restrict__ ou, double* __restrict__ ov, double* __restrict__ of,
@@ -670,11 +696,12 @@ __global__ void __launch_bounds__(256) k_download(
     if (b >= n) return;
     const int s = slot_of[b];
     const uint32_t im = img[s];
+    const Box& B = boxes[flag_box(tf[s])];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const double xv = x[d * n + s];
         if (ox) ox[3 * b + d] = xv;
-        if (ou) ou[3 * b + d] = xv + (double)img_get(im, d) * K->L[d] + (off ? off[d * n + b] : 0.0);
+        if (ou) ou[3 * b + d] = xv + (double)img_get(im, d) * B.L[d] + (off ? off[d * n + b] : 0.0);
         if (ov) ov[3 * b + d] = v[d * n + s];
         if (of) of[3 * b + d] = (double)F[d * n + s];
     }
@@ -682,7 +709,7 @@ __global__ void __launch_bounds__(256) k_download(
 #pragma unroll
         for (int q = 0; q < 9; ++q) ost[9 * b + q] = stress ? (double)stress[q * n + s] : 0.0;
     }
-    if (ocell) ocell[b] = cell[s];
+    if (ocell) ocell[b] = cell[s] - B.cell_base;
 }
 
 }  // namespace dpd

@@ -45,9 +45,9 @@ __host__ __device__ constexpr size_t pair_tables_bytes(int nt)
     return ((3 * sizeof(real) * (size_t)nt * nt + 15) / 16) * 16;
 }
 template <typename real>
-__host__ __device__ constexpr size_t pair_smem_bytes(int nt, int hitcap)
+__host__ __device__ constexpr size_t pair_smem_bytes(int nt, int hitcap, bool multi)
 {
-    return pair_tables_bytes<real>(nt) + sizeof(uint32_t) * hitcap * kPairBlock;
+    return (multi ? 0 : pair_tables_bytes<real>(nt)) + sizeof(uint32_t) * hitcap * kPairBlock;
 }
 
 // Hit entry: candidate slot in bits 0..25, cell offsets + 1 (x, y, z) in
@@ -69,7 +69,7 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
 {
     typedef typename Vec4<real>::type V4;
     const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    const int ti = (real_bits(pi.w) & 0xFFFF) * nt;
+    const int ti = (real_bits(pi.w) & 0xFF) * nt;
     const uint32_t idi = (uint32_t)real_bits(vi.w);
     const int m2 = nt * nt;
     for (int k = 0; k < trip; ++k) {
@@ -84,7 +84,7 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
             const real r2 = dx * dx + dy * dy + dz * dz;
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
-            const int tt = ti + (real_bits(pj.w) & 0xFFFF);
+            const int tt = ti + (real_bits(pj.w) & 0xFF);
             const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
             const uint32_t idj = (uint32_t)real_bits(vj.w);
             uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
@@ -111,9 +111,12 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
 // Persistent blocks: block b evaluates the contiguous tiles [b*tpb, (b+1)*tpb)
 // of kPairBlock slots, so consecutive tiles of one block walk neighbouring
 // cells and reuse the neighbour rows already in its SM's L1.
-template <typename real, bool VIRIAL>
+// MULTI: beads of many boxes (a replica batch); each bead takes its box, pair
+// tables and noise key from the packed box table, tables are read through the
+// read-only cache.  Otherwise one box whose tables are staged in shared memory.
+template <typename real, bool VIRIAL, bool MULTI>
 __global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces(
-    int n, const StepConst* __restrict__ K, const int64_t* __restrict__ step_ptr,
+    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
@@ -122,15 +125,11 @@ __global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces(
     typedef typename Vec4<real>::type V4;
     extern __shared__ __align__(16) unsigned char pair_dyn[];
     const int nt = K->ntypes;
-    real* T = reinterpret_cast<real*>(pair_dyn);      // a, gamma, sigma: 3 * ntypes^2
-    uint32_t* list = reinterpret_cast<uint32_t*>(pair_dyn + pair_tables_bytes<real>(nt)) + threadIdx.x;
-    for (int k = threadIdx.x; k < 3 * nt * nt; k += kPairBlock) T[k] = tab[k];
-    uint32_t keys[10];
-    {
-        uint32_t k = philox_step_key(K->seed, *step_ptr);
-#pragma unroll
-        for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
-    }
+    real* Tsh = reinterpret_cast<real*>(pair_dyn);    // a, gamma, sigma: 3 * ntypes^2
+    uint32_t* list = reinterpret_cast<uint32_t*>(pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt))) + threadIdx.x;
+    if (!MULTI)
+        for (int k = threadIdx.x; k < 3 * nt * nt; k += kPairBlock) Tsh[k] = tab[k];
+    const int64_t step = *step_ptr;
     __syncthreads();   // tables
     const int tile0 = blockIdx.x * tiles_per_block;
     for (int tile = tile0; tile < tile0 + tiles_per_block; ++tile) {
@@ -139,18 +138,28 @@ __global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces(
     const bool live = i < n;
     V4 pi, vi;
     int cx = 0, cy = 0, cz = 0;
-    const int nx = K->nc[0], ny = K->nc[1], nz = K->nc[2];
     if (live) {
         pi = pos4[i];
         vi = vel4[i];
-        const int c = cell[i];
-        cx = c % nx;
-        cy = (c / nx) % ny;
-        cz = c / (nx * ny);
     } else {
         pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
     }
-    const real wx = (real)K->w[0], wy = (real)K->w[1], wz = (real)K->w[2];
+    const Box& B = boxes[MULTI ? flag_box(real_bits(pi.w)) : 0];
+    const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
+    if (live) {
+        const int c = cell[i] - B.cell_base;
+        cx = c % nx;
+        cy = (c / nx) % ny;
+        cz = c / (nx * ny);
+    }
+    const real* T = MULTI ? tab + B.tab : Tsh;
+    uint32_t keys[10];
+    {
+        uint32_t k = philox_step_key(B.seed, step);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
+    }
+    const real wx = (real)B.w[0], wy = (real)B.w[1], wz = (real)B.w[2];
     // home x shifted into the frame of the row's cells x-1, x, x+1
     const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
     constexpr int NACC = VIRIAL ? 12 : 3;
@@ -163,7 +172,7 @@ __global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces(
         int y2 = cy + dy, z2 = cz + dz;
         y2 += (y2 < 0) ? ny : ((y2 >= ny) ? -ny : 0);
         z2 += (z2 < 0) ? nz : ((z2 >= nz) ? -nz : 0);
-        const int rb = nx * (y2 + ny * z2);
+        const int rb = B.cell_base + nx * (y2 + ny * z2);
         const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
         const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
         for (int seg = 0; seg < 2; ++seg) {

@@ -31,7 +31,8 @@ EXPORTED = [
     "dpd_engine_set_conservative", "dpd_engine_step", "dpd_engine_status", "dpd_engine_download",
     "dpd_engine_cells", "dpd_engine_observables", "dpd_engine_launch_count",
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
-    "dpd_engine_profile_read", "dpd_engine_set_sample_period",
+    "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
+    "dpd_batch_observables",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -44,6 +45,12 @@ class DpdParams(C.Structure):
                 ("dt", C.c_double), ("lam", C.c_double), ("kT", C.c_double),
                 ("ntypes", C.c_int32), ("a", C.POINTER(C.c_double)), ("gamma", C.POINTER(C.c_double)),
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+class DpdBox(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("wx", C.c_double), ("wy", C.c_double), ("wz", C.c_double),
+                ("a", C.POINTER(C.c_double)), ("gamma", C.POINTER(C.c_double)), ("seed", C.c_uint64)]
 
 
 class DpdObs(C.Structure):
@@ -94,6 +101,9 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
+    L.dpd_batch_create.argtypes = [C.POINTER(DpdParams), C.c_int32, C.POINTER(DpdBox), C.POINTER(vp)]
+    L.dpd_batch_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 8
+    L.dpd_batch_observables.argtypes = [vp, C.c_int32, C.POINTER(DpdObs)]
     L.dpd_engine_destroy.argtypes = [vp]
     L.dpd_engine_destroy.restype = None
     _lib = L
@@ -233,3 +243,51 @@ class DpdEngine:
             self.close()
         except Exception:
             pass
+
+
+class DpdBatch(DpdEngine):
+    """Many independent boxes (replicas) advanced by the same kernel launches.
+
+    ``systems`` are DpdSystem objects with the same bead types, dt, lambda and
+    kT and no bonds; bead arrays in and out are the concatenation of the
+    systems in order, positions box-local."""
+
+    def __init__(self, systems, precision: int = MIXED, device: int = -1):
+        L = load()
+        s0 = systems[0]
+        self.systems = list(systems)
+        self._tabs = []
+        boxes = (DpdBox * len(systems))()
+        for k, s in enumerate(systems):
+            a = np.ascontiguousarray(s.a, np.float64)
+            g = np.ascontiguousarray(s.gamma, np.float64)
+            self._tabs.append((a, g))
+            boxes[k] = DpdBox(s.cells[0], s.cells[1], s.cells[2], *[float(w) for w in s.widths],
+                              a.ctypes.data_as(C.POINTER(C.c_double)), g.ctypes.data_as(C.POINTER(C.c_double)),
+                              abs(int(s.seed)) & 0xFFFFFFFFFFFFFFFF)
+        self._a = self._tabs[0][0]
+        self._g = self._tabs[0][1]
+        p = DpdParams(0, 0, 0, 0.0, 0.0, 0.0, float(s0.dt), float(s0.lam), float(s0.kT), len(s0.type_names),
+                      self._a.ctypes.data_as(C.POINTER(C.c_double)), self._g.ctypes.data_as(C.POINTER(C.c_double)),
+                      0, int(precision), int(device))
+        h = C.c_void_p()
+        rc = L.dpd_batch_create(C.byref(p), len(systems), boxes, C.byref(h))
+        if rc != 0:
+            raise EngineError(f"dpd_batch_create failed ({rc})")
+        self.h = h
+        self.precision = precision
+        self.offsets = np.cumsum([0] + [s.n for s in systems])
+        cat = lambda f, dt: np.ascontiguousarray(np.concatenate([getattr(s, f) for s in systems]), dt)
+        box = np.concatenate([np.full(s.n, k, np.int32) for k, s in enumerate(systems)])
+        arrs = [box, cat("ids", np.int64), cat("types", np.int32), cat("movable", np.uint8), cat("x", np.float64),
+                cat("unpbc", np.float64), cat("v", np.float64), cat("f", np.float64)]
+        self.n = int(self.offsets[-1])
+        self._check(L.dpd_batch_upload_beads(self.h, self.n, *[_p(a) for a in arrs]), "batch_upload_beads")
+
+    def box_observables(self, box: int) -> dict:
+        o = DpdObs()
+        self._check(load().dpd_batch_observables(self.h, int(box), C.byref(o)), "batch_observables")
+        return o.as_dict()
+
+    def split(self, arr):
+        return [arr[self.offsets[k]:self.offsets[k + 1]] for k in range(len(self.systems))]
