@@ -176,9 +176,23 @@ def run_reference_arm(args):
     return 0
 
 
-def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool):
+def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool):
+    """Pair-kernel launch shape from the autotuner (cached per GPU and workload)."""
+    if not enabled:
+        return None
+    from osprey_dpd_b200 import autotune
+    sig = autotune.signature(torch.cuda.get_device_name(dev), system.n, system.ncells, len(system.type_names),
+                             precision, 1)
+    make = lambda: engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
+    return autotune.tune(make, sig, steps=10, reps=2)
+
+
+def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
+                shape=None):
     """Per-step device time (ms) with L2 flushed before each step."""
     eng = engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
+    if shape:
+        eng.set_launch_shape(*shape)
     eng.set_sample_period(SAMPLE_PERIOD)
     stream = torch.cuda.Stream(device=dev)
     eng.set_stream(stream.cuda_stream)
@@ -251,6 +265,87 @@ def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch):
     return times, (h2d + topo_bytes) / E2E_PERIOD, d2h / E2E_PERIOD
 
 
+def run_replica_sweep(args, dev, torch, E):
+    """512 independent A/B replicas (box edges 8..24, A fraction 0.1..0.5,
+    a_AB 25 -> 60, own seeds): one batch advanced as a captured 100-step CUDA
+    graph, against the same replicas stepped one engine at a time (each also
+    replaying its own 100-step graph).  The state (~1 GB) exceeds L2."""
+    from osprey_dpd_b200 import workloads as W
+    nrep = args.replicas
+    systems = [W.replica(r, nrep) for r in range(nrep)]
+    ntot = sum(s.n for s in systems)
+    K = args.graph_steps
+    stream = torch.cuda.Stream(device=dev)
+    shape = None
+    if not args.no_autotune:
+        from osprey_dpd_b200 import autotune
+        sig = autotune.signature(torch.cuda.get_device_name(dev), ntot, sum(s.ncells for s in systems), 2, 0, nrep)
+        shape = autotune.tune(lambda: E.DpdBatch(systems, precision=E.MIXED, device=dev.index), sig, steps=K,
+                              reps=1)["shape"]
+    batch = E.DpdBatch(systems, precision=E.MIXED, device=dev.index)
+    if shape:
+        batch.set_launch_shape(*shape)
+    batch.set_sample_period(K)
+    batch.set_stream(stream.cuda_stream)
+    t = 1
+    for _ in range(args.warmup):
+        batch.step(t, K)
+        t += K
+    torch.cuda.synchronize(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    l0 = batch.launch_count()
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+    for _ in range(args.steps):
+        batch.step(t, K)
+        t += K
+    with torch.cuda.stream(stream):
+        ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    batch_ms = ev[0].elapsed_time(ev[1])
+    batch_launches = batch.launch_count() - l0
+    batch_status = batch.status()
+    batch.close()
+    # one at a time
+    engines = []
+    for s in systems:
+        e = E.DpdEngine.from_system(s, precision=E.MIXED, device=dev.index, topology=False)
+        e.set_sample_period(K)
+        e.set_stream(stream.cuda_stream)
+        engines.append(e)
+    t = 1
+    for _ in range(args.warmup):
+        for e in engines:
+            e.step(t, K)
+        t += K
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+    for _ in range(args.steps):
+        for e in engines:
+            e.step(t, K)
+        t += K
+    with torch.cuda.stream(stream):
+        ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    single_ms = ev[0].elapsed_time(ev[1])
+    for e in engines:
+        e.close()
+    work = ntot * K * args.steps
+    return {
+        "metric": "bead-steps/s, 512-replica A/B sweep: one batch vs replicas one at a time, 1 B200",
+        "value": work / (batch_ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": args.steps * K,
+        "warmup": args.warmup * K, "ms_per_step": batch_ms / (args.steps * K), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 state",
+        "data": "synthetic (seeded replica table)",
+        "config": {"workload": f"{nrep} A/B replicas, edges 8..24, {ntot} beads in total", "n_beads": ntot,
+                   "graph_steps": K, "l2": "state (~1 GB) larger than L2", "precision": "mixed"},
+        "one_at_a_time": {"value": work / (single_ms / 1000.0), "ms_per_step": single_ms / (args.steps * K)},
+        "batch_over_one_at_a_time": single_ms / batch_ms,
+        "gpu_launches": batch_launches, "status_bits": batch_status, "launch_shape": shape,
+    }
+
+
 def read_traffic(n_beads: int):
     """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "pair_forces_traffic.json")
@@ -268,11 +363,14 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", default="bilayer", choices=["bilayer", "water", "binary", "polymer"])
+    ap.add_argument("--workload", default="bilayer", choices=["bilayer", "water", "binary", "polymer", "replicas"])
+    ap.add_argument("--replicas", type=int, default=512)
+    ap.add_argument("--graph-steps", type=int, default=100, help="steps per captured graph (replicas)")
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=12, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -292,6 +390,14 @@ def main():
     torch.cuda.set_device(dev)
     from osprey_dpd_b200 import engine as E
 
+    if args.workload == "replicas":
+        line = run_replica_sweep(args, dev, torch, __import__("osprey_dpd_b200.engine", fromlist=["x"]))
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
     system, desc = workload(args.workload, seed_offset=rank)
     peaks, peak_kind = load_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -319,15 +425,17 @@ def main():
         sampler = ClockSampler(local) if prec_name == "mixed" else None
         if sampler:
             sampler.start()
+        tuned = tuned_shape(E, system, prec, dev, torch, not args.no_autotune)
         torch.cuda.synchronize(dev)
-        ms, prof, launches, status = time_engine(E, system, prec, args.steps, args.warmup, dev, torch, True)
+        ms, prof, launches, status = time_engine(E, system, prec, args.steps, args.warmup, dev, torch, True,
+                                                 tuned["shape"] if tuned else None)
         torch.cuda.synchronize(dev)
         barrier()
         if sampler:
             clocks = sampler.stop()
         total_ms = max_over_ranks(sum(ms))
         results[prec_name] = {"ms": ms, "total_ms": total_ms, "prof": prof, "launches": launches,
-                              "status": status,
+                              "status": status, "shape": tuned["shape"] if tuned else None,
                               "value": ws * system.n * args.steps / (total_ms / 1000.0)}
 
     e2e_value = h2d_step = d2h_step = None
@@ -383,6 +491,7 @@ def main():
                               "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),
                               "bytes_per_bead_step": ALG_BYTES_PER_BEAD_STEP["mixed"], "basis": peak_kind},
         "kernel_share": kern_share,
+        "launch_shape": {k: v["shape"] for k, v in results.items()},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_step, "d2h_bytes_per_step": d2h_step,
                 "call": f"upload_beads + upload_topology + step({E2E_PERIOD}) + observables + download, host pinned "

@@ -155,6 +155,13 @@ DPD_API int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps);
  * extra work, so other steps skip it as the reference's monitor does. */
 DPD_API int dpd_engine_set_sample_period(dpd_engine* e, int64_t period);
 
+/* Launch shape of the pair-force kernel (what the autotuner varies): hit-list
+ * capacity per bead before a force pass (8..64, default 32), resident blocks
+ * per SM of a persistent grid (0 = one 128-bead tile per block, the default),
+ * preferred shared-memory carveout in percent (-1 = driver default). */
+DPD_API int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persistent_blocks_per_sm,
+                                        int32_t smem_carveout);
+
 /* Waits for queued work; returns the device status bits seen so far. */
 DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
 

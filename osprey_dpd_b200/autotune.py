@@ -1,0 +1,76 @@
+"""Autotuner for the pair-force kernel's launch shape.
+
+The shape of the force kernel (hit-list capacity per bead, persistent grid
+or one tile per block, shared-memory carveout) is chosen by timing candidate
+shapes on the live workload: for each candidate the engine advances a scratch
+copy of the system by a few captured multi-step calls and the fastest shape
+wins.  Results are cached in a JSON file keyed by the GPU name and a
+signature of the workload (bead count, cell count, bead types, precision,
+number of boxes), so a run pays for tuning once.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from typing import Callable, Dict, Iterable, Optional, Tuple
+
+Shape = Tuple[int, int, int]          # (hitcap, persistent blocks per SM, carveout)
+
+DEFAULT_CANDIDATES: Tuple[Shape, ...] = (
+    (32, 0, -1), (40, 0, -1), (24, 0, -1), (48, 0, -1), (32, 0, 100), (32, 4, -1), (32, 8, -1),
+)
+CACHE = os.environ.get("DPD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "osprey_dpd_b200",
+                                                       "launch_shapes.json"))
+
+
+def signature(gpu: str, n: int, ncells: int, ntypes: int, precision: int, nboxes: int) -> str:
+    return f"{gpu}|n={n}|cells={ncells}|types={ntypes}|prec={precision}|boxes={nboxes}"
+
+
+def _load(path: str) -> Dict[str, dict]:
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path: str, table: Dict[str, dict]) -> None:
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as fh:
+        json.dump(table, fh, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def tune(make_engine: Callable[[], object], sig: str, candidates: Iterable[Shape] = DEFAULT_CANDIDATES,
+         steps: int = 20, reps: int = 3, sync: Optional[Callable[[], None]] = None,
+         cache_path: str = CACHE, force: bool = False) -> dict:
+    """Times every candidate shape on a fresh engine from ``make_engine`` and
+    returns {"shape": best, "ms_per_step": ..., "trials": {...}}; cached by sig."""
+    table = _load(cache_path)
+    if not force and sig in table:
+        return table[sig]
+    trials = {}
+    for shape in candidates:
+        eng = make_engine()
+        eng.set_launch_shape(*shape)
+        t = 1
+        eng.step(t, steps)       # capture + warm-up
+        t += steps
+        eng.status()
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            eng.step(t, steps)
+            eng.status()         # waits for the work
+            best = min(best, (time.perf_counter() - t0) * 1000.0 / steps)
+            t += steps
+        eng.close()
+        trials[",".join(map(str, shape))] = best
+    win = min(trials, key=trials.get)
+    res = {"shape": [int(v) for v in win.split(",")], "ms_per_step": trials[win], "trials": trials}
+    table[sig] = res
+    _store(cache_path, table)
+    return res

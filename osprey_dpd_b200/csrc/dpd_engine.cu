@@ -88,7 +88,10 @@ struct dpd_engine {
     // download staging
     double* d_out = nullptr;    // 3n x, 3n u, 3n v, 3n f, 9n stress
     int* d_out_cell = nullptr;
-    // topology
+    // topology (buffers grow but never move for same-size uploads, so
+    // captured graphs stay valid)
+    size_t cap_csr_ptr = 0, cap_csr_term = 0, cap_bond = 0, cap_ang = 0, cap_off = 0;
+    bool off_active = false;
     int* d_csr_ptr = nullptr;
     int* d_csr_term = nullptr;
     int* d_bond_h = nullptr;
@@ -172,6 +175,21 @@ void dfree(dpd_engine* e, void* p)
         cudaFree(p);
         e->allocations.erase(it);
     }
+}
+
+// Grows *p to hold count elements; sets *moved when the address changes.
+template <typename T>
+int ensure(dpd_engine* e, T** p, size_t& cap, size_t count, bool* moved)
+{
+    if (*p && count <= cap) return DPD_OK;
+    dfree(e, *p);
+    *p = nullptr;
+    cap = 0;
+    const int rc = dalloc(e, p, count ? count : 1);
+    if (rc) return rc;
+    cap = count ? count : 1;
+    *moved = true;
+    return DPD_OK;
 }
 
 size_t real_size(const dpd_engine* e) { return e->precision == DPD_PRECISION_FP64 ? sizeof(double) : sizeof(float); }
@@ -383,7 +401,7 @@ int queue_step(dpd_engine* e, bool sample)
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
     const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
                         e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_ang_k3, e->d_ang_cos0,
-                        e->d_ang_sin0, e->d_off};
+                        e->d_ang_sin0, e->off_active ? e->d_off : nullptr};
     {
         Timed t(e, DPD_KERNEL_UPDATE_MOM);
         auto kern = sample ? k_update_mom<real, true> : k_update_mom<real, false>;
@@ -438,15 +456,17 @@ void release_topology(dpd_engine* e)
     for (auto q : ip) { dfree(e, *q); *q = nullptr; }
     double** dp[] = {&e->d_bond_k2, &e->d_bond_l0, &e->d_ang_k3, &e->d_ang_cos0, &e->d_ang_sin0};
     for (auto q : dp) { dfree(e, *q); *q = nullptr; }
+    e->cap_csr_ptr = e->cap_csr_term = e->cap_bond = e->cap_ang = 0;
 }
 
 // Empty topology: csr_ptr all zero.
 int empty_topology(dpd_engine* e)
 {
-    release_topology(e);
+    bool moved = false;
     int rc;
-    if ((rc = dalloc(e, &e->d_csr_ptr, (size_t)e->n + 1))) return rc;
+    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved))) return rc;
     CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
+    if (moved) drop_graphs(e);
     return DPD_OK;
 }
 
@@ -593,6 +613,23 @@ void dpd_engine_destroy(dpd_engine* e)
 
 const char* dpd_engine_last_error(const dpd_engine* e) { return e ? e->err.c_str() : "null engine"; }
 
+int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persistent_blocks_per_sm,
+                                int32_t smem_carveout)
+{
+    if (!e) return DPD_E_ARG;
+    if (hitcap < 8 || hitcap > kHitCapMax || persistent_blocks_per_sm < 0 || smem_carveout < -1 ||
+        smem_carveout > 100)
+        return fail(e, DPD_E_ARG, "launch shape out of range");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    e->pair_hitcap = hitcap;
+    e->pair_bps = persistent_blocks_per_sm;
+    e->pair_carveout = smem_carveout;
+    memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
+    drop_graphs(e);
+    return DPD_OK;
+}
+
 int dpd_engine_set_sample_period(dpd_engine* e, int64_t period)
 {
     if (!e) return DPD_E_ARG;
@@ -653,7 +690,6 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
                        const double* f3)
 {
     if (!e) return DPD_E_ARG;
-    drop_graphs(e);
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
     if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
     CU(cudaSetDevice(e->device));
@@ -718,8 +754,10 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
         slot_of[b] = (int)s;
         order[s] = (int)b;
     }
-    // (re)allocate per-bead buffers
+    // (re)allocate per-bead buffers; new addresses invalidate the captured graphs
     if (e->n != n) {
+        drop_graphs(e);
+        release_topology(e);
         void** bufs[] = {(void**)&e->d_x[0], (void**)&e->d_x[1], (void**)&e->d_v[0], (void**)&e->d_v[1],
                          (void**)&e->d_bid[0], (void**)&e->d_bid[1], (void**)&e->d_tf[0], (void**)&e->d_tf[1],
                          (void**)&e->d_img[0], (void**)&e->d_img[1], (void**)&e->d_cell[0], (void**)&e->d_cell[1],
@@ -751,13 +789,16 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
         if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
         e->n = n;
     }
-    dfree(e, e->d_off);
-    e->d_off = nullptr;
     if (any_off) {
+        bool moved = false;
         int rc;
-        if ((rc = dalloc(e, &e->d_off, 3 * (size_t)n))) return rc;
+        if ((rc = ensure(e, &e->d_off, e->cap_off, 3 * (size_t)n, &moved))) return rc;
         CU(cudaMemcpy(e->d_off, off.data(), off.size() * sizeof(double), cudaMemcpyHostToDevice));
+        if (moved || !e->off_active) drop_graphs(e);
+    } else if (e->off_active) {
+        drop_graphs(e);        // the kernels' offset pointer becomes null
     }
+    e->off_active = any_off;
     // host staging in slot order
     std::vector<double> hx(3 * n), hv(3 * n), hf(3 * n);
     std::vector<int> hbid(n), htf(n), hcell(n), hpid(n);
@@ -828,7 +869,6 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads before the topology");
     if (e->hboxes.size() > 1 && (nb > 0 || na > 0))
         return fail(e, DPD_E_STATE, "bonds are not supported in a replica batch");
-    drop_graphs(e);
     if (nb < 0 || na < 0 || (nb && (!bond_head_id || !bond_tail_id || !k2 || !l0)) ||
         (na && (!first_bond || !second_bond || !k3 || !phi0)))
         return fail(e, DPD_E_ARG, "bad topology arrays");
@@ -898,33 +938,46 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         }
         CU(cudaMemcpy(e->d_tf[c], tf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     }
-    release_topology(e);
+    bool moved = false;
     int rc;
-    if ((rc = dalloc(e, &e->d_csr_ptr, (size_t)n + 1))) return rc;
-    if ((rc = dalloc(e, &e->d_csr_term, terms.size()))) return rc;
+    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)n + 1, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, terms.size(), &moved))) return rc;
     CU(cudaMemcpy(e->d_csr_ptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
     if (!terms.empty()) CU(cudaMemcpy(e->d_csr_term, terms.data(), terms.size() * sizeof(int), cudaMemcpyHostToDevice));
     if (nb) {
-        if ((rc = dalloc(e, &e->d_bond_h, nb)) || (rc = dalloc(e, &e->d_bond_t, nb)) ||
-            (rc = dalloc(e, &e->d_bond_k2, nb)) || (rc = dalloc(e, &e->d_bond_l0, nb)))
-            return rc;
+        size_t c = e->cap_bond;
+        if ((rc = ensure(e, &e->d_bond_h, c, nb, &moved))) return rc;
+        c = e->cap_bond;
+        if ((rc = ensure(e, &e->d_bond_t, c, nb, &moved))) return rc;
+        c = e->cap_bond;
+        if ((rc = ensure(e, &e->d_bond_k2, c, nb, &moved))) return rc;
+        c = e->cap_bond;
+        if ((rc = ensure(e, &e->d_bond_l0, c, nb, &moved))) return rc;
+        e->cap_bond = std::max(e->cap_bond, (size_t)nb);
         CU(cudaMemcpy(e->d_bond_h, bh.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_bond_t, bt.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_bond_k2, k2, nb * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_bond_l0, l0, nb * sizeof(double), cudaMemcpyHostToDevice));
     }
     if (na) {
+        const size_t c0 = e->cap_ang;
         for (int k = 0; k < 4; ++k) {
-            if ((rc = dalloc(e, &e->d_ang[k], na))) return rc;
+            size_t c = c0;
+            if ((rc = ensure(e, &e->d_ang[k], c, na, &moved))) return rc;
             CU(cudaMemcpy(e->d_ang[k], a4[k].data(), na * sizeof(int), cudaMemcpyHostToDevice));
         }
-        if ((rc = dalloc(e, &e->d_ang_k3, na)) || (rc = dalloc(e, &e->d_ang_cos0, na)) ||
-            (rc = dalloc(e, &e->d_ang_sin0, na)))
-            return rc;
+        size_t c = c0;
+        if ((rc = ensure(e, &e->d_ang_k3, c, na, &moved))) return rc;
+        c = c0;
+        if ((rc = ensure(e, &e->d_ang_cos0, c, na, &moved))) return rc;
+        c = c0;
+        if ((rc = ensure(e, &e->d_ang_sin0, c, na, &moved))) return rc;
+        e->cap_ang = std::max(c0, (size_t)na);
         CU(cudaMemcpy(e->d_ang_k3, k3, na * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_ang_cos0, acos0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_ang_sin0, asin0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
     }
+    if (moved) drop_graphs(e);
     return DPD_OK;
 }
 
@@ -1090,12 +1143,12 @@ static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, doubl
     const int c = e->cur;
     if (e->precision == DPD_PRECISION_FP64)
         k_download<double><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->d_off,
+            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
             e->sampled ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     else
         k_download<float><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->d_off,
+            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
             e->sampled ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     int rc = check_launch(e, "k_download");

@@ -32,7 +32,7 @@ EXPORTED = [
     "dpd_engine_cells", "dpd_engine_observables", "dpd_engine_launch_count",
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
-    "dpd_batch_observables",
+    "dpd_batch_observables", "dpd_engine_set_launch_shape",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -99,6 +99,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_last_error.restype = C.c_char_p
     L.dpd_engine_set_stream.argtypes = [vp, vp]
     L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
+    L.dpd_engine_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
     L.dpd_batch_create.argtypes = [C.POINTER(DpdParams), C.c_int32, C.POINTER(DpdBox), C.POINTER(vp)]
@@ -212,6 +213,10 @@ class DpdEngine:
         o = DpdObs()
         self._check(load().dpd_engine_observables(self.h, C.byref(o)), "observables")
         return o.as_dict()
+
+    def set_launch_shape(self, hitcap: int = 32, persistent_blocks_per_sm: int = 0, carveout: int = -1) -> None:
+        self._check(load().dpd_engine_set_launch_shape(self.h, int(hitcap), int(persistent_blocks_per_sm),
+                                                       int(carveout)), "set_launch_shape")
 
     def set_sample_period(self, period: int) -> None:
         self._check(load().dpd_engine_set_sample_period(self.h, int(period)), "set_sample_period")

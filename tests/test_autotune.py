@@ -1,0 +1,42 @@
+"""Autotuner logic on a fake engine (no GPU): picks the fastest shape and
+caches it by signature."""
+import time
+
+from osprey_dpd_b200 import autotune
+
+
+class FakeEngine:
+    costs = {(32, 0, -1): 0.002, (40, 0, -1): 0.001, (24, 0, -1): 0.003}
+
+    def __init__(self):
+        self.shape = None
+        self.created = True
+
+    def set_launch_shape(self, *shape):
+        self.shape = tuple(shape)
+
+    def step(self, t, n):
+        time.sleep(self.costs[self.shape] * n / 10)
+
+    def status(self):
+        return 0
+
+    def close(self):
+        pass
+
+
+def test_tune_picks_fastest_and_caches(tmp_path):
+    cache = str(tmp_path / "shapes.json")
+    made = []
+
+    def make():
+        e = FakeEngine()
+        made.append(e)
+        return e
+
+    sig = autotune.signature("B200", 1000, 100, 2, 0, 1)
+    res = autotune.tune(make, sig, candidates=list(FakeEngine.costs), steps=5, reps=2, cache_path=cache)
+    assert res["shape"] == [40, 0, -1]
+    assert len(made) == 3
+    again = autotune.tune(make, sig, candidates=list(FakeEngine.costs), steps=5, reps=2, cache_path=cache)
+    assert again == res and len(made) == 3          # served from the cache
