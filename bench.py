@@ -176,23 +176,35 @@ def run_reference_arm(args):
     return 0
 
 
-def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool):
+def tune_candidates(reproducible: bool):
+    from osprey_dpd_b200 import autotune
+    if reproducible:
+        return autotune.DEFAULT_CANDIDATES
+    return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES
+
+
+def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False):
     """Pair-kernel launch shape from the autotuner (cached per GPU and workload)."""
     if not enabled:
         return None
     from osprey_dpd_b200 import autotune
     sig = autotune.signature(torch.cuda.get_device_name(dev), system.n, system.ncells, len(system.type_names),
-                             precision, 1)
+                             precision, 1, reproducible)
     make = lambda: engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
-    return autotune.tune(make, sig, steps=10, reps=2)
+    return autotune.tune(make, sig, tune_candidates(reproducible), steps=10, reps=2)
+
+
+def pair_scheme_name(shape) -> str:
+    return "half shell (atomics)" if shape and len(shape) > 3 and shape[3] == 1 else "full shell (reproducible)"
 
 
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
                 shape=None):
     """Per-step device time (ms) with L2 flushed before each step."""
+    from osprey_dpd_b200 import autotune
     eng = engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
     if shape:
-        eng.set_launch_shape(*shape)
+        autotune.apply_shape(eng, shape)
     eng.set_sample_period(SAMPLE_PERIOD)
     stream = torch.cuda.Stream(device=dev)
     eng.set_stream(stream.cuda_stream)
@@ -233,7 +245,7 @@ def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev
     return ms, prof, launches, status
 
 
-def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch):
+def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch, shape=None):
     """Reference-facing call sequence with host buffers: upload, one sample
     period of steps, single-bead sums and the full state back to the host."""
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -242,6 +254,9 @@ def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch):
     out = {k: torch.empty((system.n, 3), dtype=torch.float64).pin_memory().numpy() for k in ("x", "u", "v", "f")}
     eng = engine_mod.DpdEngine(system.cells, system.widths, system.dt, system.lam, system.kT, system.a,
                                system.gamma, abs(int(system.seed)), precision, dev.index)
+    if shape:
+        from osprey_dpd_b200 import autotune
+        autotune.apply_shape(eng, shape)
     h2d = ids.nbytes + types.nbytes + mov.nbytes + x.nbytes + u.nbytes + v.nbytes + f.nbytes
     d2h = sum(a.nbytes for a in out.values()) + 8 * 23
     times = []
@@ -277,14 +292,15 @@ def run_replica_sweep(args, dev, torch, E):
     K = args.graph_steps
     stream = torch.cuda.Stream(device=dev)
     shape = None
+    from osprey_dpd_b200 import autotune
     if not args.no_autotune:
-        from osprey_dpd_b200 import autotune
-        sig = autotune.signature(torch.cuda.get_device_name(dev), ntot, sum(s.ncells for s in systems), 2, 0, nrep)
-        shape = autotune.tune(lambda: E.DpdBatch(systems, precision=E.MIXED, device=dev.index), sig, steps=K,
-                              reps=1)["shape"]
+        sig = autotune.signature(torch.cuda.get_device_name(dev), ntot, sum(s.ncells for s in systems), 2, 0, nrep,
+                                 args.reproducible)
+        shape = autotune.tune(lambda: E.DpdBatch(systems, precision=E.MIXED, device=dev.index), sig,
+                              tune_candidates(args.reproducible), steps=K, reps=1)["shape"]
     batch = E.DpdBatch(systems, precision=E.MIXED, device=dev.index)
     if shape:
-        batch.set_launch_shape(*shape)
+        autotune.apply_shape(batch, shape)
     batch.set_sample_period(K)
     batch.set_stream(stream.cuda_stream)
     t = 1
@@ -310,6 +326,8 @@ def run_replica_sweep(args, dev, torch, E):
     engines = []
     for s in systems:
         e = E.DpdEngine.from_system(s, precision=E.MIXED, device=dev.index, topology=False)
+        if shape:     # the same pair scheme; the batch's tuned shape
+            autotune.apply_shape(e, shape)
         e.set_sample_period(K)
         e.set_stream(stream.cuda_stream)
         engines.append(e)
@@ -339,7 +357,8 @@ def run_replica_sweep(args, dev, torch, E):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 state",
         "data": "synthetic (seeded replica table)",
         "config": {"workload": f"{nrep} A/B replicas, edges 8..24, {ntot} beads in total", "n_beads": ntot,
-                   "graph_steps": K, "l2": "state (~1 GB) larger than L2", "precision": "mixed"},
+                   "graph_steps": K, "l2": "state (~1 GB) larger than L2", "precision": "mixed",
+                   "pair_scheme": pair_scheme_name(shape)},
         "one_at_a_time": {"value": work / (single_ms / 1000.0), "ms_per_step": single_ms / (args.steps * K)},
         "batch_over_one_at_a_time": single_ms / batch_ms,
         "gpu_launches": batch_launches, "status_bits": batch_status, "launch_shape": shape,
@@ -371,6 +390,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
+    ap.add_argument("--reproducible", action="store_true",
+                    help="tune over the full-shell (bitwise reproducible) pair scheme only")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -425,7 +446,7 @@ def main():
         sampler = ClockSampler(local) if prec_name == "mixed" else None
         if sampler:
             sampler.start()
-        tuned = tuned_shape(E, system, prec, dev, torch, not args.no_autotune)
+        tuned = tuned_shape(E, system, prec, dev, torch, not args.no_autotune, args.reproducible)
         torch.cuda.synchronize(dev)
         ms, prof, launches, status = time_engine(E, system, prec, args.steps, args.warmup, dev, torch, True,
                                                  tuned["shape"] if tuned else None)
@@ -441,7 +462,8 @@ def main():
     e2e_value = h2d_step = d2h_step = None
     e2e_times = []
     if not args.no_e2e:
-        e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch)
+        mshape = (results.get("mixed") or {}).get("shape")
+        e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch, mshape)
         e2e_t = max_over_ranks(sum(e2e_times))
         e2e_value = ws * system.n * E2E_PERIOD * len(e2e_times) / e2e_t
 
@@ -476,7 +498,7 @@ def main():
         "data": "synthetic (seeded generator, reference workload shapes)",
         "config": {"workload": desc, "n_beads": system.n, "cells": list(system.cells), "dt": system.dt,
                    "precision": "mixed", "l2": "flushed before every timed step (256 MiB write, then 256 MiB read so no dirty lines remain)",
-                   "sample_period": SAMPLE_PERIOD,
+                   "sample_period": SAMPLE_PERIOD, "pair_scheme": pair_scheme_name(mixed["shape"]),
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
         "fp64": ({"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
                   "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]} if "fp64" in results else None),

@@ -162,6 +162,17 @@ DPD_API int dpd_engine_set_sample_period(dpd_engine* e, int64_t period);
 DPD_API int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persistent_blocks_per_sm,
                                         int32_t smem_carveout);
 
+/* Pair-force scheme.  DPD_PAIR_FULL_SHELL (default): each bead sums its own
+ * 27-cell neighbourhood; every pair is evaluated twice and the forces are
+ * bitwise reproducible.  DPD_PAIR_HALF_SHELL: every pair once, over the
+ * reference's own 13-cell half shell (CNTCell.cpp:1103-1572); the partner's
+ * share is added with atomics, so the last bits of the FP32/FP64 force sums
+ * vary from run to run, and the sampled pair virial goes whole to one bead of
+ * the pair.  No counterpart in the reference's interface. */
+#define DPD_PAIR_FULL_SHELL 0
+#define DPD_PAIR_HALF_SHELL 1
+DPD_API int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme);
+
 /* Waits for queued work; returns the device status bits seen so far. */
 DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
 

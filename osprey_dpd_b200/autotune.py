@@ -1,7 +1,8 @@
 """Autotuner for the pair-force kernel's launch shape.
 
 The shape of the force kernel (hit-list capacity per bead, persistent grid
-or one tile per block, shared-memory carveout) is chosen by timing candidate
+or one tile per block, shared-memory carveout, and where the caller allows
+run-to-run variation in the last bits, the half-shell pair scheme) is chosen by timing candidate
 shapes on the live workload: for each candidate the engine advances a scratch
 copy of the system by a few captured multi-step calls and the fastest shape
 wins.  Results are cached in a JSON file keyed by the GPU name and a
@@ -15,17 +16,31 @@ import os
 import time
 from typing import Callable, Dict, Iterable, Optional, Tuple
 
-Shape = Tuple[int, int, int]          # (hitcap, persistent blocks per SM, carveout)
+Shape = Tuple[int, ...]     # (hitcap, persistent blocks per SM, carveout[, pair scheme])
 
+# full-shell shapes: bitwise reproducible forces
 DEFAULT_CANDIDATES: Tuple[Shape, ...] = (
     (32, 0, -1), (40, 0, -1), (24, 0, -1), (48, 0, -1), (32, 0, 100), (32, 4, -1), (32, 8, -1),
+)
+# half-shell shapes (pair scheme 1): each pair once, atomics, last bits vary
+HALF_SHELL_CANDIDATES: Tuple[Shape, ...] = (
+    (32, 0, -1, 1), (24, 0, -1, 1), (40, 0, -1, 1), (32, 0, 50, 1),
 )
 CACHE = os.environ.get("DPD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "osprey_dpd_b200",
                                                        "launch_shapes.json"))
 
 
-def signature(gpu: str, n: int, ncells: int, ntypes: int, precision: int, nboxes: int) -> str:
-    return f"{gpu}|n={n}|cells={ncells}|types={ntypes}|prec={precision}|boxes={nboxes}"
+def signature(gpu: str, n: int, ncells: int, ntypes: int, precision: int, nboxes: int,
+              reproducible: bool = True) -> str:
+    sig = f"{gpu}|n={n}|cells={ncells}|types={ntypes}|prec={precision}|boxes={nboxes}"
+    return sig if reproducible else sig + "|half"
+
+
+def apply_shape(eng, shape: Shape) -> None:
+    """Sets a tuned shape on an engine (the scheme only when the shape names one)."""
+    eng.set_launch_shape(*shape[:3])
+    if len(shape) > 3:
+        eng.set_pair_scheme(shape[3])
 
 
 def _load(path: str) -> Dict[str, dict]:
@@ -55,7 +70,7 @@ def tune(make_engine: Callable[[], object], sig: str, candidates: Iterable[Shape
     trials = {}
     for shape in candidates:
         eng = make_engine()
-        eng.set_launch_shape(*shape)
+        apply_shape(eng, shape)
         t = 1
         eng.step(t, steps)       # capture + warm-up
         t += steps

@@ -138,6 +138,7 @@ struct dpd_engine {
     int pair_hitcap = 32;
     int pair_bps = 0;          // resident blocks per SM for the persistent grid
     int pair_carveout = -1;    // preferred shared-memory carveout in percent, -1 = driver default
+    bool pair_half = false;    // half-shell pair kernel (atomics, not bitwise reproducible)
     bool pair_attr_set[2][2] = {{false, false}, {false, false}};   // [fp64][sample]; one box kind per engine
 };
 
@@ -326,6 +327,17 @@ struct Timed {
     }
 };
 
+// The pair kernel variant for (box table, sample step, half shell).
+template <typename real>
+auto pair_kernel(bool multi, bool sample, bool half)
+{
+    if (half)
+        return multi ? (sample ? k_pair_forces_half<real, true, true> : k_pair_forces_half<real, false, true>)
+                     : (sample ? k_pair_forces_half<real, true, false> : k_pair_forces_half<real, false, false>);
+    return multi ? (sample ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
+                 : (sample ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+}
+
 // Dynamic shared memory and carveout of the pair kernel's variants (outside
 // any stream capture).
 template <typename real>
@@ -335,8 +347,7 @@ int set_pair_attributes(dpd_engine* e)
     const int pv = sizeof(real) == 8 ? 1 : 0;
     for (int sv = 0; sv < 2; ++sv) {
         if (e->pair_attr_set[pv][sv]) continue;
-        auto kern = multi ? (sv ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
-                          : (sv ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+        auto kern = pair_kernel<real>(multi, sv != 0, e->pair_half);
         const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         if (e->pair_carveout >= 0)
@@ -384,10 +395,11 @@ int queue_step(dpd_engine* e, bool sample)
     if ((rc = check_launch(e, "k_gather"))) return rc;
     {
         const bool multi = e->hboxes.size() > 1;
-        auto kern = multi ? (sample ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
-                          : (sample ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+        auto kern = pair_kernel<real>(multi, sample, e->pair_half);
         const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
         if ((rc = set_pair_attributes<real>(e))) return rc;
+        // the half shell accumulates into F with atomics
+        if (e->pair_half) CU(cudaMemsetAsync(e->d_F, 0, (size_t)3 * n * sizeof(real), st));
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
@@ -421,8 +433,9 @@ int queue_step(dpd_engine* e, bool sample)
     return DPD_OK;
 }
 
-// "hitcap=32,bps=8,carveout=50": pair-kernel hit-list capacity (8..64), resident
-// blocks per SM for its persistent grid, preferred shared-memory carveout (%).
+// "hitcap=32,bps=8,carveout=50,half=1": pair-kernel hit-list capacity (8..64),
+// resident blocks per SM for its persistent grid, preferred shared-memory
+// carveout (%), half-shell kernel.
 void parse_tuning(dpd_engine* e, const char* spec)
 {
     std::string str(spec);
@@ -438,6 +451,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             if (key == "hitcap") e->pair_hitcap = std::min(std::max(val, 8), (int)kHitCapMax);
             else if (key == "bps") e->pair_bps = std::max(val, 0);
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
+            else if (key == "half") e->pair_half = val != 0;
         }
         pos = end + 1;
     }
@@ -625,6 +639,18 @@ int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persisten
     e->pair_hitcap = hitcap;
     e->pair_bps = persistent_blocks_per_sm;
     e->pair_carveout = smem_carveout;
+    memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
+    drop_graphs(e);
+    return DPD_OK;
+}
+
+int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
+{
+    if (!e) return DPD_E_ARG;
+    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL) return fail(e, DPD_E_ARG, "unknown pair scheme");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    e->pair_half = scheme == DPD_PAIR_HALF_SHELL;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
     return DPD_OK;

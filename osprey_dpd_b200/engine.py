@@ -25,6 +25,9 @@ STATUS_CELL_SKIP = 0x1
 STATUS_NONFINITE = 0x2
 STATUS_IMAGE_OVERFLOW = 0x4
 
+PAIR_FULL_SHELL = 0      # default: bitwise reproducible forces
+PAIR_HALF_SHELL = 1      # each pair once, partner force by atomics
+
 EXPORTED = [
     "dpd_engine_create", "dpd_engine_upload_beads", "dpd_engine_upload_topology",
     "dpd_engine_set_pair_params", "dpd_engine_set_dt", "dpd_engine_set_thermostat",
@@ -32,7 +35,7 @@ EXPORTED = [
     "dpd_engine_cells", "dpd_engine_observables", "dpd_engine_launch_count",
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
-    "dpd_batch_observables", "dpd_engine_set_launch_shape",
+    "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -100,6 +103,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_stream.argtypes = [vp, vp]
     L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
     L.dpd_engine_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+    L.dpd_engine_set_pair_scheme.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
     L.dpd_batch_create.argtypes = [C.POINTER(DpdParams), C.c_int32, C.POINTER(DpdBox), C.POINTER(vp)]
@@ -217,6 +221,10 @@ class DpdEngine:
     def set_launch_shape(self, hitcap: int = 32, persistent_blocks_per_sm: int = 0, carveout: int = -1) -> None:
         self._check(load().dpd_engine_set_launch_shape(self.h, int(hitcap), int(persistent_blocks_per_sm),
                                                        int(carveout)), "set_launch_shape")
+
+    def set_pair_scheme(self, scheme: int) -> None:
+        """PAIR_FULL_SHELL (reproducible) or PAIR_HALF_SHELL (each pair once)."""
+        self._check(load().dpd_engine_set_pair_scheme(self.h, int(scheme)), "set_pair_scheme")
 
     def set_sample_period(self, period: int) -> None:
         self._check(load().dpd_engine_set_sample_period(self.h, int(period)), "set_sample_period")
