@@ -183,8 +183,15 @@ def tune_candidates(reproducible: bool):
     return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES
 
 
-def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False):
-    """Pair-kernel launch shape from the autotuner (cached per GPU and workload)."""
+FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1)}
+
+
+def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False,
+                scheme: str = "auto"):
+    """Pair-kernel launch shape from the autotuner (cached per GPU and workload),
+    or the default shape of a fixed scheme."""
+    if scheme != "auto":
+        return {"shape": list(FIXED_SHAPES[scheme])}
     if not enabled:
         return None
     from osprey_dpd_b200 import autotune
@@ -291,9 +298,9 @@ def run_replica_sweep(args, dev, torch, E):
     ntot = sum(s.n for s in systems)
     K = args.graph_steps
     stream = torch.cuda.Stream(device=dev)
-    shape = None
+    shape = list(FIXED_SHAPES[args.pair_scheme]) if args.pair_scheme != "auto" else None
     from osprey_dpd_b200 import autotune
-    if not args.no_autotune:
+    if shape is None and not args.no_autotune:
         sig = autotune.signature(torch.cuda.get_device_name(dev), ntot, sum(s.ncells for s in systems), 2, 0, nrep,
                                  args.reproducible)
         shape = autotune.tune(lambda: E.DpdBatch(systems, precision=E.MIXED, device=dev.index), sig,
@@ -365,13 +372,14 @@ def run_replica_sweep(args, dev, torch, E):
     }
 
 
-def read_traffic(n_beads: int):
-    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
+def read_traffic(n_beads: int, scheme: str = "full"):
+    """Per-launch DRAM bytes of the pair kernel (full or half shell) from the
+    committed ncu summary, scaled to the bead count."""
     p = os.path.join(ROOT, "profiles", "pair_forces_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
-        d = json.load(fh)
+        d = json.load(fh).get(scheme) or {}
     per_bead = d.get("dram_bytes_per_bead")
     return None if per_bead is None else per_bead * n_beads
 
@@ -392,6 +400,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
     ap.add_argument("--reproducible", action="store_true",
                     help="tune over the full-shell (bitwise reproducible) pair scheme only")
+    ap.add_argument("--pair-scheme", choices=["auto", "full", "half"], default="auto",
+                    help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -446,7 +456,8 @@ def main():
         sampler = ClockSampler(local) if prec_name == "mixed" else None
         if sampler:
             sampler.start()
-        tuned = tuned_shape(E, system, prec, dev, torch, not args.no_autotune, args.reproducible)
+        tuned = tuned_shape(E, system, prec, dev, torch, not args.no_autotune, args.reproducible,
+                            args.pair_scheme)
         torch.cuda.synchronize(dev)
         ms, prof, launches, status = time_engine(E, system, prec, args.steps, args.warmup, dev, torch, True,
                                                  tuned["shape"] if tuned else None)
@@ -482,6 +493,7 @@ def main():
         return 0
 
     mixed = results.get("mixed") or results["fp64"]
+    half = bool(mixed["shape"] and len(mixed["shape"]) > 3 and mixed["shape"][3] == 1)
     pair = mixed["prof"]["pair_forces"]
     t_pair = pair["ms"] / max(pair["launches"], 1) / 1000.0
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -502,13 +514,13 @@ def main():
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
         "fp64": ({"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
                   "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]} if "fp64" in results else None),
-        "roofline": {"bound": "issue", "kernel": "pair_forces (mixed)",
+        "roofline": {"bound": "issue", "kernel": ("k_pair_forces_half" if half else "k_pair_forces") + " (mixed)",
                      "achieved": achieved / 1e9, "peak": issue_peak / 1e9, "unit": "Gslot/s",
                      "frac": achieved / issue_peak,
                      "peak_basis": f"{sms} SMs x 128 FP32/INT32 lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz)",
                      "work_per_bead_step": SLOTS_PER_BEAD_STEP,
                      "avg_launch_ms": t_pair * 1000.0,
-                     "traffic": read_traffic(system.n)},
+                     "traffic": read_traffic(system.n, "half" if half else "full")},
         "roofline_step_hbm": {"bound": "hbm", "achieved": hbm_ach / 1e9, "peak": float(peaks["hbm_gbs"]),
                               "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),
                               "bytes_per_bead_step": ALG_BYTES_PER_BEAD_STEP["mixed"], "basis": peak_kind},
