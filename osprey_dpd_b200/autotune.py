@@ -24,7 +24,7 @@ DEFAULT_CANDIDATES: Tuple[Shape, ...] = (
 )
 # half-shell shapes (pair scheme 1): each pair once, atomics, last bits vary
 HALF_SHELL_CANDIDATES: Tuple[Shape, ...] = (
-    (32, 0, -1, 1), (24, 0, -1, 1), (40, 0, -1, 1), (32, 0, 50, 1),
+    (32, 0, -1, 1), (24, 0, -1, 1), (32, 0, 100, 1), (24, 0, 100, 1), (40, 0, 100, 1),
 )
 CACHE = os.environ.get("DPD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "osprey_dpd_b200",
                                                        "launch_shapes.json"))

@@ -26,6 +26,9 @@ namespace dpd {
 
 constexpr int kPairWarps = 4;
 constexpr int kPairBlock = 32 * kPairWarps;
+// Resident blocks per SM the pair kernels are compiled for: 8 (64 registers,
+// 32 warps) in FP32; the FP64 variants keep 6 to avoid spills.
+template <typename real> struct PairOcc { static constexpr int value = sizeof(real) == 4 ? 8 : 6; };
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
 
 template <typename real> struct RealOps;
@@ -139,7 +142,7 @@ __device__ __forceinline__ void row_segment(bool live, int seg, int rb, int cx, 
 // tables and noise key from the packed box table, tables are read through the
 // read-only cache.  Otherwise one box whose tables are staged in shared memory.
 template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces(
+__global__ void __launch_bounds__(kPairBlock, PairOcc<real>::value) k_pair_forces(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
@@ -327,7 +330,7 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
 // run.  F must be zero on entry.  The pair virial goes whole to bead i, the
 // reference's convention (CNTCell.cpp:1283-1301).
 template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kPairBlock, 6) k_pair_forces_half(
+__global__ void __launch_bounds__(kPairBlock, PairOcc<real>::value) k_pair_forces_half(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
