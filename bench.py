@@ -206,8 +206,10 @@ def pair_scheme_name(shape) -> str:
 
 
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
-                shape=None):
-    """Per-step device time (ms) with L2 flushed before each step."""
+                shape=None, profile_steps: int = 20):
+    """Per-step device time (ms) of single-step calls with L2 flushed before
+    each step; then, when asked, a separate pass with CUDA events around every
+    kernel (launched one by one) for the per-kernel durations."""
     from osprey_dpd_b200 import autotune
     eng = engine_mod.DpdEngine.from_system(system, precision=precision, device=dev.index)
     if shape:
@@ -232,8 +234,6 @@ def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev
         t += 1
     torch.cuda.synchronize(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    if profile:
-        eng.profile(True)
     launches0 = eng.launch_count()
     for k in range(steps):
         with torch.cuda.stream(stream):
@@ -246,7 +246,17 @@ def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev
     torch.cuda.synchronize(dev)
     launches = eng.launch_count() - launches0
     ms = [a.elapsed_time(b) for a, b in evs]
-    prof = eng.profile_read() if profile else None
+    prof = None
+    if profile:
+        eng.profile(True)
+        for _ in range(profile_steps):
+            with torch.cuda.stream(stream):
+                flush_l2()
+            eng.step(t, 1)
+            t += 1
+        torch.cuda.synchronize(dev)
+        prof = eng.profile_read()
+        eng.profile(False)
     status = eng.status()
     eng.close()
     return ms, prof, launches, status
@@ -520,6 +530,8 @@ def main():
                      "peak_basis": f"{sms} SMs x 128 FP32/INT32 lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz)",
                      "work_per_bead_step": SLOTS_PER_BEAD_STEP,
                      "avg_launch_ms": t_pair * 1000.0,
+                     "timing": "CUDA events around every kernel on the engine's stream, in a 20-step pass "
+                               "after the timed region (same engine and workload, kernels launched one by one)",
                      "traffic": read_traffic(system.n, "half" if half else "full")},
         "roofline_step_hbm": {"bound": "hbm", "achieved": hbm_ach / 1e9, "peak": float(peaks["hbm_gbs"]),
                               "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),

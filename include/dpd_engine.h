@@ -61,11 +61,12 @@ extern "C" {
 #define DPD_KERNEL_PERMUTE      2   /* arrival slot -> new slot                */
 #define DPD_KERNEL_GATHER       3   /* cell-sorted state + force shadows       */
 #define DPD_KERNEL_PAIR_FORCES  4   /* DPD pair forces (UpdateForce)           */
-#define DPD_KERNEL_UPDATE_MOM   5   /* bonded forces + UpdateMom + sums        */
+#define DPD_KERNEL_UPDATE_MOM   5   /* UpdateMom + single-bead sums            */
 #define DPD_KERNEL_REDUCE_OBS   6   /* final FP64 sums                         */
 #define DPD_KERNEL_DOWNLOAD     7   /* slot order -> bead order                */
 #define DPD_KERNEL_KINETIC      8   /* kinetic sums without a step             */
-#define DPD_NUM_KERNELS         9
+#define DPD_KERNEL_BONDED       9   /* bond + bond-pair forces (FP64)          */
+#define DPD_NUM_KERNELS         10
 
 typedef struct dpd_engine dpd_engine;
 
@@ -144,8 +145,11 @@ DPD_API int dpd_engine_set_thermostat(dpd_engine* e, int32_t on);
 DPD_API int dpd_engine_set_conservative(dpd_engine* e, int32_t on);
 
 /* Runs nsteps timesteps; first_step is the reference's m_SimTime of the first
- * (it keys the pair noise).  Asynchronous: returns once the work is queued.
- * The single-bead sums are taken at the end of the last step. */
+ * (it keys the pair noise).  Asynchronous: returns once the work is queued,
+ * without waiting for earlier calls.  The kernels of a call are captured once
+ * as a CUDA graph per (step count, buffer parity, sample pattern, stream) and
+ * replayed after that (DPD_GRAPHS=0 launches them one by one).  The
+ * single-bead sums are taken at the end of the last step. */
 DPD_API int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps);
 
 /* Steps at which the single-bead sums and the per-bead virial are taken:

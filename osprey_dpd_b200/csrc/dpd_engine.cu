@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "dpd_kernels.cuh"
@@ -37,6 +38,8 @@ struct DevBuf {
 struct dpd_engine {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;          // bonded-force branch, forked from and joined to s()
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     dpd_params params{};
     int precision = DPD_PRECISION_MIXED;
     std::vector<double> a, gamma, gamma_backup, a_backup;   // host copies of the tables
@@ -77,8 +80,13 @@ struct dpd_engine {
     void* d_vel4 = nullptr;
     int* d_rank = nullptr;
     int* d_perm = nullptr;
-    int* d_slot_of = nullptr;
-    int* d_pid_of = nullptr;
+    int* d_pid[2] = {nullptr, nullptr};   // noise id (reference bead id) in slot order
+    int* d_pid_of = nullptr;              // noise id by upload index
+    double4* d_ubuf = nullptr;            // unPBC position of bonded beads by upload index (FP64)
+    int* d_bb = nullptr;                  // bonded beads' upload indices, ascending
+    int64_t nbb = 0;
+    double4* d_Fb = nullptr;              // bonded force by upload index (FP64)
+    double* d_Sb = nullptr;               // bond virial, 9 planes by upload index (sample steps)
     double* d_off = nullptr;
     int* d_count = nullptr;
     int* d_start = nullptr;
@@ -90,7 +98,8 @@ struct dpd_engine {
     int* d_out_cell = nullptr;
     // topology (buffers grow but never move for same-size uploads, so
     // captured graphs stay valid)
-    size_t cap_csr_ptr = 0, cap_csr_term = 0, cap_bond = 0, cap_ang = 0, cap_off = 0;
+    size_t cap_csr_ptr = 0, cap_csr_term = 0, cap_bond = 0, cap_ang = 0, cap_off = 0, cap_ubuf = 0, cap_bb = 0,
+           cap_Fb = 0, cap_Sb = 0;
     bool off_active = false;
     int* d_csr_ptr = nullptr;
     int* d_csr_term = nullptr;
@@ -103,7 +112,6 @@ struct dpd_engine {
     double* d_ang_cos0 = nullptr;
     double* d_ang_sin0 = nullptr;
     // pinned host
-    int64_t* h_step = nullptr;
     unsigned* h_status = nullptr;
     double* h_obs = nullptr;
     bool obs_valid = false;
@@ -129,6 +137,7 @@ struct dpd_engine {
         std::vector<char> samples;
         cudaStream_t stream;
         cudaGraphExec_t exec;
+        int64_t launches;          // kernels per replay
     };
     std::vector<Graph> graphs;
     bool graphs_enabled = true;
@@ -357,8 +366,11 @@ int set_pair_attributes(dpd_engine* e)
     return DPD_OK;
 }
 
+// One timestep.  The first step of a call starts with k_update_pos; the
+// others had their UpdatePos fused into the k_update_mom before them, which
+// does so for every step but the last of the call.
 template <typename real>
-int queue_step(dpd_engine* e, bool sample)
+int queue_step(dpd_engine* e, bool sample, bool first, bool last)
 {
     typedef typename Vec4<real>::type V4;
     const int n = (int)e->n;
@@ -366,13 +378,15 @@ int queue_step(dpd_engine* e, bool sample)
     const int nb = blocks_for(n, kThreads);
     cudaStream_t st = e->s();
     int rc;
-    {
-        Timed t(e, DPD_KERNEL_UPDATE_POS);
-        k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a], (const real*)e->d_F,
-                                                    e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
-                                                    e->d_block_count, e->d_status);
+    if (first) {
+        {
+            Timed t(e, DPD_KERNEL_UPDATE_POS);
+            k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
+                                                        (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a],
+                                                        e->d_rank, e->d_count, e->d_block_count, e->d_status);
+        }
+        if ((rc = check_launch(e, "k_update_pos"))) return rc;
     }
-    if ((rc = check_launch(e, "k_update_pos"))) return rc;
     {
         Timed t(e, DPD_KERNEL_SCAN_CELLS);
         k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, n, e->d_count, e->d_block_count,
@@ -390,9 +404,31 @@ int queue_step(dpd_engine* e, bool sample)
         k_gather<real><<<nb, kThreads, 0, st>>>(
             n, e->d_K, e->d_boxes, e->d_perm, e->d_start, e->d_x[a], e->d_v[a], (const real*)e->d_F, e->d_bid[a],
             e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
-            e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_slot_of, e->d_pid_of, (V4*)e->d_pos4, (V4*)e->d_vel4);
+            e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b], (V4*)e->d_pos4, (V4*)e->d_vel4,
+            e->d_ubuf, e->off_active ? e->d_off : nullptr);
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
+    // bond and bond-pair forces: a branch beside the pair kernel (on the
+    // launching stream itself while profiling, so every kernel is timed)
+    const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
+                        e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_ang_k3, e->d_ang_cos0,
+                        e->d_ang_sin0, e->d_ubuf};
+    const bool fork = e->nbb > 0 && !e->profiling;
+    if (e->nbb > 0) {
+        cudaStream_t bst = st;
+        if (fork) {
+            CU(cudaEventRecord(e->ev_fork, st));
+            CU(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+            bst = e->side;
+        }
+        {
+            Timed t(e, DPD_KERNEL_BONDED);
+            auto kern = sample ? k_bonds<true> : k_bonds<false>;
+            kern<<<blocks_for(e->nbb, kThreads), kThreads, 0, bst>>>((int)e->nbb, n, e->d_bb, topo, e->d_Fb, e->d_Sb);
+        }
+        if ((rc = check_launch(e, "k_bonds"))) return rc;
+        if (fork) CU(cudaEventRecord(e->ev_join, e->side));
+    }
     {
         const bool multi = e->hboxes.size() > 1;
         auto kern = pair_kernel<real>(multi, sample, e->pair_half);
@@ -411,15 +447,15 @@ int queue_step(dpd_engine* e, bool sample)
                                                                (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status);
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
-    const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
-                        e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_ang_k3, e->d_ang_cos0,
-                        e->d_ang_sin0, e->off_active ? e->d_off : nullptr};
+    if (fork) CU(cudaStreamWaitEvent(st, e->ev_join, 0));
     {
         Timed t(e, DPD_KERNEL_UPDATE_MOM);
-        auto kern = sample ? k_update_mom<real, true> : k_update_mom<real, false>;
+        auto kern = sample ? (last ? k_update_mom<real, true, false> : k_update_mom<real, true, true>)
+                           : (last ? k_update_mom<real, false, false> : k_update_mom<real, false, true>);
         kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
-                                       (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_img[b],
-                                       e->d_slot_of, topo, (real*)e->d_stress, e->d_partials, e->d_status);
+                                       (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_Fb, e->d_Sb,
+                                       (real*)e->d_stress, e->d_partials, e->d_img[b], e->d_cell[b], e->d_rank,
+                                       e->d_count, e->d_block_count, e->d_status);
     }
     if ((rc = check_launch(e, "k_update_mom"))) return rc;
     if (sample) {
@@ -480,7 +516,8 @@ int empty_topology(dpd_engine* e)
     int rc;
     if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved))) return rc;
     CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
-    if (moved) drop_graphs(e);
+    if (moved || e->nbb) drop_graphs(e);
+    e->nbb = 0;
     return DPD_OK;
 }
 
@@ -552,7 +589,10 @@ static int create_impl(const dpd_params* p, int32_t nboxes, const dpd_box* bx, d
         cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device);
         if (const char* tune = getenv("DPD_TUNE")) parse_tuning(e, tune);
         if (const char* g = getenv("DPD_GRAPHS")) e->graphs_enabled = atoi(g) != 0;
-        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming) != cudaSuccess) {
             rc = fail(e, DPD_E_CUDA, "cudaStreamCreate failed");
             break;
         }
@@ -568,8 +608,7 @@ static int create_impl(const dpd_params* p, int32_t nboxes, const dpd_box* bx, d
         if ((rc = dalloc(e, &e->d_start, (size_t)ncell + 1))) break;
         if ((rc = dalloc(e, &e->d_block_count, (size_t)e->nchunk))) break;
         if ((rc = dalloc(e, &e->d_obs, kObsTerms))) break;
-        if (cudaMallocHost(&e->h_step, sizeof(int64_t)) != cudaSuccess ||
-            cudaMallocHost(&e->h_status, sizeof(unsigned)) != cudaSuccess ||
+        if (cudaMallocHost(&e->h_status, sizeof(unsigned)) != cudaSuccess ||
             cudaMallocHost(&e->h_obs, kObsTerms * sizeof(double)) != cudaSuccess) {
             rc = fail(e, DPD_E_NOMEM, "cudaMallocHost failed");
             break;
@@ -618,9 +657,12 @@ void dpd_engine_destroy(dpd_engine* e)
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
     for (void* p : e->allocations) cudaFree(p);
     e->allocations.clear();
-    if (e->h_step) cudaFreeHost(e->h_step);
     if (e->h_status) cudaFreeHost(e->h_status);
     if (e->h_obs) cudaFreeHost(e->h_obs);
+    if (e->side) cudaStreamSynchronize(e->side);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
+    if (e->side) cudaStreamDestroy(e->side);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -774,12 +816,8 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     for (int64_t b = 0; b < n; ++b) start[cell[b] + 1]++;
     for (int64_t c = 0; c < e->ncell; ++c) start[c + 1] += start[c];
     std::vector<int64_t> fill(start.begin(), start.end() - 1);
-    std::vector<int> slot_of(n), order(n);
-    for (int64_t b = 0; b < n; ++b) {
-        const int64_t s = fill[cell[b]]++;
-        slot_of[b] = (int)s;
-        order[s] = (int)b;
-    }
+    std::vector<int> order(n);
+    for (int64_t b = 0; b < n; ++b) order[fill[cell[b]]++] = (int)b;
     // (re)allocate per-bead buffers; new addresses invalidate the captured graphs
     if (e->n != n) {
         drop_graphs(e);
@@ -788,7 +826,8 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
                          (void**)&e->d_bid[0], (void**)&e->d_bid[1], (void**)&e->d_tf[0], (void**)&e->d_tf[1],
                          (void**)&e->d_img[0], (void**)&e->d_img[1], (void**)&e->d_cell[0], (void**)&e->d_cell[1],
                          &e->d_F, &e->d_Fold, &e->d_stress, &e->d_pos4, &e->d_vel4, (void**)&e->d_rank,
-                         (void**)&e->d_perm, (void**)&e->d_slot_of, (void**)&e->d_pid_of, (void**)&e->d_partials,
+                         (void**)&e->d_perm, (void**)&e->d_pid[0], (void**)&e->d_pid[1], (void**)&e->d_pid_of,
+                         (void**)&e->d_partials,
                          (void**)&e->d_out, (void**)&e->d_out_cell};
         for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
         const size_t rs = real_size(e);
@@ -800,6 +839,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
             if ((rc = dalloc(e, &e->d_tf[k], (size_t)n))) return rc;
             if ((rc = dalloc(e, &e->d_img[k], (size_t)n))) return rc;
             if ((rc = dalloc(e, &e->d_cell[k], (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_pid[k], (size_t)n))) return rc;
         }
         if ((rc = dalloc(e, (char**)&e->d_F, 3 * rs * (size_t)n))) return rc;
         if ((rc = dalloc(e, (char**)&e->d_Fold, 3 * rs * (size_t)n))) return rc;
@@ -808,7 +848,6 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
         if ((rc = dalloc(e, (char**)&e->d_vel4, 4 * rs * (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_rank, (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_perm, (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_slot_of, (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_pid_of, (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(n, kThreads) * kObsTerms))) return rc;
         if ((rc = dalloc(e, &e->d_out, 21 * (size_t)n))) return rc;
@@ -827,7 +866,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     e->off_active = any_off;
     // host staging in slot order
     std::vector<double> hx(3 * n), hv(3 * n), hf(3 * n);
-    std::vector<int> hbid(n), htf(n), hcell(n), hpid(n);
+    std::vector<int> hbid(n), htf(n), hcell(n), hpid(n), hpids(n);
     std::vector<uint32_t> himg(n);
     for (int64_t s = 0; s < n; ++s) {
         const int b = order[s];
@@ -840,6 +879,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
         htf[s] = type[b] | ((box ? box[b] : 0) << 8) | ((movable && !movable[b]) ? kFlagFrozen : 0);
         hcell[s] = cell[b];
         himg[s] = img[b];
+        hpids[s] = (int)id[b];
     }
     for (int64_t b = 0; b < n; ++b) hpid[b] = (int)id[b];
     const int c = e->cur;
@@ -855,7 +895,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     CU(cudaMemcpy(e->d_tf[c], htf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(e->d_cell[c], hcell.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(e->d_img[c], himg.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_slot_of, slot_of.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(e->d_pid[c], hpids.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(e->d_pid_of, hpid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     std::vector<int> st32(e->ncell + 1);
     for (int64_t k = 0; k <= e->ncell; ++k) st32[k] = (int)start[k];
@@ -904,14 +944,17 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     // bead id -> upload index
     std::vector<int> hpid(n);
     CU(cudaMemcpy(hpid.data(), e->d_pid_of, n * sizeof(int), cudaMemcpyDeviceToHost));
-    std::vector<int> dense;
     bool identity = true;
     for (int64_t b = 0; b < n && identity; ++b) identity = (hpid[b] == b + 1);
+    std::unordered_map<int64_t, int> by_id;
+    if (!identity && (nb || na)) {
+        by_id.reserve((size_t)n);
+        for (int64_t b = 0; b < n; ++b) by_id.emplace((int64_t)hpid[b], (int)b);
+    }
     auto index_of = [&](int64_t idv) -> int {
         if (identity) return (idv >= 1 && idv <= n) ? (int)(idv - 1) : -1;
-        for (int64_t b = 0; b < n; ++b)
-            if (hpid[b] == idv) return (int)b;
-        return -1;
+        const auto it = by_id.find(idv);
+        return it == by_id.end() ? -1 : it->second;
     };
     std::vector<int> bh(nb), bt(nb);
     for (int64_t i = 0; i < nb; ++i) {
@@ -951,8 +994,9 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         terms[fillp[a4[0][i]]++] = (int)(i * 8 + kAngle1);   // middle bead:       force [1]
         terms[fillp[a4[2][i]]++] = (int)(i * 8 + kAngle2);   // second bond's head: force [2]
     }
-    // mark the beads that have terms (flag bit 17) so k_update_mom skips the
-    // topology lookup for all others
+    // mark the beads that have terms (kFlagBonded) so k_update_mom skips the
+    // topology lookup for all others, and k_gather writes their unPBC
+    // position into the FP64 buffer the bonded terms read
     {
         std::vector<int> tf(n), bid(n);
         const int c = e->cur;
@@ -966,6 +1010,18 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     }
     bool moved = false;
     int rc;
+    std::vector<int> bbl;
+    for (int64_t b = 0; b < n; ++b)
+        if (cnt[b + 1] > cnt[b]) bbl.push_back((int)b);
+    if (!bbl.empty()) {
+        if ((rc = ensure(e, &e->d_ubuf, e->cap_ubuf, (size_t)n, &moved))) return rc;
+        if ((rc = ensure(e, &e->d_Fb, e->cap_Fb, (size_t)n, &moved))) return rc;
+        if ((rc = ensure(e, &e->d_Sb, e->cap_Sb, 9 * (size_t)n, &moved))) return rc;
+        if ((rc = ensure(e, &e->d_bb, e->cap_bb, bbl.size(), &moved))) return rc;
+        CU(cudaMemcpy(e->d_bb, bbl.data(), bbl.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if ((int64_t)bbl.size() != e->nbb) drop_graphs(e);   // the bonded branch appears or changes size
+    e->nbb = (int64_t)bbl.size();
     if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)n + 1, &moved))) return rc;
     if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, terms.size(), &moved))) return rc;
     CU(cudaMemcpy(e->d_csr_ptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1075,9 +1131,9 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     CU(cudaSetDevice(e->device));
     // the step counter keys the pair noise; it is advanced on the device
     // by the last kernel of every step
-    CU(cudaStreamSynchronize(e->s()));
-    *e->h_step = first_step;
-    CU(cudaMemcpyAsync(e->d_step, e->h_step, sizeof(int64_t), cudaMemcpyHostToDevice, e->s()));
+    k_set_step<<<1, 1, 0, e->s()>>>(e->d_step, first_step);
+    CU(cudaGetLastError());
+    e->launches += 1;
     std::vector<char> samples(nsteps);
     for (int32_t k = 0; k < nsteps; ++k) {
         const int64_t t = first_step + k;
@@ -1086,14 +1142,15 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     }
     auto queue_all = [&](void) -> int {
         for (int32_t k = 0; k < nsteps; ++k) {
-            const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, samples[k])
-                                                                 : queue_step<float>(e, samples[k]);
+            const bool first = k == 0, last = k == nsteps - 1;
+            const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, samples[k], first, last)
+                                                                 : queue_step<float>(e, samples[k], first, last);
             if (rc) return rc;
         }
         return DPD_OK;
     };
     const int parity = e->cur;
-    if (e->graphs_enabled && !e->profiling && nsteps >= 2) {
+    if (e->graphs_enabled && !e->profiling) {
         // one captured graph per (step count, buffer parity, sample pattern, stream)
         dpd_engine::Graph* g = nullptr;
         for (auto& cand : e->graphs)
@@ -1120,15 +1177,13 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
             ce = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             if (ce != cudaSuccess) return fail(e, DPD_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-            e->graphs.push_back({nsteps, parity, samples, e->s(), exec});
+            e->graphs.push_back({nsteps, parity, samples, e->s(), exec, e->launches - launches0});
             g = &e->graphs.back();
             e->launches = launches0;   // counted per replay below
             e->cur = parity;
         }
         CU(cudaGraphLaunch(g->exec, e->s()));
-        int64_t nsample = 0;
-        for (char c : samples) nsample += c;
-        e->launches += 6 * (int64_t)nsteps + nsample;   // six kernels a step, plus the sum on sample steps
+        e->launches += g->launches;
         e->cur = (nsteps % 2) ? 1 - parity : parity;
     } else {
         const int rc = queue_all();
@@ -1169,12 +1224,12 @@ static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, doubl
     const int c = e->cur;
     if (e->precision == DPD_PRECISION_FP64)
         k_download<double><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
+            n, e->d_boxes, e->d_tf[c], e->d_bid[c], e->d_x[c], e->d_v[c], (const double*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
             e->sampled ? (const double*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     else
         k_download<float><<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(
-            n, e->d_boxes, e->d_tf[c], e->d_slot_of, e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
+            n, e->d_boxes, e->d_tf[c], e->d_bid[c], e->d_x[c], e->d_v[c], (const float*)e->d_F, e->d_img[c], e->off_active ? e->d_off : nullptr,
             e->sampled ? (const float*)e->d_stress : nullptr, e->d_cell[c], ox, ou, ov, of, ost,
             cell ? e->d_out_cell : nullptr);
     int rc = check_launch(e, "k_download");

@@ -92,11 +92,97 @@ __device__ __forceinline__ int real_bits(double v) { return (int)__double_as_lon
 
 // ------------------------------------------------------------- UpdatePos
 
-// Drift and cell migration of every bead (CCNTCell::UpdatePos).  The
-// reference's 27-way decision tree moves a bead by one cell along each axis
-// where x > TR (+1) or x < BL (-1), TR = BL + w with BL = ix*w
-// (CNTCell.cpp:598-604, 1768-2254), wrapping the moved coordinates only when
-// both cells lie on the box boundary.  Frozen beads keep their cell.
+// One bead's drift and cell move; returns its new cell and writes x, img and
+// cell of slot s.  x0, v0, f0 are the bead's position, velocity and force.
+__device__ __forceinline__ int drift_and_move(const StepConst* __restrict__ K, const Box* __restrict__ boxes,
+                                              int n, int s, int c, int tfl, const double x0[3], const double v0[3],
+                                              const double f0[3], uint32_t im0, double* __restrict__ x,
+                                              uint32_t* __restrict__ img, int* __restrict__ cell, unsigned& bad)
+{
+    if (flag_frozen(tfl)) return c;
+    int cnew = c;
+    const double dt = K->dt, h2 = K->halfdt2;
+    const Box& B = boxes[flag_box(tfl)];
+    const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
+    const int cl = c - B.cell_base;
+    int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
+    const bool ext = ci[0] == 0 || ci[0] == nx - 1 || ci[1] == 0 || ci[1] == ny - 1 ||
+                     ci[2] == 0 || ci[2] == nz - 1;
+    double xn[3];
+    int mv[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        // x += dt*v + dt^2/2*F with the reference's rounding (no fused multiply-add)
+        const double dx = __dadd_rn(__dmul_rn(dt, v0[d]), __dmul_rn(h2, f0[d]));
+        xn[d] = __dadd_rn(x0[d], dx);
+        const double BL = __dmul_rn((double)ci[d], B.w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
+        const double TR = __dadd_rn(BL, B.w[d]);
+        mv[d] = (xn[d] > TR) ? 1 : ((xn[d] < BL) ? -1 : 0);
+    }
+    uint32_t im = im0;
+    if (mv[0] | mv[1] | mv[2]) {
+        int nci[3];
+        for (int d = 0; d < 3; ++d) {
+            nci[d] = ci[d] + mv[d];
+            if (nci[d] < 0) nci[d] += B.nc[d];
+            else if (nci[d] >= B.nc[d]) nci[d] -= B.nc[d];
+        }
+        const bool next = nci[0] == 0 || nci[0] == nx - 1 || nci[1] == 0 || nci[1] == ny - 1 ||
+                          nci[2] == 0 || nci[2] == nz - 1;
+        if (ext && next) {
+            int ii[3] = {img_get(im, 0), img_get(im, 1), img_get(im, 2)};
+            for (int d = 0; d < 3; ++d) {
+                if (mv[d] > 0 && xn[d] > B.L[d]) { xn[d] -= B.L[d]; ++ii[d]; }
+                else if (mv[d] < 0 && xn[d] < 0.0) { xn[d] += B.L[d]; --ii[d]; }
+                if (ii[d] < -511 || ii[d] > 511) bad |= 0x4u;
+            }
+            im = img_pack(ii[0], ii[1], ii[2]);
+        }
+        cnew = B.cell_base + nci[0] + nx * (nci[1] + ny * nci[2]);
+    }
+    // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650)
+    const long long ax = (long long)(xn[0] / B.w[0]);
+    const long long ay = (long long)(xn[1] / B.w[1]);
+    const long long az = (long long)(xn[2] / B.w[2]);
+    if (B.cell_base + (long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!isfinite(xn[d])) bad |= 0x2u;
+        x[d * n + s] = xn[d];
+    }
+    img[s] = im;
+    cell[s] = cnew;
+    return cnew;
+}
+
+// Warp-aggregated counting of the beads arriving in each cell: lanes bound
+// for the same cell take one atomic (beads are cell-sorted, so a warp spans
+// ~11 cells) and ranks follow lane order inside the group; one atomic per scan
+// chunk per warp as well.  Called by every lane of the warp.
+__device__ __forceinline__ void count_arrival(bool live, int s, int cnew, int* __restrict__ rank,
+                                              int* __restrict__ count, int* __restrict__ block_count)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (live) {
+        const int lane = threadIdx.x & 31;
+        const unsigned peers = __match_any_sync(act, cnew);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&count[cnew], __popc(peers));
+        base = __shfl_sync(act, base, leader);
+        rank[s] = base + __popc(peers & ((1u << lane) - 1u));
+        const int chunk = cnew / kScanChunk;
+        const unsigned cpeers = __match_any_sync(act, chunk);
+        if (lane == __ffs(cpeers) - 1) atomicAdd(&block_count[chunk], __popc(cpeers));   // result unused: a reduction
+    }
+}
+
+// Drift and cell migration of every bead (CCNTCell::UpdatePos) for the first
+// step of a call; later steps run it fused into k_update_mom of the step
+// before.  The reference's 27-way decision tree moves a bead by one cell
+// along each axis where x > TR (+1) or x < BL (-1), TR = BL + w with
+// BL = ix*w (CNTCell.cpp:598-604, 1768-2254), wrapping the moved coordinates
+// only when both cells lie on the box boundary.  Frozen beads keep their cell.
 template <typename real>
 __global__ void __launch_bounds__(256, 6) k_update_pos(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, double* __restrict__ x,
@@ -121,77 +207,9 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
             f0[d] = (double)F[d * n + s];
         }
         const uint32_t im0 = img[s];
-        cnew = c;
-        if (!flag_frozen(tfl)) {
-            const double dt = K->dt, h2 = K->halfdt2;
-            const Box& B = boxes[flag_box(tfl)];
-            const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
-            const int cl = c - B.cell_base;
-            int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
-            const bool ext = ci[0] == 0 || ci[0] == nx - 1 || ci[1] == 0 || ci[1] == ny - 1 ||
-                             ci[2] == 0 || ci[2] == nz - 1;
-            double xn[3];
-            int mv[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                // x += dt*v + dt^2/2*F with the reference's rounding (no fused multiply-add)
-                const double dx = __dadd_rn(__dmul_rn(dt, v0[d]), __dmul_rn(h2, f0[d]));
-                xn[d] = __dadd_rn(x0[d], dx);
-                const double BL = __dmul_rn((double)ci[d], B.w[d]);   // CCNTCell ctor, CNTCell.cpp:598-604
-                const double TR = __dadd_rn(BL, B.w[d]);
-                mv[d] = (xn[d] > TR) ? 1 : ((xn[d] < BL) ? -1 : 0);
-            }
-            uint32_t im = im0;
-            if (mv[0] | mv[1] | mv[2]) {
-                int nci[3];
-                for (int d = 0; d < 3; ++d) {
-                    nci[d] = ci[d] + mv[d];
-                    if (nci[d] < 0) nci[d] += B.nc[d];
-                    else if (nci[d] >= B.nc[d]) nci[d] -= B.nc[d];
-                }
-                const bool next = nci[0] == 0 || nci[0] == nx - 1 || nci[1] == 0 || nci[1] == ny - 1 ||
-                                  nci[2] == 0 || nci[2] == nz - 1;
-                if (ext && next) {
-                    int ii[3] = {img_get(im, 0), img_get(im, 1), img_get(im, 2)};
-                    for (int d = 0; d < 3; ++d) {
-                        if (mv[d] > 0 && xn[d] > B.L[d]) { xn[d] -= B.L[d]; ++ii[d]; }
-                        else if (mv[d] < 0 && xn[d] < 0.0) { xn[d] += B.L[d]; --ii[d]; }
-                        if (ii[d] < -511 || ii[d] > 511) bad |= 0x4u;
-                    }
-                    im = img_pack(ii[0], ii[1], ii[2]);
-                }
-                cnew = B.cell_base + nci[0] + nx * (nci[1] + ny * nci[2]);
-            }
-            // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650)
-            const long long ax = (long long)(xn[0] / B.w[0]);
-            const long long ay = (long long)(xn[1] / B.w[1]);
-            const long long az = (long long)(xn[2] / B.w[2]);
-            if (B.cell_base + (long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if (!isfinite(xn[d])) bad |= 0x2u;
-                x[d * n + s] = xn[d];
-            }
-            img[s] = im;
-            cell[s] = cnew;
-        }
+        cnew = drift_and_move(K, boxes, n, s, c, tfl, x0, v0, f0, im0, x, img, cell, bad);
     }
-    // Warp-aggregated counting: lanes bound for the same cell take one atomic
-    // (beads are cell-sorted, so a warp spans ~11 cells) and ranks follow lane
-    // order inside the group; one atomic per scan chunk per warp as well.
-    const unsigned act = __ballot_sync(0xffffffffu, live);
-    if (live) {
-        const int lane = threadIdx.x & 31;
-        const unsigned peers = __match_any_sync(act, cnew);
-        const int leader = __ffs(peers) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&count[cnew], __popc(peers));
-        base = __shfl_sync(act, base, leader);
-        rank[s] = base + __popc(peers & ((1u << lane) - 1u));
-        const int chunk = cnew / kScanChunk;
-        const unsigned cpeers = __match_any_sync(act, chunk);
-        if (lane == __ffs(cpeers) - 1) atomicAdd(&block_count[chunk], __popc(cpeers));   // result unused: a reduction
-    }
+    count_arrival(live, s, cnew, rank, count, block_count);
     if (bad) atomicOr(status, bad);
 }
 
@@ -276,9 +294,9 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     const int* __restrict__ bid_in, const int* __restrict__ tf_in, const uint32_t* __restrict__ img_in,
     const int* __restrict__ cell_in, double* __restrict__ x_out, double* __restrict__ v_out,
     real* __restrict__ Fold_out, int* __restrict__ bid_out, int* __restrict__ tf_out,
-    uint32_t* __restrict__ img_out, int* __restrict__ cell_out, int* __restrict__ slot_of,
-    const int* __restrict__ pid_of, typename Vec4<real>::type* __restrict__ pos4,
-    typename Vec4<real>::type* __restrict__ vel4)
+    uint32_t* __restrict__ img_out, int* __restrict__ cell_out, const int* __restrict__ pid_in,
+    int* __restrict__ pid_out, typename Vec4<real>::type* __restrict__ pos4,
+    typename Vec4<real>::type* __restrict__ vel4, double4* __restrict__ ubuf, const double* __restrict__ off)
 {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
@@ -289,6 +307,7 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     const int b = bid_in[s];
     const int tfl = tf_in[s];
     const uint32_t im = img_in[s];
+    const int pid = pid_in[s];
     double xs[3], vs[3];
     real fs[3];
 #pragma unroll
@@ -322,13 +341,21 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     tf_out[o] = tfl;
     img_out[o] = im;
     cell_out[o] = c;
-    slot_of[b] = o;
+    pid_out[o] = pid;
     typedef typename Vec4<real>::type V4;
     V4 p, w;
     p.x = rel[0]; p.y = rel[1]; p.z = rel[2]; p.w = as_real_bits(tfl & kShadowMask, real(0));
-    w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid_of[b], real(0));
+    w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid, real(0));
     pos4[o] = p;
     vel4[o] = w;
+    if (flag_bonded(tfl)) {
+        // unPBC position (x + image*L + upload offset) for the bonded terms,
+        // stored by upload index: chain partners sit in the same lines
+        double u[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) u[q] = xs[q] + (double)img_get(im, q) * B.L[q] + (off ? off[q * n + b] : 0.0);
+        ubuf[b] = make_double4(u[0], u[1], u[2], 0.0);
+    }
 }
 
 // ------------------------------------------------------------ pair forces
@@ -458,58 +485,36 @@ struct Topology {
     const double* ang_k3;
     const double* ang_cos0; // cos(phi0); 1 when phi0 <= 0
     const double* ang_sin0; // sin(phi0); exactly 0 when phi0 <= 0 (the k3/|b1||b2| branch)
-    const double* off;      // unPBC - (x + img*L) at upload, 3 planes by upload index, or null
+    const double4* ubuf;    // unPBC position by upload index, written by k_gather for bonded beads
 };
 
 enum TermCode { kBondHead = 0, kBondTail = 1, kAngle0 = 2, kAngle1 = 3, kAngle2 = 4 };
 
-__device__ __forceinline__ void unwrapped(const Box& B, const double* __restrict__ x,
-                                          const uint32_t* __restrict__ img, const double* __restrict__ off,
-                                          int n, int nb_total, int slot, int b, double u[3])
+__device__ __forceinline__ void unwrapped(const double4* __restrict__ ubuf, int b, double u[3])
 {
-    const uint32_t im = img[slot];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        u[d] = x[d * n + slot] + (double)img_get(im, d) * B.L[d];
-        if (off) u[d] += off[d * nb_total + b];
-    }
+    const double4 q = ubuf[b];
+    u[0] = q.x;
+    u[1] = q.y;
+    u[2] = q.z;
 }
 
-// Bond and bond-pair forces gathered per bead (each bond is evaluated by both
-// of its beads and each bond pair by its three beads, so no atomics), then the
-// velocity update of CCNTCell::UpdateMom: v = v_old + dt/2 (F + F_old) for
-// movable beads.  Non-movable beads keep v and, as in the reference (whose
-// UpdatePos skips them), keep accumulating force.  On sample steps the FP64
-// single-bead sums are reduced per block.
-template <typename real, bool SAMPLE>
-__global__ void __launch_bounds__(256, 4) k_update_mom(
-    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, int64_t* __restrict__ step_ptr,
-    const double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
-    const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
-    const uint32_t* __restrict__ img, const int* __restrict__ slot_of, Topology topo,
-    real* __restrict__ stress, double* __restrict__ partials, unsigned* __restrict__ status)
+// Bond and bond-pair forces of one bonded bead each, in upload order (chains
+// are contiguous there, so the partners' positions and the term tables are
+// read as whole lines), FP64 in both precision modes: the bond-pair force
+// with phi0 > 0 divides by sqrt(1/cos^2 - 1), which FP32 cannot resolve for
+// nearly straight chains.  Each bond is evaluated by both of its beads and
+// each bond pair by its three beads, so no atomics.  Writes the bonded force
+// (and on sample steps the bond virial of the head bead) by upload index.
+template <bool SAMPLE>
+__global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __restrict__ bb, Topology topo,
+                                               double4* __restrict__ Fb, double* __restrict__ Sb)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    double acc[kObsTerms];
-#pragma unroll
-    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
-    if (s < n) {
-        const int b = bid[s];
-        const int tfl = tf[s];
-        const bool frozen = flag_frozen(tfl);
-        real f[3] = {F[s], F[n + s], F[2 * n + s]};
-        real fo[3] = {Fold[s], Fold[n + s], Fold[2 * n + s]};
-        const double v0[3] = {v[s], v[n + s], v[2 * n + s]};
-        if (frozen) { f[0] += fo[0]; f[1] += fo[1]; f[2] += fo[2]; }
-        // Bonded terms in FP64 in both precision modes: only bonded beads pay
-        // for it, and the bond-pair force with phi0 > 0 divides by
-        // sqrt(1/cos^2 - 1), which FP32 cannot resolve for nearly straight
-        // chains.  The sum is rounded once into the force accumulator.
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nbb) {
+        const int b = bb[k];
         double bf[3] = {0.0, 0.0, 0.0};
         double bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const bool bonded = flag_bonded(tfl);
-        const Box& B = boxes[flag_box(tfl)];
-        const int t0 = bonded ? topo.csr_ptr[b] : 0, t1 = bonded ? topo.csr_ptr[b + 1] : 0;
+        const int t0 = topo.csr_ptr[b], t1 = topo.csr_ptr[b + 1];
         for (int t = t0; t < t1; ++t) {
             const int term = topo.csr_term[t];
             const int code = term & 7, idx = term >> 3;
@@ -517,8 +522,8 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 // CBond::AddForce, Bond.cpp:123-160 (serial build: unPBC coordinates)
                 const int h = topo.bond_h[idx], tl = topo.bond_t[idx];
                 double uh[3], ut[3];
-                unwrapped(B, x, img, topo.off, n, n, slot_of[h], h, uh);
-                unwrapped(B, x, img, topo.off, n, n, slot_of[tl], tl, ut);
+                unwrapped(topo.ubuf, h, uh);
+                unwrapped(topo.ubuf, tl, ut);
                 const double bx = uh[0] - ut[0], by = uh[1] - ut[1], bz = uh[2] - ut[2];
                 const double len = sqrt(bx * bx + by * by + bz * bz);
                 const double k2 = topo.bond_k2[idx], l0 = topo.bond_l0[idx];
@@ -540,10 +545,10 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 double u1h[3], u1t[3], u2h[3], u2t[3];
                 const int a1h = topo.ang_b1h[idx], a1t = topo.ang_b1t[idx];
                 const int a2h = topo.ang_b2h[idx], a2t = topo.ang_b2t[idx];
-                unwrapped(B, x, img, topo.off, n, n, slot_of[a1h], a1h, u1h);
-                unwrapped(B, x, img, topo.off, n, n, slot_of[a1t], a1t, u1t);
-                unwrapped(B, x, img, topo.off, n, n, slot_of[a2h], a2h, u2h);
-                unwrapped(B, x, img, topo.off, n, n, slot_of[a2t], a2t, u2t);
+                unwrapped(topo.ubuf, a1h, u1h);
+                unwrapped(topo.ubuf, a1t, u1t);
+                unwrapped(topo.ubuf, a2h, u2h);
+                unwrapped(topo.ubuf, a2t, u2t);
                 double b1[3], b2[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -574,6 +579,69 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 }
             }
         }
+        Fb[b] = make_double4(bf[0], bf[1], bf[2], 0.0);
+        if (SAMPLE) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Sb[(size_t)q * n + b] = bs[q];
+        }
+    }
+}
+
+// The bonded force of k_bonds added per bead, then the velocity update of
+// CCNTCell::UpdateMom: v = v_old + dt/2 (F + F_old) for movable beads.
+// Non-movable beads keep v and, as in the reference (whose UpdatePos skips
+// them), keep accumulating force.  On sample steps the FP64 single-bead sums
+// are reduced per block.  With POS the same thread goes on with the next
+// step's UpdatePos (drift, cell move, arrival counts), which saves a launch
+// and a second pass over x, v, F and the flags.
+template <typename real, bool SAMPLE, bool POS>
+__global__ void __launch_bounds__(256, 4) k_update_mom(
+    int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, int64_t* __restrict__ step_ptr,
+    double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
+    const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
+    const double4* __restrict__ Fb, const double* __restrict__ Sb,
+    real* __restrict__ stress, double* __restrict__ partials, uint32_t* __restrict__ img, int* __restrict__ cell,
+    int* __restrict__ rank, int* __restrict__ count, int* __restrict__ block_count, unsigned* __restrict__ status)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = s < n;
+    double acc[kObsTerms];
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
+    int cnew = 0;
+    unsigned bad = 0;
+    if (live) {
+        const int b = bid[s];
+        const int tfl = tf[s];
+        const bool frozen = flag_frozen(tfl);
+        real f[3] = {F[s], F[n + s], F[2 * n + s]};
+        real fo[3] = {Fold[s], Fold[n + s], Fold[2 * n + s]};
+        const double v0[3] = {v[s], v[n + s], v[2 * n + s]};
+        double xs[3] = {0.0, 0.0, 0.0};
+        int c = 0;
+        uint32_t im0 = 0;
+        if (SAMPLE || POS) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) xs[d] = x[d * n + s];
+        }
+        if (POS) {
+            c = cell[s];
+            im0 = img[s];
+        }
+        if (frozen) { f[0] += fo[0]; f[1] += fo[1]; f[2] += fo[2]; }
+        // Bonded terms (k_bonds, FP64) are added once, rounded into the
+        // force accumulator.
+        double bf[3] = {0.0, 0.0, 0.0};
+        double bs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const bool bonded = flag_bonded(tfl);
+        if (bonded) {
+            const double4 g = Fb[b];
+            bf[0] = g.x; bf[1] = g.y; bf[2] = g.z;
+            if (SAMPLE) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) bs[q] = Sb[(size_t)q * n + b];
+            }
+        }
         if (bonded) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) f[d] = (real)((double)f[d] + bf[d]);
@@ -581,8 +649,7 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
         F[s] = f[0];
         F[n + s] = f[1];
         F[2 * n + s] = f[2];
-        if (!isfinite((double)f[0]) || !isfinite((double)f[1]) || !isfinite((double)f[2]))
-            atomicOr(status, 0x2u);
+        if (!isfinite((double)f[0]) || !isfinite((double)f[1]) || !isfinite((double)f[2])) bad |= 0x2u;
         double vn[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -592,8 +659,12 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
                 v[d * n + s] = vn[d];
             }
         }
+        if (POS) {
+            // UpdatePos of the next step (the drift uses this step's v and F)
+            const double f0[3] = {(double)f[0], (double)f[1], (double)f[2]};
+            cnew = drift_and_move(K, boxes, n, s, c, tfl, xs, vn, f0, im0, x, img, cell, bad);
+        }
         if (SAMPLE) {
-            const double xs[3] = {x[s], x[n + s], x[2 * n + s]};
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
                 const real st = (real)((double)stress[q * n + s] + bs[q]);
@@ -625,20 +696,36 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
         if (threadIdx.x < kObsTerms) {
             double a = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w][threadIdx.x];
-            partials[blockIdx.x * kObsTerms + threadIdx.x] = a;
+            partials[threadIdx.x * gridDim.x + blockIdx.x] = a;   // term-major
         }
     }
+    if (POS) count_arrival(live, s, cnew, rank, count, block_count);
+    if (bad) atomicOr(status, bad);
     if (s == 0) *step_ptr += 1;
 }
 
+// Sets the step counter that keys the pair noise (a launch argument, so the
+// host queues it without waiting for earlier work).
+static __global__ void k_set_step(int64_t* __restrict__ step_ptr, int64_t value) { *step_ptr = value; }
+
 // Fixed-order sum of the per-block partials (deterministic): one warp per
-// term, a fixed strided split and a fixed shuffle tree.
+// term, coalesced reads of the term-major partials into four running sums per
+// lane, then a fixed shuffle tree.
 static __global__ void __launch_bounds__(32 * kObsTerms) k_reduce_obs(int nblocks, const double* __restrict__ partials,
                                                                        double* __restrict__ out)
 {
     const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double a = 0.0;
-    for (int b = lane; b < nblocks; b += 32) a += partials[b * kObsTerms + q];
+    const double* p = partials + (size_t)q * nblocks;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int b = lane;
+    for (; b + 96 < nblocks; b += 128) {
+        a0 += p[b];
+        a1 += p[b + 32];
+        a2 += p[b + 64];
+        a3 += p[b + 96];
+    }
+    for (; b < nblocks; b += 32) a0 += p[b];
+    double a = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     if (lane == 0) out[q] = a;
@@ -676,7 +763,7 @@ static __global__ void __launch_bounds__(256) k_kinetic_partials(int n, const do
     if (threadIdx.x < kObsTerms) {
         double a = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w][threadIdx.x];
-        partials[blockIdx.x * kObsTerms + threadIdx.x] = a;
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = a;   // term-major
     }
 }
 
@@ -685,16 +772,16 @@ static __global__ void __launch_bounds__(256) k_kinetic_partials(int n, const do
 // Slot order -> upload order, FP64, xyz interleaved; unPBC = x + img*L + off.
 template <typename real>
 __global__ void __launch_bounds__(256) k_download(
-    int n, const Box* __restrict__ boxes, const int* __restrict__ tf, const int* __restrict__ slot_of,
+    int n, const Box* __restrict__ boxes, const int* __restrict__ tf, const int* __restrict__ bid,
     const double* __restrict__ x,
     const double* __restrict__ v, const real* __restrict__ F, const uint32_t* __restrict__ img,
     const double* __restrict__ off, const real* __restrict__ stress, const int* __restrict__ cell,
     double* __restrict__ ox, double* __restrict__ ou, double* __restrict__ ov, double* __restrict__ of,
     double* __restrict__ ost, int* __restrict__ ocell)
 {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n) return;
-    const int s = slot_of[b];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int b = bid[s];
     const uint32_t im = img[s];
     const Box& B = boxes[flag_box(tf[s])];
 #pragma unroll

@@ -39,7 +39,7 @@ EXPORTED = [
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
-                "reduce_obs", "download", "kinetic"]
+                "reduce_obs", "download", "kinetic", "bonds"]
 
 
 class DpdParams(C.Structure):
