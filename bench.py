@@ -180,10 +180,12 @@ def tune_candidates(reproducible: bool):
     from osprey_dpd_b200 import autotune
     if reproducible:
         return autotune.DEFAULT_CANDIDATES
-    return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES
+    return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES + autotune.STAGED_CANDIDATES
 
 
-FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1)}
+FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1), "staged": (16, 0, 100, 2)}
+SCHEME_NAMES = {0: "full", 1: "half", 2: "staged"}
+PAIR_KERNELS = {"full": "k_pair_forces", "half": "k_pair_forces_half", "staged": "k_pair_forces_staged"}
 
 
 def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False,
@@ -201,8 +203,13 @@ def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, r
     return autotune.tune(make, sig, tune_candidates(reproducible), steps=10, reps=2)
 
 
+def scheme_of(shape) -> str:
+    return SCHEME_NAMES[shape[3]] if shape and len(shape) > 3 else "full"
+
+
 def pair_scheme_name(shape) -> str:
-    return "half shell (atomics)" if shape and len(shape) > 3 and shape[3] == 1 else "full shell (reproducible)"
+    return {"full": "full shell (reproducible)", "half": "half shell (atomics)",
+            "staged": "half shell staged in shared memory (atomics)"}[scheme_of(shape)]
 
 
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
@@ -383,7 +390,7 @@ def run_replica_sweep(args, dev, torch, E):
 
 
 def read_traffic(n_beads: int, scheme: str = "full"):
-    """Per-launch DRAM bytes of the pair kernel (full or half shell) from the
+    """Per-launch DRAM bytes of the pair kernel (full, half or staged) from the
     committed ncu summary, scaled to the bead count."""
     p = os.path.join(ROOT, "profiles", "pair_forces_traffic.json")
     if not os.path.exists(p):
@@ -410,7 +417,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
     ap.add_argument("--reproducible", action="store_true",
                     help="tune over the full-shell (bitwise reproducible) pair scheme only")
-    ap.add_argument("--pair-scheme", choices=["auto", "full", "half"], default="auto",
+    ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged"], default="auto",
                     help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     args = ap.parse_args()
@@ -503,7 +510,7 @@ def main():
         return 0
 
     mixed = results.get("mixed") or results["fp64"]
-    half = bool(mixed["shape"] and len(mixed["shape"]) > 3 and mixed["shape"][3] == 1)
+    scheme = scheme_of(mixed["shape"])
     pair = mixed["prof"]["pair_forces"]
     t_pair = pair["ms"] / max(pair["launches"], 1) / 1000.0
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -524,7 +531,7 @@ def main():
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
         "fp64": ({"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["total_ms"] / args.steps,
                   "mixed_over_fp64": mixed["value"] / results["fp64"]["value"]} if "fp64" in results else None),
-        "roofline": {"bound": "issue", "kernel": ("k_pair_forces_half" if half else "k_pair_forces") + " (mixed)",
+        "roofline": {"bound": "issue", "kernel": PAIR_KERNELS[scheme] + " (mixed)",
                      "achieved": achieved / 1e9, "peak": issue_peak / 1e9, "unit": "Gslot/s",
                      "frac": achieved / issue_peak,
                      "peak_basis": f"{sms} SMs x 128 FP32/INT32 lanes x {sm_max:.0f} MHz ({peak_kind} sm_max_mhz)",
@@ -532,7 +539,7 @@ def main():
                      "avg_launch_ms": t_pair * 1000.0,
                      "timing": "CUDA events around every kernel on the engine's stream, in a 20-step pass "
                                "after the timed region (same engine and workload, kernels launched one by one)",
-                     "traffic": read_traffic(system.n, "half" if half else "full")},
+                     "traffic": read_traffic(system.n, scheme)},
         "roofline_step_hbm": {"bound": "hbm", "achieved": hbm_ach / 1e9, "peak": float(peaks["hbm_gbs"]),
                               "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),
                               "bytes_per_bead_step": ALG_BYTES_PER_BEAD_STEP["mixed"], "basis": peak_kind},

@@ -175,6 +175,10 @@ DPD_API int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t p
  * the pair.  No counterpart in the reference's interface. */
 #define DPD_PAIR_FULL_SHELL 0
 #define DPD_PAIR_HALF_SHELL 1
+/* DPD_PAIR_STAGED: the half-shell pair set with each 128-bead tile's
+ * neighbour rows staged in shared memory; same accuracy and run-to-run
+ * variation as DPD_PAIR_HALF_SHELL (slower on a B200: kept for comparison). */
+#define DPD_PAIR_STAGED     2
 DPD_API int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme);
 
 /* Waits for queued work; returns the device status bits seen so far. */

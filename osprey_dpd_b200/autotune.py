@@ -26,6 +26,8 @@ DEFAULT_CANDIDATES: Tuple[Shape, ...] = (
 HALF_SHELL_CANDIDATES: Tuple[Shape, ...] = (
     (32, 0, -1, 1), (24, 0, -1, 1), (32, 0, 100, 1), (24, 0, 100, 1), (40, 0, 100, 1),
 )
+# staged half-shell shape (pair scheme 2): smaller hit lists leave room for the staged rows
+STAGED_CANDIDATES: Tuple[Shape, ...] = ((16, 0, 100, 2),)
 CACHE = os.environ.get("DPD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "osprey_dpd_b200",
                                                        "launch_shapes.json"))
 

@@ -19,6 +19,7 @@
 
 #include "dpd_kernels.cuh"
 #include "pair_forces.cuh"
+#include "pair_staged.cuh"
 
 using namespace dpd;
 
@@ -147,7 +148,7 @@ struct dpd_engine {
     int pair_hitcap = 32;
     int pair_bps = 0;          // resident blocks per SM for the persistent grid
     int pair_carveout = -1;    // preferred shared-memory carveout in percent, -1 = driver default
-    bool pair_half = false;    // half-shell pair kernel (atomics, not bitwise reproducible)
+    int pair_scheme = DPD_PAIR_FULL_SHELL;   // DPD_PAIR_*: full shell (reproducible), half shell, staged half shell
     bool pair_attr_set[2][2] = {{false, false}, {false, false}};   // [fp64][sample]; one box kind per engine
 };
 
@@ -336,15 +337,27 @@ struct Timed {
     }
 };
 
-// The pair kernel variant for (box table, sample step, half shell).
+// The pair kernel variant for (box table, sample step, pair scheme).
 template <typename real>
-auto pair_kernel(bool multi, bool sample, bool half)
+auto pair_kernel(bool multi, bool sample, int scheme)
 {
-    if (half)
+    if (scheme == DPD_PAIR_STAGED)
+        return multi ? (sample ? k_pair_forces_staged<real, true, true> : k_pair_forces_staged<real, false, true>)
+                     : (sample ? k_pair_forces_staged<real, true, false> : k_pair_forces_staged<real, false, false>);
+    if (scheme == DPD_PAIR_HALF_SHELL)
         return multi ? (sample ? k_pair_forces_half<real, true, true> : k_pair_forces_half<real, false, true>)
                      : (sample ? k_pair_forces_half<real, true, false> : k_pair_forces_half<real, false, false>);
     return multi ? (sample ? k_pair_forces<real, true, true> : k_pair_forces<real, false, true>)
                  : (sample ? k_pair_forces<real, true, false> : k_pair_forces<real, false, false>);
+}
+
+// Dynamic shared memory of the engine's pair kernel.
+template <typename real>
+size_t pair_dyn_bytes(const dpd_engine* e, bool multi)
+{
+    if (e->pair_scheme == DPD_PAIR_STAGED) return StgLayout<real>(e->ntypes, e->pair_hitcap, multi).total;
+    if (e->pair_scheme == DPD_PAIR_HALF_SHELL) return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+    return pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
 }
 
 // Dynamic shared memory and carveout of the pair kernel's variants (outside
@@ -356,8 +369,8 @@ int set_pair_attributes(dpd_engine* e)
     const int pv = sizeof(real) == 8 ? 1 : 0;
     for (int sv = 0; sv < 2; ++sv) {
         if (e->pair_attr_set[pv][sv]) continue;
-        auto kern = pair_kernel<real>(multi, sv != 0, e->pair_half);
-        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+        auto kern = pair_kernel<real>(multi, sv != 0, e->pair_scheme);
+        const size_t dyn = pair_dyn_bytes<real>(e, multi);
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         if (e->pair_carveout >= 0)
             CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, e->pair_carveout));
@@ -431,11 +444,14 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     }
     {
         const bool multi = e->hboxes.size() > 1;
-        auto kern = pair_kernel<real>(multi, sample, e->pair_half);
-        const size_t dyn = pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+        auto kern = pair_kernel<real>(multi, sample, e->pair_scheme);
+        const size_t dyn = pair_dyn_bytes<real>(e, multi);
         if ((rc = set_pair_attributes<real>(e))) return rc;
         // the half shell accumulates into F with atomics
-        if (e->pair_half) CU(cudaMemsetAsync(e->d_F, 0, (size_t)3 * n * sizeof(real), st));
+        if (e->pair_scheme != DPD_PAIR_FULL_SHELL) CU(cudaMemsetAsync(e->d_F, 0, (size_t)3 * n * sizeof(real), st));
+        // the half-shell kernels add each owner's pair virial in pieces
+        if (sample && e->pair_scheme != DPD_PAIR_FULL_SHELL)
+            CU(cudaMemsetAsync(e->d_stress, 0, (size_t)9 * n * sizeof(real), st));
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
@@ -469,9 +485,9 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     return DPD_OK;
 }
 
-// "hitcap=32,bps=8,carveout=50,half=1": pair-kernel hit-list capacity (8..64),
-// resident blocks per SM for its persistent grid, preferred shared-memory
-// carveout (%), half-shell kernel.
+// "hitcap=32,bps=8,carveout=50,half=1,scheme=2": pair-kernel hit-list
+// capacity (8..64), resident blocks per SM for its persistent grid, preferred
+// shared-memory carveout (%), half-shell kernel, pair scheme (DPD_PAIR_*).
 void parse_tuning(dpd_engine* e, const char* spec)
 {
     std::string str(spec);
@@ -487,7 +503,8 @@ void parse_tuning(dpd_engine* e, const char* spec)
             if (key == "hitcap") e->pair_hitcap = std::min(std::max(val, 8), (int)kHitCapMax);
             else if (key == "bps") e->pair_bps = std::max(val, 0);
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
-            else if (key == "half") e->pair_half = val != 0;
+            else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
+            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
         }
         pos = end + 1;
     }
@@ -689,10 +706,11 @@ int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persisten
 int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
 {
     if (!e) return DPD_E_ARG;
-    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL) return fail(e, DPD_E_ARG, "unknown pair scheme");
+    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED)
+        return fail(e, DPD_E_ARG, "unknown pair scheme");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
-    e->pair_half = scheme == DPD_PAIR_HALF_SHELL;
+    e->pair_scheme = scheme;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
     return DPD_OK;

@@ -1,24 +1,24 @@
-// pair_forces.cuh -- the engine's DPD pair-force kernel (CCNTCell::UpdateForce,
-// DPD branch, CNTCell.cpp:1103-1572) with warp-level hit compaction.
+// pair_forces.cuh -- the engine's DPD pair-force kernels (CCNTCell::UpdateForce,
+// DPD branch, CNTCell.cpp:1103-1572) with per-lane hit lists.
 //
-// Only ~15% of the candidates in the 27 neighbour cells lie inside the cut-off
-// (rho = 3: 81 candidates, 12.6 partners per bead), so evaluating the force
-// where the distance test passes would run the expensive body (sqrt, Philox,
-// ~80 instructions) with a few lanes active on almost every iteration.  The
-// kernel therefore splits the work in two phases inside each warp:
+// Only ~15% of the candidates in the neighbour cells lie inside the cut-off
+// (rho = 3: 81 candidates in the full shell, 12.6 partners per bead), so
+// evaluating the force where the distance test passes would run the expensive
+// body (sqrt, Philox, ~80 instructions) with a few lanes active on almost
+// every iteration.  The kernels therefore split the work in two phases:
 //
 //   test   : every lane owns one bead i (a slot in cell order) and walks its
-//            9 neighbour rows; a row (cells x-1, x, x+1 at fixed y', z') is one
+//            neighbour rows; a row (cells x-1, x, x+1 at fixed y', z') is one
 //            contiguous slot range in the cell-sorted layout, split in two
-//            only where it wraps around the x boundary.  Passing candidates are
-//            appended to a per-warp queue in shared memory (ballot + popc).
-//   force  : whenever 32 hits are queued, all 32 lanes evaluate one pair each
-//            and add the force to the owning lane's accumulator in shared
-//            memory.
-//
-// Every pair is evaluated from both sides (full shell), so bead i only ever
-// accumulates its own force: no global atomics, and the result depends only on
-// the cell-sorted order, which is deterministic.
+//            only where it wraps around the x boundary.  Passing candidates
+//            are appended to the lane's own list column in shared memory.
+//   force  : the listed pairs are evaluated.  Full shell (k_pair_forces):
+//            every lane walks its own list, every pair is evaluated from both
+//            sides, so bead i only accumulates its own force -- no atomics,
+//            and the result depends only on the deterministic cell-sorted
+//            order.  Half shell (k_pair_forces_half): every pair once, the
+//            warp's lists are cut into 32 equal runs so all lanes evaluate
+//            the same number of pairs, and forces are added with atomics.
 #pragma once
 #include "dpd_kernels.cuh"
 
@@ -27,16 +27,21 @@ namespace dpd {
 constexpr int kPairWarps = 4;
 constexpr int kPairBlock = 32 * kPairWarps;
 // Resident blocks per SM the pair kernels are compiled for: 8 (64 registers,
-// 32 warps) in FP32; the FP64 variants keep 6 to avoid spills.
-template <typename real> struct PairOcc { static constexpr int value = sizeof(real) == 4 ? 8 : 6; };
+// 32 warps) for one FP32 box; a replica batch (per-owner box tables) 7, and
+// the FP64 variants 5, to keep their register spills small.
+template <typename real, bool MULTI = false> struct PairOcc {
+    static constexpr int value = sizeof(real) == 8 ? 5 : (MULTI ? 7 : 8);
+};
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
 
 template <typename real> struct RealOps;
 template <> struct RealOps<float> {
     static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float rnd(float x) { return rintf(x); }
 };
 template <> struct RealOps<double> {
     static __device__ __forceinline__ double rsqrt(double x) { return 1.0 / sqrt(x); }
+    static __device__ __forceinline__ double rnd(double x) { return rint(x); }
 };
 
 // Dynamic shared memory of one block: pair tables, then the hit lists
@@ -142,7 +147,7 @@ __device__ __forceinline__ void row_segment(bool live, int seg, int rb, int cx, 
 // tables and noise key from the packed box table, tables are read through the
 // read-only cache.  Otherwise one box whose tables are staged in shared memory.
 template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kPairBlock, PairOcc<real>::value) k_pair_forces(
+__global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pair_forces(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
@@ -265,31 +270,147 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real>::value) k_pair_force
 
 // ------------------------------------------------------------ half shell
 
-// This lane's listed pairs, each evaluated once: the force goes to the lane's
-// own accumulator and, negated, to the partner through atomics.
-template <typename real, bool VIRIAL>
-__device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __restrict__ list,
-                                                     const typename Vec4<real>::type& pi,
-                                                     const typename Vec4<real>::type& vi, const real* __restrict__ T,
-                                                     int nt, real wx, real wy, real wz, const uint32_t* keys,
-                                                     const typename Vec4<real>::type* __restrict__ pos4,
-                                                     const typename Vec4<real>::type* __restrict__ vel4, real* acc,
-                                                     real* __restrict__ F, int n)
+// Per-warp scratch of the balanced force pass in shared memory: the home
+// beads' shadows (read by whichever lane evaluates their pairs) and the hit
+// counts with their exclusive prefix.
+template <typename real>
+struct HalfShared {
+    typename Vec4<real>::type* hpos;   // kPairBlock entries
+    typename Vec4<real>::type* hvel;   // kPairBlock entries
+    real* hxw;                         // kPairBlock entries (staged scheme only)
+    int* wcnt;                         // kPairBlock entries: hits of each thread
+    int* wexc;                         // kPairBlock entries: exclusive prefix inside the warp
+};
+
+// Hit-list entry formats of the two half-shell kernels.
+// Unstaged: candidate slot in bits 0..25, cell offsets + 1 (x, y, z) in 2-bit
+// fields at bits 26, 28, 30.  Staged: staged index in bits 0..11, window
+// (row offset, see stg_row_shift) in bits 12..14.
+__device__ __forceinline__ void stg_row_shift(int r, int& dy, int& dz)
+{
+    dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
+    dz = r >= 2 ? 1 : 0;
+}
+
+// Force phase of one warp for the half-shell schemes, called by all 32 lanes
+// with cnt = this lane's listed hits.  The warp's lists are read as one
+// owner-major sequence (lane 0's hits, then lane 1's, ...) cut into 32 equal
+// runs, one per lane, so every lane evaluates the same number of pairs
+// whatever the per-bead hit counts.  A lane keeps the partial force of its
+// current owner in registers and adds it to the owner's global force with
+// atomics when the owner changes (or the run ends); the partner's share is
+// added with atomics.  The pair force is CNTCell.cpp:1192-1220 with rc = 1:
+//   w = 1 - r; F = (a_ij w - gamma_ij w^2 (r.v)/r + sigma_ij w (0.5 - U)) r_vec / r
+// w0 holds the cell widths of a single-box engine; a replica batch (MULTI)
+// reloads widths, tables and noise key per owner.  F (and on sample steps
+// stress) must be zero before the kernel.
+template <typename real, bool VIRIAL, bool MULTI, bool STAGED>
+__device__ __forceinline__ void balanced_force_pass(
+    int cnt, const uint32_t* __restrict__ lists, const HalfShared<real>& sh,
+    const typename Vec4<real>::type* stg, int tile_base, const Box* __restrict__ boxes, const real* Tsh,
+    const real* __restrict__ tab, int nt, const uint32_t* keys0, const real* w0, int64_t step,
+    const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
+    real* __restrict__ F, real* __restrict__ stress, int n)
 {
     typedef typename Vec4<real>::type V4;
-    const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    const int ti = (real_bits(pi.w) & 0xFF) * nt;
-    const uint32_t idi = (uint32_t)real_bits(vi.w);
-    const int m2 = nt * nt;
-    for (int k = 0; k < trip; ++k) {
-        if (k < cnt) {
-            const uint32_t e = list[k * kPairBlock];
-            const int j = (int)(e & 0x03FFFFFFu);
-            const V4 pj = pos4[j];
+    const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
+    const int tot = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
+    if (tot == 0) return;
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    int* wcnt = sh.wcnt + wbase;
+    int* wexc = sh.wexc + wbase;
+    wcnt[lane] = cnt;
+    wexc[lane] = inc - cnt;
+    __syncwarp();
+    const int per = (tot + 31) >> 5;
+    int f = lane * per;
+    const int f1 = min(f + per, tot);
+    if (f < f1) {
+        // owner of entry f: the last lane whose exclusive offset is <= f
+        int o = 0;
+#pragma unroll
+        for (int s = 16; s; s >>= 1)
+            if (wexc[o + s] <= f) o += s;
+        int e = f - wexc[o], co = wcnt[o];
+        const int m2 = nt * nt;
+        V4 pi, vi;
+        real xwi = real(0), wx = w0[0], wy = w0[1], wz = w0[2], iw = STAGED ? real(1) / w0[0] : real(0);
+        int islot, ti;
+        uint32_t idi;
+        const real* T = Tsh;
+        uint32_t keys[10];
+        if (!MULTI) {
+#pragma unroll
+            for (int q = 0; q < 10; ++q) keys[q] = keys0[q];
+        }
+        auto load_owner = [&](int oo) {
+            const int to = wbase + oo;
+            pi = sh.hpos[to];
+            vi = sh.hvel[to];
+            if (STAGED) xwi = sh.hxw[to];
+            islot = tile_base + to;
+            ti = (real_bits(pi.w) & 0xFF) * nt;
+            idi = (uint32_t)real_bits(vi.w);
+            if (MULTI) {   // the owner's box: cell widths, pair tables, noise key
+                const Box& B = boxes[flag_box(real_bits(pi.w))];
+                wx = (real)B.w[0]; wy = (real)B.w[1]; wz = (real)B.w[2];
+                if (STAGED) iw = real(1) / wx;
+                T = tab + B.tab;
+                uint32_t k = philox_step_key(B.seed, step);
+#pragma unroll
+                for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
+            }
+        };
+        load_owner(o);
+        constexpr int NACC = VIRIAL ? 12 : 3;
+        real acc[NACC];
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) acc[q] = real(0);
+        for (; f < f1; ++f) {
+            if (e == co) {
+                atomicAdd(F + islot, acc[0]);
+                atomicAdd(F + n + islot, acc[1]);
+                atomicAdd(F + 2 * n + islot, acc[2]);
+                if (VIRIAL) {
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) atomicAdd(stress + q * n + islot, acc[3 + q]);
+                }
+#pragma unroll
+                for (int q = 0; q < NACC; ++q) acc[q] = real(0);
+                do { ++o; } while (o < 31 && wcnt[o] == 0);   // a later owner holds entry f, since f < tot
+                e = 0;
+                co = wcnt[o];
+                load_owner(o);
+            }
+            const uint32_t ent = lists[e * kPairBlock + wbase + o];
+            ++e;
+            int j;
+            real dx, dy, dz;
+            V4 pj;
+            if (STAGED) {
+                const V4 sj = stg[ent & 0xFFFu];
+                int dyi, dzi;
+                stg_row_shift((int)(ent >> 12), dyi, dzi);
+                j = real_bits(sj.w);
+                pj = pos4[j];
+                const real bx = pi.x - pj.x;
+                const real ox = RealOps<real>::rnd((bx - (xwi - sj.x)) * iw);   // cell x offset of j
+                dx = bx - ox * wx;
+                dy = (pi.y - pj.y) - (real)dyi * wy;
+                dz = (pi.z - pj.z) - (real)dzi * wz;
+            } else {
+                j = (int)(ent & 0x03FFFFFFu);
+                pj = pos4[j];
+                dx = (pi.x - pj.x) - (real)((int)((ent >> 26) & 3u) - 1) * wx;
+                dy = (pi.y - pj.y) - (real)((int)((ent >> 28) & 3u) - 1) * wy;
+                dz = (pi.z - pj.z) - (real)((int)(ent >> 30) - 1) * wz;
+            }
             const V4 vj = vel4[j];
-            const real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
-            const real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
-            const real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
             const real r2 = dx * dx + dy * dy + dz * dz;
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
@@ -299,13 +420,15 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
             uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
 #pragma unroll
             for (int q = 0; q < 10; ++q) {
-                const uint64_t prod = (uint64_t)0xD256D193u * c0;
+                const uint64_t prod = (uint64_t)0xD256D193u * c0;   // one wide multiply per round
                 c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
                 c1 = (uint32_t)prod;
             }
             const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
                              T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-            const real m = mag * inv;
+            // the staged test decides pairs at the cut-off from rounded
+            // window coordinates: re-apply the exact cut-off here
+            const real m = (!STAGED || (r2 < real(1) && r2 > real(1e-18))) ? mag * inv : real(0);
             const real gx = m * dx, gy = m * dy, gz = m * dz;
             acc[0] += gx; acc[1] += gy; acc[2] += gz;
             atomicAdd(F + j, -gx);
@@ -317,145 +440,190 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
                 acc[9] += dx * gz; acc[10] += dy * gz; acc[11] += dz * gz;
             }
         }
+        atomicAdd(F + islot, acc[0]);
+        atomicAdd(F + n + islot, acc[1]);
+        atomicAdd(F + 2 * n + islot, acc[2]);
+        if (VIRIAL) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) atomicAdd(stress + q * n + islot, acc[3 + q]);
+        }
     }
+    __syncwarp();   // every lane is done with the lists before they are refilled
 }
 
-// Half-shell variant: every pair once, as CCNTCell::UpdateForce visits them
-// (CNTCell.cpp:1103-1572, m_aIntNNCells): the beads after bead i in its own cell and the 13
-// cells of the half shell (dz = +1: all nine; dz = 0: dy = +1 row; dy = 0:
-// the cell at dx = +1).  In slot terms: own row [i+1, end of cell x+1), the
-// (dy=+1, dz=0) row and the three dz=+1 rows.  Half the distance tests and
-// force bodies of the full shell; the partner's share is added with global
-// atomics, so the FP32 summation order (and the last bits) vary from run to
-// run.  F must be zero on entry.  The pair virial goes whole to bead i, the
-// reference's convention (CNTCell.cpp:1283-1301).
+// Dynamic shared memory of k_pair_forces_half: pair tables (single box), hit
+// lists, then the balanced pass's per-thread scratch.
+template <typename real>
+__host__ __device__ constexpr size_t half_scratch_bytes()
+{
+    return (2 * 4 * sizeof(real) + 2 * sizeof(int)) * (size_t)kPairBlock;
+}
+template <typename real>
+__host__ __device__ constexpr size_t half_smem_bytes(int nt, int hitcap, bool multi)
+{
+    return pair_smem_bytes<real>(nt, hitcap, multi) + half_scratch_bytes<real>();
+}
+template <typename real>
+__device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
+{
+    typedef typename Vec4<real>::type V4;
+    HalfShared<real> sh;
+    sh.hpos = reinterpret_cast<V4*>(base);
+    sh.hvel = sh.hpos + kPairBlock;
+    sh.hxw = nullptr;
+    sh.wcnt = reinterpret_cast<int*>(sh.hvel + kPairBlock);
+    sh.wexc = sh.wcnt + kPairBlock;
+    return sh;
+}
+
+// Half-shell scheme: every pair once, over the beads after bead i in its own
+// cell and 13 neighbour cells (dz = +1: all nine; dz = 0: the dy = +1 row;
+// dz = dy = 0: the cell at dx = +1) -- one of the two symmetric halves of the
+// 26 neighbours, as CCNTCell::UpdateForce visits each pair once through its
+// m_aIntNNCells half shell (CNTCell.cpp:1103-1572).  In slot terms: own row
+// [i+1, end of cell x+1), the (dy=+1, dz=0) row and the three dz=+1 rows.
+// The partner's share is added with global atomics, so the FP32 summation
+// order (and the last bits) vary from run to run.  The pair virial goes whole
+// to bead i, the reference's convention (CNTCell.cpp:1283-1301).
+// One tile of kPairBlock slots; `lists` the block's hit lists (this thread's
+// column at lists + threadIdx.x), Tsh the staged pair tables (single box), sh
+// the balanced pass's scratch.  Called by every thread of the block for the
+// same tile.
 template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kPairBlock, PairOcc<real>::value) k_pair_forces_half(
+__device__ __forceinline__ void half_shell_tile(
+    int tile, int n, int nt, const Box* __restrict__ boxes, int64_t step, const real* __restrict__ tab,
+    const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
+    const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
+    real* __restrict__ F, real* __restrict__ stress, int hitcap, uint32_t* lists, const HalfShared<real>& sh,
+    const uint32_t* keys0)
+{
+    typedef typename Vec4<real>::type V4;
+    uint32_t* list = lists + threadIdx.x;
+    const int i = tile * kPairBlock + threadIdx.x;
+    const bool live = i < n;
+    V4 pi, vi;
+    int cx = 0, cy = 0, cz = 0;
+    if (live) {
+        pi = pos4[i];
+        vi = vel4[i];
+    } else {
+        pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
+    }
+    const Box& B = boxes[MULTI ? flag_box(real_bits(pi.w)) : 0];
+    const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
+    if (live) {
+        const int c = cell[i] - B.cell_base;
+        cx = c % nx;
+        cy = (c / nx) % ny;
+        cz = c / (nx * ny);
+    }
+    sh.hpos[threadIdx.x] = pi;
+    sh.hvel[threadIdx.x] = vi;
+    const real wx = (real)B.w[0], wy = (real)B.w[1], wz = (real)B.w[2];
+    const real w0[3] = {wx, wy, wz};   // the box of a single-box engine (MULTI reloads per owner)
+    const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
+    const int tile_base = tile * kPairBlock;
+    int cnt = 0;
+    __syncwarp();   // home shadows visible to the warp
+    for (int r = 0; r < 5; ++r) {
+        const int dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
+        const int dz = r < 2 ? 0 : 1;
+        int y2 = cy + dy, z2 = cz + dz;
+        y2 += (y2 >= ny) ? -ny : 0;
+        z2 += (z2 >= nz) ? -nz : 0;
+        y2 += (y2 < 0) ? ny : 0;
+        const int rb = B.cell_base + nx * (y2 + ny * z2);
+        const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
+        const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
+        for (int seg = 0; seg < 2; ++seg) {
+            int lo, hi, b1, b2;
+            if (r > 0) {
+                row_segment(live, seg, rb, cx, nx, start, lo, hi, b1, b2);
+            } else if (!live) {
+                lo = hi = b1 = b2 = 0;
+            } else if (cx < nx - 1) {
+                // own cell after i, then cell x+1 (offset +1 from b2)
+                if (seg == 0) { lo = b1 = i + 1; b2 = start[rb + cx + 1]; hi = start[rb + cx + 2]; }
+                else { lo = hi = b1 = b2 = 0; }
+            } else {
+                // cx = nx-1: own cell after i, then cell 0 across the boundary
+                if (seg == 0) { lo = b1 = i + 1; b2 = hi = start[rb + cx + 1]; }
+                else { lo = b1 = b2 = start[rb]; hi = start[rb + 1]; }
+            }
+            const int len = hi - lo;
+            const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+            // chunks of at most hitcap candidates, so a list can never overflow
+            for (int base = 0; base < trip; base += hitcap) {
+                const int clen = min(max(len - base, 0), hitcap);
+                if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
+                    balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh,
+                                                                    tab, nt, keys0, w0, step, pos4, vel4, F, stress,
+                                                                    n);
+                    cnt = 0;
+                }
+                const int tend = base + min(trip - base, hitcap);
+                // Four candidates per iteration: their loads are issued
+                // together, so four L1/L2 round trips overlap.  The bead
+                // itself (r2 = 0) fails r2 > 1e-18, the reference's dr > 1e-9
+                // test (CNTCell.cpp:1202), so no separate j != i test.
+                // cnt + clen <= hitcap holds here, so the stores stay in range.
+                for (int t = base; t < tend; t += 4) {
+                    V4 p[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (t + q < len && t + q < tend) p[q] = pos4[lo + t + q];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int jq = lo + t + q;
+                        if (t + q < len && t + q < tend) {
+                            const bool ge1 = jq >= b1, ge2 = jq >= b2;
+                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
+                            const real ddy = piy - p[q].y, ddz = piz - p[q].z;
+                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
+                                list[cnt * kPairBlock] = (uint32_t)jq | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
+                                ++cnt;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh, tab, nt, keys0,
+                                                    w0, step, pos4, vel4, F, stress, n);
+}
+
+// F must be zero on entry, and on sample steps (VIRIAL) the stress array too.
+template <typename real, bool VIRIAL, bool MULTI>
+__global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pair_forces_half(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
     unsigned* __restrict__ status)
 {
-    typedef typename Vec4<real>::type V4;
     extern __shared__ __align__(16) unsigned char pair_dyn[];
     const int nt = K->ntypes;
     real* Tsh = reinterpret_cast<real*>(pair_dyn);
-    uint32_t* list = reinterpret_cast<uint32_t*>(pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt))) + threadIdx.x;
+    unsigned char* lbase = pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt));
+    uint32_t* lists = reinterpret_cast<uint32_t*>(lbase);
+    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)hitcap * kPairBlock);
     if (!MULTI)
         for (int k = threadIdx.x; k < 3 * nt * nt; k += kPairBlock) Tsh[k] = tab[k];
     const int64_t step = *step_ptr;
+    uint32_t keys0[10];
+    {
+        uint32_t k = philox_step_key(boxes[0].seed, step);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) { keys0[q] = k; k += 0x9E3779B9u; }
+    }
     __syncthreads();   // tables
     const int tile0 = blockIdx.x * tiles_per_block;
     for (int tile = tile0; tile < tile0 + tiles_per_block; ++tile) {
-        const int i = tile * kPairBlock + threadIdx.x;
         if (tile * kPairBlock >= n) break;
-        const bool live = i < n;
-        V4 pi, vi;
-        int cx = 0, cy = 0, cz = 0;
-        if (live) {
-            pi = pos4[i];
-            vi = vel4[i];
-        } else {
-            pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
-        }
-        const Box& B = boxes[MULTI ? flag_box(real_bits(pi.w)) : 0];
-        const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
-        if (live) {
-            const int c = cell[i] - B.cell_base;
-            cx = c % nx;
-            cy = (c / nx) % ny;
-            cz = c / (nx * ny);
-        }
-        const real* T = MULTI ? tab + B.tab : Tsh;
-        uint32_t keys[10];
-        {
-            uint32_t k = philox_step_key(B.seed, step);
-#pragma unroll
-            for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
-        }
-        const real wx = (real)B.w[0], wy = (real)B.w[1], wz = (real)B.w[2];
-        const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
-        constexpr int NACC = VIRIAL ? 12 : 3;
-        real acc[NACC];
-#pragma unroll
-        for (int q = 0; q < NACC; ++q) acc[q] = real(0);
-        int cnt = 0;
-        for (int r = 0; r < 5; ++r) {
-            const int dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
-            const int dz = r < 2 ? 0 : 1;
-            int y2 = cy + dy, z2 = cz + dz;
-            y2 += (y2 >= ny) ? -ny : 0;
-            z2 += (z2 >= nz) ? -nz : 0;
-            y2 += (y2 < 0) ? ny : 0;
-            const int rb = B.cell_base + nx * (y2 + ny * z2);
-            const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
-            const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
-            for (int seg = 0; seg < 2; ++seg) {
-                int lo, hi, b1, b2;
-                if (r > 0) {
-                    row_segment(live, seg, rb, cx, nx, start, lo, hi, b1, b2);
-                } else if (!live) {
-                    lo = hi = b1 = b2 = 0;
-                } else if (cx < nx - 1) {
-                    // own cell after i, then cell x+1 (offset +1 from b2)
-                    if (seg == 0) { lo = b1 = i + 1; b2 = start[rb + cx + 1]; hi = start[rb + cx + 2]; }
-                    else { lo = hi = b1 = b2 = 0; }
-                } else {
-                    // cx = nx-1: own cell after i, then cell 0 across the boundary
-                    if (seg == 0) { lo = b1 = i + 1; b2 = hi = start[rb + cx + 1]; }
-                    else { lo = b1 = b2 = start[rb]; hi = start[rb + 1]; }
-                }
-                const int len = hi - lo;
-                const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
-                for (int base = 0; base < trip; base += hitcap) {
-                    const int clen = min(max(len - base, 0), hitcap);
-                    if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
-                        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4,
-                                                           acc, F, n);
-                        cnt = 0;
-                    }
-                    const int tend = base + min(trip - base, hitcap);
-                    for (int t = base; t < tend; t += 2) {
-                        const int j0 = lo + t, j1 = j0 + 1;
-                        const bool h0 = t < len, h1 = t + 1 < len && t + 1 < tend;
-                        V4 p0, p1;
-                        if (h0) p0 = pos4[j0];
-                        if (h1) p1 = pos4[j1];
-                        if (h0) {
-                            const bool ge1 = j0 >= b1, ge2 = j0 >= b2;
-                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p0.x;
-                            const real ddy = piy - p0.y, ddz = piz - p0.z;
-                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
-                                list[cnt * kPairBlock] = (uint32_t)j0 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
-                                ++cnt;
-                            }
-                        }
-                        if (h1) {
-                            const bool ge1 = j1 >= b1, ge2 = j1 >= b2;
-                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p1.x;
-                            const real ddy = piy - p1.y, ddz = piz - p1.z;
-                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
-                                list[cnt * kPairBlock] = (uint32_t)j1 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
-                                ++cnt;
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n);
-        if (live) {
-            atomicAdd(F + i, acc[0]);
-            atomicAdd(F + n + i, acc[1]);
-            atomicAdd(F + 2 * n + i, acc[2]);
-            if (VIRIAL) {
-#pragma unroll
-                for (int q = 0; q < 9; ++q) stress[q * n + i] = acc[3 + q];
-            }
-        }
+        half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F, stress,
+                                             hitcap, lists, sh, keys0);
     }
 }
 

@@ -27,6 +27,7 @@ STATUS_IMAGE_OVERFLOW = 0x4
 
 PAIR_FULL_SHELL = 0      # default: bitwise reproducible forces
 PAIR_HALF_SHELL = 1      # each pair once, partner force by atomics
+PAIR_STAGED = 2          # half shell with the neighbour rows staged in shared memory
 
 EXPORTED = [
     "dpd_engine_create", "dpd_engine_upload_beads", "dpd_engine_upload_topology",
@@ -223,7 +224,8 @@ class DpdEngine:
                                                        int(carveout)), "set_launch_shape")
 
     def set_pair_scheme(self, scheme: int) -> None:
-        """PAIR_FULL_SHELL (reproducible) or PAIR_HALF_SHELL (each pair once)."""
+        """PAIR_FULL_SHELL (reproducible), PAIR_HALF_SHELL (each pair once) or
+        PAIR_STAGED (each pair once, neighbour rows staged in shared memory)."""
         self._check(load().dpd_engine_set_pair_scheme(self.h, int(scheme)), "set_pair_scheme")
 
     def set_sample_period(self, period: int) -> None:

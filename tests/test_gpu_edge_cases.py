@@ -98,10 +98,12 @@ def _system_with_widths(widths=(1.5, 1.0, 1.25), cells=(5, 7, 6)):
                        types[order], u[order], v[order])
 
 
+@pytest.mark.parametrize("scheme", [0, 1, 2], ids=["full", "half", "staged"])
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
-def test_non_unit_cell_widths_and_ragged_box(engine_mod, oracle_mod, precision):
+def test_non_unit_cell_widths_and_ragged_box(engine_mod, oracle_mod, precision, scheme):
     s = _system_with_widths()
     eng, orc = _both(engine_mod, oracle_mod, s, precision)
+    eng.set_pair_scheme(scheme)
     eng.step(1, 5)
     orc.step(1, 5)
     g, o = eng.download(), orc.state()

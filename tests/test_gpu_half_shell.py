@@ -1,5 +1,6 @@
-"""The half-shell pair scheme (each pair evaluated once, the partner's share
-added with atomics) against the CPU oracle.  Its force sums are rounded in
+"""The half-shell pair schemes (each pair evaluated once, the partner's share
+added with atomics; unstaged and staged in shared memory) against the CPU
+oracle.  Its force sums are rounded in
 a run-dependent order, so the bounds are the tolerances of the full-shell
 tests rather than bit equality:
   * mixed precision: forces within 1e-5 of the force RMS after one step,
@@ -24,18 +25,22 @@ SYSTEMS = {
 }
 
 
-def _half(engine_mod, oracle_mod, s, precision, **kw):
+SCHEMES = pytest.mark.parametrize("scheme", [1, 2], ids=["half", "staged"])
+
+
+def _half(engine_mod, oracle_mod, s, precision, scheme=1, **kw):
     eng = engine_mod.DpdEngine.from_system(s, precision=precision, **kw)
-    eng.set_pair_scheme(engine_mod.PAIR_HALF_SHELL)
+    eng.set_pair_scheme(scheme)
     orc = oracle_mod.Oracle(s, noise=oracle_mod.NOISE_PHILOX, **kw)
     return eng, orc
 
 
+@SCHEMES
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
 @pytest.mark.parametrize("name", list(SYSTEMS))
-def test_half_shell_one_step(engine_mod, oracle_mod, name, precision):
+def test_half_shell_one_step(engine_mod, oracle_mod, name, precision, scheme):
     s = SYSTEMS[name]()
-    eng, orc = _half(engine_mod, oracle_mod, s, precision, gamma_scale=0.0)
+    eng, orc = _half(engine_mod, oracle_mod, s, precision, scheme, gamma_scale=0.0)
     eng.step(1, 1)
     orc.step(1, 1)
     g, o = eng.download(), orc.state()
@@ -46,11 +51,12 @@ def test_half_shell_one_step(engine_mod, oracle_mod, name, precision):
     assert eng.status() == 0
 
 
+@SCHEMES
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
 @pytest.mark.parametrize("name", list(SYSTEMS))
-def test_half_shell_thermostat_steps(engine_mod, oracle_mod, name, precision):
+def test_half_shell_thermostat_steps(engine_mod, oracle_mod, name, precision, scheme):
     s = SYSTEMS[name]()
-    eng, orc = _half(engine_mod, oracle_mod, s, precision)
+    eng, orc = _half(engine_mod, oracle_mod, s, precision, scheme)
     eng.step(1, 5)
     orc.step(1, 5)
     g, o = eng.download(), orc.state()
@@ -60,10 +66,11 @@ def test_half_shell_thermostat_steps(engine_mod, oracle_mod, name, precision):
     assert np.array_equal(eng.cells(), orc.cells())
 
 
+@SCHEMES
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
-def test_half_shell_virial(engine_mod, oracle_mod, precision):
+def test_half_shell_virial(engine_mod, oracle_mod, precision, scheme):
     s = SYSTEMS["bilayer"]()
-    eng, orc = _half(engine_mod, oracle_mod, s, precision)
+    eng, orc = _half(engine_mod, oracle_mod, s, precision, scheme)
     eng.step(1, 3)
     orc.step(1, 3)
     obs = eng.observables()
@@ -85,7 +92,8 @@ def _dense_cluster_system():
                        np.concatenate([s.v, np.zeros((extra, 3))]))
 
 
-@pytest.mark.parametrize("tune", ["half=1", "half=1,hitcap=8", "half=1,hitcap=64,bps=1"])
+@pytest.mark.parametrize("tune", ["half=1", "half=1,hitcap=8", "half=1,hitcap=64,bps=1", "scheme=2",
+                                  "scheme=2,hitcap=8", "scheme=2,hitcap=64,bps=1"])
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
 def test_half_shell_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precision, tune, monkeypatch):
     """Selected through DPD_TUNE, with a 60-bead cell and extreme hit-list sizes."""
@@ -100,18 +108,22 @@ def test_half_shell_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precisi
     assert eng.status() == 0
 
 
-def test_half_shell_replica_batch(engine_mod, oracle_mod):
+@SCHEMES
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_half_shell_replica_batch(engine_mod, oracle_mod, precision, scheme):
     edges, fracs, a_ab, seeds = W.replica_table(4, lo=4, hi=7)
     systems = [W.binary_mixture(n=int(edges[r]), seed=int(seeds[r]), a_ab=float(a_ab[r]), frac_a=float(fracs[r]))
                for r in range(4)]
-    batch = engine_mod.DpdBatch(systems, precision=1)
-    batch.set_pair_scheme(engine_mod.PAIR_HALF_SHELL)
+    batch = engine_mod.DpdBatch(systems, precision=precision)
+    batch.set_pair_scheme(scheme)
     batch.step(1, 3)
     f = batch.split(batch.download()["f"])
+    tol = 1e-4 if precision == 0 else 1e-10
     for k, s in enumerate(systems):
         o = oracle_mod.Oracle(s, noise=oracle_mod.NOISE_PHILOX)
         o.step(1, 3)
-        assert rel_err(f[k], o.state()["f"]) < 1e-10
+        assert rel_err(f[k], o.state()["f"]) < tol
+    assert batch.status() == 0
 
 
 def test_switching_schemes_between_calls(engine_mod):
@@ -128,5 +140,30 @@ def test_switching_schemes_between_calls(engine_mod):
     b.step(8, 3)
     ga, gb = a.download(), b.download()
     assert rel_err(gb["f"], ga["f"]) < 1e-10
+    b.set_pair_scheme(engine_mod.PAIR_STAGED)
+    b.step(11, 3)
+    a.step(11, 3)
+    assert rel_err(b.download()["f"], a.download()["f"]) < 1e-10
     with pytest.raises(engine_mod.EngineError):
         b.set_pair_scheme(7)
+
+
+@pytest.mark.parametrize("scheme", [1, 2], ids=["half", "staged"])
+@pytest.mark.parametrize("workload", ["bilayer", "polymer"])
+def test_half_shell_matches_full_shell_at_full_size(engine_mod, workload, scheme):
+    """The half-shell schemes against the full-shell kernel on the full-size
+    workloads (393,216 and 6,291,456 beads), one thermostatted step from the
+    same state: the kernels evaluate the same pairs with the same noise, so
+    the forces agree to FP32 summation-order rounding."""
+    s = W.bilayer() if workload == "bilayer" else W.polymer_solution()
+    ref = engine_mod.DpdEngine.from_system(s, precision=0)
+    ref.step(1, 1)
+    fr = ref.download()["f"]
+    ref.close()
+    eng = engine_mod.DpdEngine.from_system(s, precision=0)
+    eng.set_pair_scheme(scheme)
+    eng.step(1, 1)
+    fs = eng.download()["f"]
+    assert eng.status() == 0
+    eng.close()
+    assert rel_err(fs, fr) < 2e-5
