@@ -27,10 +27,9 @@ namespace dpd {
 constexpr int kPairWarps = 4;
 constexpr int kPairBlock = 32 * kPairWarps;
 // Resident blocks per SM the pair kernels are compiled for: 8 (64 registers,
-// 32 warps) for one FP32 box; a replica batch (per-owner box tables) 7, and
-// the FP64 variants 5, to keep their register spills small.
+// 32 warps) in FP32; the FP64 variants keep 6 to limit spills.
 template <typename real, bool MULTI = false> struct PairOcc {
-    static constexpr int value = sizeof(real) == 8 ? 5 : (MULTI ? 7 : 8);
+    static constexpr int value = sizeof(real) == 8 ? 6 : 8;
 };
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
 
@@ -348,6 +347,7 @@ __device__ __forceinline__ void balanced_force_pass(
 #pragma unroll
             for (int q = 0; q < 10; ++q) keys[q] = keys0[q];
         }
+        int cur_box = -1;
         auto load_owner = [&](int oo) {
             const int to = wbase + oo;
             pi = sh.hpos[to];
@@ -356,8 +356,11 @@ __device__ __forceinline__ void balanced_force_pass(
             islot = tile_base + to;
             ti = (real_bits(pi.w) & 0xFF) * nt;
             idi = (uint32_t)real_bits(vi.w);
-            if (MULTI) {   // the owner's box: cell widths, pair tables, noise key
-                const Box& B = boxes[flag_box(real_bits(pi.w))];
+            // the owner's box (cell widths, pair tables, noise key), reloaded
+            // only when it changes: a batch's boxes are contiguous in slot order
+            if (MULTI && flag_box(real_bits(pi.w)) != cur_box) {
+                cur_box = flag_box(real_bits(pi.w));
+                const Box& B = boxes[cur_box];
                 wx = (real)B.w[0]; wy = (real)B.w[1]; wz = (real)B.w[2];
                 if (STAGED) iw = real(1) / wx;
                 T = tab + B.tab;
@@ -449,6 +452,186 @@ __device__ __forceinline__ void balanced_force_pass(
         }
     }
     __syncwarp();   // every lane is done with the lists before they are refilled
+}
+
+// This lane's listed pairs, each evaluated once: the force goes to the lane's
+// own accumulator and, negated, to the partner through atomics.
+template <typename real, bool VIRIAL>
+__device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __restrict__ list,
+                                                     const typename Vec4<real>::type& pi,
+                                                     const typename Vec4<real>::type& vi, const real* __restrict__ T,
+                                                     int nt, real wx, real wy, real wz, const uint32_t* keys,
+                                                     const typename Vec4<real>::type* __restrict__ pos4,
+                                                     const typename Vec4<real>::type* __restrict__ vel4, real* acc,
+                                                     real* __restrict__ F, int n)
+{
+    typedef typename Vec4<real>::type V4;
+    const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    const int ti = (real_bits(pi.w) & 0xFF) * nt;
+    const uint32_t idi = (uint32_t)real_bits(vi.w);
+    const int m2 = nt * nt;
+    for (int k = 0; k < trip; ++k) {
+        if (k < cnt) {
+            const uint32_t e = list[k * kPairBlock];
+            const int j = (int)(e & 0x03FFFFFFu);
+            const V4 pj = pos4[j];
+            const V4 vj = vel4[j];
+            const real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
+            const real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
+            const real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
+            const real r2 = dx * dx + dy * dy + dz * dz;
+            const real inv = RealOps<real>::rsqrt(r2);
+            const real wr = real(1) - r2 * inv;
+            const int tt = ti + (real_bits(pj.w) & 0xFF);
+            const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
+            const uint32_t idj = (uint32_t)real_bits(vj.w);
+            uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                const uint64_t prod = (uint64_t)0xD256D193u * c0;
+                c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
+                c1 = (uint32_t)prod;
+            }
+            const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
+                             T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
+            const real m = mag * inv;
+            const real gx = m * dx, gy = m * dy, gz = m * dz;
+            acc[0] += gx; acc[1] += gy; acc[2] += gz;
+            atomicAdd(F + j, -gx);
+            atomicAdd(F + n + j, -gy);
+            atomicAdd(F + 2 * n + j, -gz);
+            if (VIRIAL) {
+                acc[3] += dx * gx; acc[4] += dy * gx; acc[5] += dz * gx;
+                acc[6] += dx * gy; acc[7] += dy * gy; acc[8] += dz * gy;
+                acc[9] += dx * gz; acc[10] += dy * gz; acc[11] += dz * gz;
+            }
+        }
+    }
+}
+
+// The same tile with the per-lane force pass of the previous kernel
+// generation: every lane evaluates its own hits (the warp runs as long as
+// its busiest lane) and keeps bead i's force in registers.  Measured faster
+// than the balanced pass for the FP64 and replica-batch variants, whose
+// register budgets the balanced pass exceeds.
+template <typename real, bool VIRIAL, bool MULTI>
+__device__ __forceinline__ void half_shell_tile_lanes(
+    int tile, int n, int nt, const Box* __restrict__ boxes, int64_t step, const real* __restrict__ tab,
+    const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
+    const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
+    real* __restrict__ F, real* __restrict__ stress, int hitcap, uint32_t* lists)
+{
+    typedef typename Vec4<real>::type V4;
+    uint32_t* list = lists + threadIdx.x;
+    {
+        const int i = tile * kPairBlock + threadIdx.x;
+        const bool live = i < n;
+        V4 pi, vi;
+        int cx = 0, cy = 0, cz = 0;
+        if (live) {
+            pi = pos4[i];
+            vi = vel4[i];
+        } else {
+            pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
+        }
+        const Box& B = boxes[MULTI ? flag_box(real_bits(pi.w)) : 0];
+        const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
+        if (live) {
+            const int c = cell[i] - B.cell_base;
+            cx = c % nx;
+            cy = (c / nx) % ny;
+            cz = c / (nx * ny);
+        }
+        const real* T = MULTI ? tab + B.tab : Tsh;
+        uint32_t keys[10];
+        {
+            uint32_t k = philox_step_key(B.seed, step);
+#pragma unroll
+            for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
+        }
+        const real wx = (real)B.w[0], wy = (real)B.w[1], wz = (real)B.w[2];
+        const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
+        constexpr int NACC = VIRIAL ? 12 : 3;
+        real acc[NACC];
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) acc[q] = real(0);
+        int cnt = 0;
+        for (int r = 0; r < 5; ++r) {
+            const int dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
+            const int dz = r < 2 ? 0 : 1;
+            int y2 = cy + dy, z2 = cz + dz;
+            y2 += (y2 >= ny) ? -ny : 0;
+            z2 += (z2 >= nz) ? -nz : 0;
+            y2 += (y2 < 0) ? ny : 0;
+            const int rb = B.cell_base + nx * (y2 + ny * z2);
+            const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
+            const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
+            for (int seg = 0; seg < 2; ++seg) {
+                int lo, hi, b1, b2;
+                if (r > 0) {
+                    row_segment(live, seg, rb, cx, nx, start, lo, hi, b1, b2);
+                } else if (!live) {
+                    lo = hi = b1 = b2 = 0;
+                } else if (cx < nx - 1) {
+                    // own cell after i, then cell x+1 (offset +1 from b2)
+                    if (seg == 0) { lo = b1 = i + 1; b2 = start[rb + cx + 1]; hi = start[rb + cx + 2]; }
+                    else { lo = hi = b1 = b2 = 0; }
+                } else {
+                    // cx = nx-1: own cell after i, then cell 0 across the boundary
+                    if (seg == 0) { lo = b1 = i + 1; b2 = hi = start[rb + cx + 1]; }
+                    else { lo = b1 = b2 = start[rb]; hi = start[rb + 1]; }
+                }
+                const int len = hi - lo;
+                const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+                for (int base = 0; base < trip; base += hitcap) {
+                    const int clen = min(max(len - base, 0), hitcap);
+                    if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
+                        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4,
+                                                           acc, F, n);
+                        cnt = 0;
+                    }
+                    const int tend = base + min(trip - base, hitcap);
+                    for (int t = base; t < tend; t += 2) {
+                        const int j0 = lo + t, j1 = j0 + 1;
+                        const bool h0 = t < len, h1 = t + 1 < len && t + 1 < tend;
+                        V4 p0, p1;
+                        if (h0) p0 = pos4[j0];
+                        if (h1) p1 = pos4[j1];
+                        if (h0) {
+                            const bool ge1 = j0 >= b1, ge2 = j0 >= b2;
+                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p0.x;
+                            const real ddy = piy - p0.y, ddz = piz - p0.z;
+                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
+                                list[cnt * kPairBlock] = (uint32_t)j0 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
+                                ++cnt;
+                            }
+                        }
+                        if (h1) {
+                            const bool ge1 = j1 >= b1, ge2 = j1 >= b2;
+                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p1.x;
+                            const real ddy = piy - p1.y, ddz = piz - p1.z;
+                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
+                                list[cnt * kPairBlock] = (uint32_t)j1 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
+                                ++cnt;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n);
+        if (live) {
+            atomicAdd(F + i, acc[0]);
+            atomicAdd(F + n + i, acc[1]);
+            atomicAdd(F + 2 * n + i, acc[2]);
+            if (VIRIAL) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) stress[q * n + i] = acc[3 + q];
+            }
+        }
+    }
 }
 
 // Dynamic shared memory of k_pair_forces_half: pair tables (single box), hit
@@ -594,6 +777,12 @@ __device__ __forceinline__ void half_shell_tile(
                                                     w0, step, pos4, vel4, F, stress, n);
 }
 
+// Which force pass a k_pair_forces_half instantiation uses: the balanced pass
+// for one FP32 box, the per-lane pass for FP64 and replica batches (each the
+// faster of the two on a B200).
+template <typename real, bool MULTI>
+constexpr bool kHalfBalanced = sizeof(real) == 4 && !MULTI;
+
 // F must be zero on entry, and on sample steps (VIRIAL) the stress array too.
 template <typename real, bool VIRIAL, bool MULTI>
 __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pair_forces_half(
@@ -622,8 +811,12 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     const int tile0 = blockIdx.x * tiles_per_block;
     for (int tile = tile0; tile < tile0 + tiles_per_block; ++tile) {
         if (tile * kPairBlock >= n) break;
-        half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F, stress,
-                                             hitcap, lists, sh, keys0);
+        if (kHalfBalanced<real, MULTI>)
+            half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
+                                                 stress, hitcap, lists, sh, keys0);
+        else
+            half_shell_tile_lanes<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
+                                                       F, stress, hitcap, lists);
     }
 }
 
