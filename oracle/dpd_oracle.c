@@ -50,6 +50,16 @@ struct dpdo_sim {
     int32_t *af, *as;
     double *k3, *phi0;
 
+    /* slice stress profile (CMonitor::AddBeadStress / AddBondStress /
+     * AddBondPairStress, Monitor.cpp:1900-2755), S = 0 when off */
+    int32_t S, nbt, nbpt;
+    double swidth, sinv;
+    int32_t *btype, *bptype;       /* bond type per bond, bondpair type per bond pair */
+    double *ssp, *ssb, *ssbp;      /* [S][T*T][9], [S][nbt][9], [S][nbpt][9] */
+    double *bpf;                   /* per bond pair the forces on its beads, [4][3]; kept
+                                      between steps like m_BeadXForce (BondPair.h:82) */
+    int64_t slice_errors;
+
     uint64_t lcg;
     int64_t step;          /* m_SimTime of the step being evaluated */
     int64_t pairs;
@@ -185,10 +195,20 @@ static void free_beads(dpdo_sim* s)
     s->id = NULL;
 }
 
+static void free_slices(dpdo_sim* s)
+{
+    free(s->btype); free(s->bptype); free(s->ssp); free(s->ssb); free(s->ssbp);
+    s->btype = s->bptype = NULL;
+    s->ssp = s->ssb = s->ssbp = NULL;
+    s->S = 0;
+}
+
 static void free_topo(dpdo_sim* s)
 {
     free(s->bh); free(s->bt); free(s->k2); free(s->l0); free(s->bdx); free(s->blen);
-    free(s->af); free(s->as); free(s->k3); free(s->phi0);
+    free(s->af); free(s->as); free(s->k3); free(s->phi0); free(s->bpf);
+    s->bpf = NULL;
+    free_slices(s);
     s->bh = NULL; s->nb = 0; s->na = 0;
 }
 
@@ -294,6 +314,7 @@ int dpdo_set_topology(dpdo_sim* s, int64_t nb, const int64_t* head_id, const int
     s->as = (int32_t*)malloc(sizeof(int32_t) * (na ? na : 1));
     s->k3 = (double*)malloc(sizeof(double) * (na ? na : 1));
     s->phi0 = (double*)malloc(sizeof(double) * (na ? na : 1));
+    s->bpf = (double*)calloc(12 * (na ? na : 1), sizeof(double));
     for (int64_t i = 0; i < nb; ++i) {
         s->bh[i] = find_id(s, head_id[i]);
         s->bt[i] = find_id(s, tail_id[i]);
@@ -382,6 +403,115 @@ static void update_pos(dpdo_sim* s)
 }
 
 /* One interacting pair, CNTCell.cpp:1192-1301 (same cell) and 1363-1522 (neighbour cell). */
+/* ------------------------------------------------- slice stress profile --- */
+
+/* The shared body of CMonitor::AddBeadStress (Monitor.cpp:1900-2107),
+ * AddBondStress (2283-2518) and AddBondPairStress (2520-2755): the
+ * Goetz-Lipowsky split of one contribution fdx (force x separation, 9
+ * components) over the z slices between two beads.  za is the z of the bead
+ * the separation points to (bead 1, the bond head, bead j+1), zb the other's;
+ * zDiff the z separation.  arr is [S][K][9]; idx the type index. */
+static void slice_add(dpdo_sim* s, double* arr, int64_t K, int64_t idx, const double fdx[9], double zDiff,
+                      double za, double zb)
+{
+    double up, lo;
+    if (zDiff > 0.00001) {
+        up = za * s->sinv;
+        lo = zb * s->sinv;
+    } else if (zDiff < -0.00001) {
+        zDiff = -zDiff;
+        up = zb * s->sinv;
+        lo = za * s->sinv;
+    } else {
+        up = za * s->sinv;
+        lo = up;
+    }
+    const int64_t S = s->S;
+    int64_t ui = (int64_t)up;
+    const double ur = up - (double)ui;
+    int64_t li = (int64_t)lo;
+    const double lr = lo - (double)li;
+    if (ui < 0 || ui >= S || li < 0 || li >= S || idx < 0 || idx >= K) { s->slice_errors++; return; }
+#define SLICE_ADD(sl, fac) do { double* q_ = arr + ((sl) * K + idx) * 9; \
+        for (int c_ = 0; c_ < 9; ++c_) q_[c_] += fdx[c_] * (fac); } while (0)
+    if (ui == li) {
+        if (up != lo || ur > 0.00001) {
+            double* q = arr + (li * K + idx) * 9;
+            for (int c = 0; c < 9; ++c) q[c] += fdx[c];
+        } else {
+            SLICE_ADD(ui, 0.5);
+            if (--li < 0) li += S;
+            SLICE_ADD(li, 0.5);
+        }
+    } else {
+        const double inner = s->swidth / zDiff;
+        if (ui > li) {
+            for (int64_t k = li + 1; k <= ui - 1; ++k) SLICE_ADD(k, inner);
+        } else {
+            for (int64_t kp = li + 1; kp <= S + ui - 1; ++kp) {
+                int64_t k = kp;
+                if (k >= S) k -= S;
+                SLICE_ADD(k, inner);
+            }
+        }
+        if (lr > 0.000001) SLICE_ADD(li, (1.0 - lr) * inner);
+        else SLICE_ADD(li, inner);
+        if (ur > 0.000001) SLICE_ADD(ui, ur * inner);
+    }
+#undef SLICE_ADD
+}
+
+static void outer9(const double f[3], const double d[3], double o[9])
+{
+    o[0] = f[0] * d[0]; o[1] = f[0] * d[1]; o[2] = f[0] * d[2];
+    o[3] = f[1] * d[0]; o[4] = f[1] * d[1]; o[5] = f[1] * d[2];
+    o[6] = f[2] * d[0]; o[7] = f[2] * d[1]; o[8] = f[2] * d[2];
+}
+
+int dpdo_set_slice_stress(dpdo_sim* s, int32_t nslices, int32_t nbondtypes, const int32_t* bond_type,
+                          int32_t nbptypes, const int32_t* bondpair_type)
+{
+    if (!s || nslices < 0 || nbondtypes < 0 || nbptypes < 0) return -1;
+    free_slices(s);
+    if (nslices == 0) return 0;
+    if ((s->nb > 0 && !bond_type) || (s->na > 0 && !bondpair_type)) return -1;
+    s->S = nslices;
+    s->nbt = nbondtypes;
+    s->nbpt = nbptypes;
+    /* m_GridZCellWidth = m_SimBoxZLength / GridZCellNo (Monitor.cpp:247), inverse as Monitor.cpp:2185 */
+    s->swidth = s->L[2] / (double)nslices;
+    s->sinv = 1.0 / s->swidth;
+    s->btype = (int32_t*)malloc(sizeof(int32_t) * (s->nb ? s->nb : 1));
+    s->bptype = (int32_t*)malloc(sizeof(int32_t) * (s->na ? s->na : 1));
+    for (int64_t i = 0; i < s->nb; ++i) s->btype[i] = bond_type[i];
+    for (int64_t i = 0; i < s->na; ++i) s->bptype[i] = bondpair_type[i];
+    s->ssp = (double*)calloc((size_t)nslices * s->T * s->T * 9, sizeof(double));
+    s->ssb = (double*)calloc((size_t)nslices * (nbondtypes ? nbondtypes : 1) * 9, sizeof(double));
+    s->ssbp = (double*)calloc((size_t)nslices * (nbptypes ? nbptypes : 1) * 9, sizeof(double));
+    return 0;
+}
+
+int dpdo_get_slice_stress(const dpdo_sim* s, double* pair, double* bond, double* bondpair)
+{
+    if (!s || !s->S) return -1;
+    if (pair) memcpy(pair, s->ssp, sizeof(double) * (size_t)s->S * s->T * s->T * 9);
+    if (bond) memcpy(bond, s->ssb, sizeof(double) * (size_t)s->S * s->nbt * 9);
+    if (bondpair) memcpy(bondpair, s->ssbp, sizeof(double) * (size_t)s->S * s->nbpt * 9);
+    return 0;
+}
+
+int64_t dpdo_slice_errors(const dpdo_sim* s) { return s ? s->slice_errors : -1; }
+
+/* CMonitor::ZeroSliceStress (Monitor.cpp:2109), called at the start of every
+ * step (SimBox.cpp:999). */
+static void zero_slices(dpdo_sim* s)
+{
+    if (!s->S) return;
+    memset(s->ssp, 0, sizeof(double) * (size_t)s->S * s->T * s->T * 9);
+    memset(s->ssb, 0, sizeof(double) * (size_t)s->S * (s->nbt ? s->nbt : 1) * 9);
+    memset(s->ssbp, 0, sizeof(double) * (size_t)s->S * (s->nbpt ? s->nbpt : 1) * 9);
+}
+
 static void pair_force(dpdo_sim* s, int32_t b1, int32_t b2, int minimg)
 {
     double dx[3], dv[3], nf[3];
@@ -423,6 +553,12 @@ static void pair_force(dpdo_sim* s, int32_t b1, int32_t b2, int minimg)
     st[0] += dx[0] * nf[0]; st[1] += dx[1] * nf[0]; st[2] += dx[2] * nf[0];
     st[3] += dx[0] * nf[1]; st[4] += dx[1] * nf[1]; st[5] += dx[2] * nf[1];
     st[6] += dx[0] * nf[2]; st[7] += dx[1] * nf[2]; st[8] += dx[2] * nf[2];
+    if (s->S) {   /* CMonitor::AddBeadStress(bead1, bead2, newForce, dx), CNTCell.cpp:1310 */
+        double fdx[9];
+        outer9(nf, dx, fdx);
+        slice_add(s, s->ssp, (int64_t)s->T * s->T, (int64_t)t1 * s->T + t2, fdx, dx[2], s->x[3 * b1 + 2],
+                  s->x[3 * b2 + 2]);
+    }
 }
 
 /* CCNTCell::UpdateForce, DPD branch, CNTCell.cpp:1103-1572. */
@@ -464,6 +600,31 @@ static void bond_forces(dpdo_sim* s)
         st[0] += bd[0] * fx; st[1] += bd[1] * fx; st[2] += bd[2] * fx;
         st[3] += bd[0] * fy; st[4] += bd[1] * fy; st[5] += bd[2] * fy;
         st[6] += bd[0] * fz; st[7] += bd[1] * fz; st[8] += bd[2] * fz;
+        if (s->S) {   /* CMonitor::AddBondStress, Polymer.cpp:677-680 */
+            const double fb[3] = {fx, fy, fz};
+            double fdx[9];
+            outer9(fb, bd, fdx);
+            slice_add(s, s->ssb, s->nbt, s->btype[i], fdx, bd[2], s->x[3 * h + 2], s->x[3 * t + 2]);
+        }
+    }
+}
+
+/* CMonitor::AddBondPairStress (Monitor.cpp:2520-2755) of bond pair i: the
+ * three bead pairs first.tail -> first.head -> second.head -> first.tail,
+ * separation = unPBC difference, force = 0.33333333 * (F[j+1] - F[j]). */
+static void bondpair_slices(dpdo_sim* s, int64_t i)
+{
+    if (!s->S) return;
+    const int32_t b1 = s->af[i], b2 = s->as[i];
+    const int32_t bead[4] = {s->bt[b1], s->bh[b1], s->bh[b2], s->bt[b1]};
+    const double* bp = s->bpf + 12 * i;
+    for (int j = 0; j < 3; ++j) {
+        const int jp1 = j + 1;
+        double dx[3], fo[3], fdx[9];
+        for (int d = 0; d < 3; ++d) dx[d] = s->u[3 * bead[jp1] + d] - s->u[3 * bead[j] + d];
+        for (int d = 0; d < 3; ++d) fo[d] = 0.33333333 * (bp[3 * jp1 + d] - bp[3 * j + d]);
+        outer9(fo, dx, fdx);
+        slice_add(s, s->ssbp, s->nbpt, s->bptype[i], fdx, dx[2], s->x[3 * bead[jp1] + 2], s->x[3 * bead[j] + 2]);
     }
 }
 
@@ -475,7 +636,10 @@ static void bondpair_forces(dpdo_sim* s)
         const int32_t b1 = s->af[i], b2 = s->as[i];
         const double firstLength = s->blen[b1], secondLength = s->blen[b2];
         const double magProduct = firstLength * secondLength;
-        if (!(magProduct > 0.0001)) continue;
+        if (!(magProduct > 0.0001)) {
+            bondpair_slices(s, i);   /* stale m_BeadXForce, as the reference */
+            continue;
+        }
         const double* first = s->bdx + 3 * b1;
         const double* second = s->bdx + 3 * b2;
         const double b1MagSq = firstLength * firstLength;
@@ -502,6 +666,9 @@ static void bondpair_forces(dpdo_sim* s)
         for (int d = 0; d < 3; ++d) s->f[3 * ft + d] += f0[d];
         for (int d = 0; d < 3; ++d) s->f[3 * sh + d] += f2[d];
         for (int d = 0; d < 3; ++d) s->f[3 * fh + d] += f1[d];
+        double* bp = s->bpf + 12 * i;   /* m_BeadXForce[0..3], [3] = [0] (BondPair.cpp:231-262) */
+        for (int d = 0; d < 3; ++d) { bp[d] = f0[d]; bp[3 + d] = f1[d]; bp[6 + d] = f2[d]; bp[9 + d] = f0[d]; }
+        bondpair_slices(s, i);
     }
 }
 
@@ -536,6 +703,7 @@ int dpdo_step(dpdo_sim* s, int64_t first_step, int32_t nsteps)
     for (int32_t k = 0; k < nsteps; ++k) {
         s->step = first_step + k;
         update_pos(s);
+        zero_slices(s);
         update_force(s);
         bond_forces(s);
         bondpair_forces(s);

@@ -14,6 +14,8 @@
  *   CSimBox::MakeCNTCells / MapCelltoIndex / AssignBeadstoCells
  *                                   SimBox.cpp:715-940
  *   CCNTCell::CheckBeadsinCell      CNTCell.cpp:2628-2700
+ *   CMonitor::AddBeadStress / AddBondStress / AddBondPairStress / ZeroSliceStress
+ *                                   Monitor.cpp:1900-2755 (slice stress profile)
  *
  * Two noise sources are provided:
  *   DPDO_NOISE_LCG    - the reference's single 64-bit LCG consumed once per
@@ -82,6 +84,18 @@ int64_t dpdo_pair_count(const dpdo_sim* s);
 
 /* Philox2x32-10 draw used for the pair noise: first output word. */
 uint32_t dpdo_philox_pair(uint64_t seed, int64_t step, uint32_t id_lo, uint32_t id_hi);
+
+/* Slice stress profile of CMonitor (Monitor.cpp:1900-2755, zeroed every
+ * step as SimBox.cpp:999): nslices z slices of width L_z/nslices (the
+ * analysis grid's GridZCellNo), pair part indexed [slice][type1*T+type2][9]
+ * with bead 1 the reference's iterating bead, bond part [slice][bond type][9],
+ * bond-pair part [slice][bondpair type][9].  nslices = 0 turns it off.  Call
+ * after dpdo_set_topology. */
+int dpdo_set_slice_stress(dpdo_sim* s, int32_t nslices, int32_t nbondtypes, const int32_t* bond_type,
+                          int32_t nbptypes, const int32_t* bondpair_type);
+int dpdo_get_slice_stress(const dpdo_sim* s, double* pair, double* bond, double* bondpair);
+/* Contributions that fell outside the slices (a z at the box edge rounded up). */
+int64_t dpdo_slice_errors(const dpdo_sim* s);
 
 /* Time-step dependent constants after a ChangeTimeStepConstants (CNTCell.cpp:357). */
 int dpdo_set_dt(dpdo_sim* s, double dt);

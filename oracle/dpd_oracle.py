@@ -61,6 +61,10 @@ def lib() -> C.CDLL:
         L.dpdo_philox_pair.restype = C.c_uint32
         L.dpdo_set_dt.argtypes = [vp, C.c_double]
         L.dpdo_set_pair.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+        L.dpdo_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
+        L.dpdo_get_slice_stress.argtypes = [vp, vp, vp, vp]
+        L.dpdo_slice_errors.argtypes = [vp]
+        L.dpdo_slice_errors.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -101,6 +105,34 @@ class Oracle:
                                  len(t[4]), _p(t[4]), _p(t[5]), _p(t[6]), _p(t[7]))
         if rc != 0:
             raise RuntimeError(f"dpdo_set_topology failed ({rc})")
+        self._sys = system
+        self._slices = 0
+
+    def set_slice_stress(self, nslices: int) -> None:
+        """Accumulates CMonitor's slice stress profile (Monitor.cpp:1900-2755)
+        over ``nslices`` z slices every step; 0 turns it off."""
+        s = self._sys
+        self._bt = np.ascontiguousarray(s.bond_type if s.bond_type is not None else [], np.int32)
+        self._at = np.ascontiguousarray(s.angle_type if s.angle_type is not None else [], np.int32)
+        self._nbt = len(s.bond_specs)
+        self._nbpt = len(s.bondpair_specs)
+        rc = lib().dpdo_set_slice_stress(self.h, int(nslices), self._nbt, _p(self._bt), self._nbpt, _p(self._at))
+        if rc != 0:
+            raise RuntimeError(f"dpdo_set_slice_stress failed ({rc})")
+        self._slices = int(nslices)
+
+    def slice_stress(self):
+        """{"pair": [S][T*T][9], "bond": [S][NBT][9], "bondpair": [S][NBPT][9]}
+        of the last step."""
+        S, T = self._slices, len(self._sys.type_names)
+        out = {"pair": np.zeros((S, T * T, 9)), "bond": np.zeros((S, self._nbt, 9)),
+               "bondpair": np.zeros((S, self._nbpt, 9))}
+        if lib().dpdo_get_slice_stress(self.h, _p(out["pair"]), _p(out["bond"]), _p(out["bondpair"])) != 0:
+            raise RuntimeError("slice stress is off")
+        return out
+
+    def slice_errors(self) -> int:
+        return int(lib().dpdo_slice_errors(self.h))
 
     def step(self, first_step: int, nsteps: int) -> None:
         if lib().dpdo_step(self.h, first_step, nsteps) != 0:
@@ -143,11 +175,13 @@ def philox_pair(seed: int, step: int, id_lo: int, id_hi: int) -> int:
 
 def run_reference(system, steps: int, workdir: str = None, kT: float = None, gamma_scale: float = 1.0,
                   inject: bool = True, dump: bool = True, topology: bool = False, timeout: float = None,
-                  rng_seed: int = None):
+                  rng_seed: int = None, slices: int = 0):
     """Runs the unmodified reference (oracle/_ref/osprey_ref_driver) on
     ``system`` for ``steps`` steps; ``rng_seed`` restarts its pair-noise LCG
-    at that value just before the step loop.  Returns (json summary, dump dict or None,
-    topology dict or None)."""
+    at that value just before the step loop; ``slices`` > 0 sets the analysis
+    grid to that many z slices and also returns the last step's slice stress
+    profile.  Returns (json summary, dump dict or None, topology dict or None)
+    or, with ``slices``, (summary, dump, topology, slice dict)."""
     from osprey_dpd_b200 import workloads  # local import: test-side helper
 
     if not os.path.exists(REF_DRIVER):
@@ -155,7 +189,8 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     own = workdir is None
     wd = workdir or tempfile.mkdtemp(prefix="dpdref_")
     run = "r"
-    workloads.write_dmpci(system, os.path.join(wd, "dmpci." + run), steps, kT=kT, gamma_scale=gamma_scale)
+    workloads.write_dmpci(system, os.path.join(wd, "dmpci." + run), steps, kT=kT, gamma_scale=gamma_scale,
+                          grid_z=max(1, int(slices)))
     args = [REF_DRIVER, run]
     if inject:
         workloads.write_state(system, os.path.join(wd, "state.bin"))
@@ -166,6 +201,9 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
         args += ["--topology", "topo.bin"]
     if rng_seed is not None:
         args += ["--rng-seed", str(int(rng_seed))]
+    if slices:
+        dims = f"{int(slices)},{len(system.type_names)},{len(system.bond_specs)},{len(system.bondpair_specs)}"
+        args += ["--slices", "slices.bin", "--slice-dims", dims]
     cp = subprocess.run(args, cwd=wd, capture_output=True, text=True, timeout=timeout)
     if cp.returncode != 0:
         raise RuntimeError(f"reference driver failed: {cp.stderr.strip()} {cp.stdout.strip()}")
@@ -173,7 +211,8 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     summary = json.loads(line)
     d = workloads.read_dump(os.path.join(wd, "out.bin")) if dump else None
     t = workloads.read_topology(os.path.join(wd, "topo.bin")) if topology else None
+    sl = workloads.read_slices(os.path.join(wd, "slices.bin")) if slices else None
     if own:
         import shutil
         shutil.rmtree(wd, ignore_errors=True)
-    return summary, d, t
+    return (summary, d, t, sl) if slices else (summary, d, t)

@@ -34,6 +34,11 @@
 //               the reference's own polymer-by-polymer order, InitialState.cpp:498-505)
 //   out.bin   : "DPDDUMP1" int64 n, int64 steps, then n records by bead id:
 //               int64 id, int64 type, double x[3], unpbc[3], v[3], f[3], stress[9]
+//   slices    : (--slices f --slice-dims S,T,NBT,NBPT) "DPDSLICE" int64 S, T, NBT,
+//               NBPT, nb, na; then the slice stress of the last step through
+//               CMonitor's public getters (Monitor.h:248-276): double
+//               pair[S][T*T][9], bond[S][NBT][9], bondpair[S][NBPT][9]; then
+//               int64 type of every bond and bond pair (CBond/CBondPair::GetType)
 
 #include "StdAfx.h"
 #include "SimDefs.h"
@@ -59,6 +64,7 @@
 #include "Bond.h"
 #include "BondPair.h"
 #include "CNTCell.h"
+#include "Monitor.h"
 
 namespace {
 
@@ -84,11 +90,15 @@ int main(int argc, char** argv)
     const char* topoPath = 0;
     const char* dumpPath = 0;
     const char* rngSeed = 0;
+    const char* slicePath = 0;
+    const char* sliceDims = 0;
     for (int a = 2; a + 1 < argc; a += 2) {
         if (!strcmp(argv[a], "--inject")) injectPath = argv[a + 1];
         else if (!strcmp(argv[a], "--topology")) topoPath = argv[a + 1];
         else if (!strcmp(argv[a], "--dump")) dumpPath = argv[a + 1];
         else if (!strcmp(argv[a], "--rng-seed")) rngSeed = argv[a + 1];
+        else if (!strcmp(argv[a], "--slices")) slicePath = argv[a + 1];
+        else if (!strcmp(argv[a], "--slice-dims")) sliceDims = argv[a + 1];
         else return fail("unknown option");
     }
 
@@ -183,6 +193,56 @@ int main(int argc, char** argv)
             for (int k = 0; k < 9; ++k) d[12 + k] = b->m_Stress[k];
             fwrite(it, 8, 2, fp);
             fwrite(d, 8, 21, fp);
+        }
+        fclose(fp);
+    }
+
+    if (slicePath) {
+        long long dims[4] = {0, 0, 0, 0};
+        if (!sliceDims || sscanf(sliceDims, "%lld,%lld,%lld,%lld", &dims[0], &dims[1], &dims[2], &dims[3]) != 4)
+            return fail("--slices needs --slice-dims S,T,NBT,NBPT");
+        const CMonitor* mon = pBox->GetMonitor();
+        FILE* fp = fopen(slicePath, "wb");
+        if (!fp) return fail("cannot open slice file");
+        const BondVector& bonds = pState->GetBonds();
+        const BondPairVector& bps = pState->GetBondPairs();
+        long long hdr[6] = {dims[0], dims[1], dims[2], dims[3], (long long)bonds.size(), (long long)bps.size()};
+        fwrite("DPDSLICE", 1, 8, fp);
+        fwrite(hdr, 8, 6, fp);
+        for (long sl = 0; sl < dims[0]; ++sl)
+            for (long k = 0; k < dims[1] * dims[1]; ++k) {
+                const double q[9] = {mon->GetSliceStress11(sl, k), mon->GetSliceStress12(sl, k),
+                                     mon->GetSliceStress13(sl, k), mon->GetSliceStress21(sl, k),
+                                     mon->GetSliceStress22(sl, k), mon->GetSliceStress23(sl, k),
+                                     mon->GetSliceStress31(sl, k), mon->GetSliceStress32(sl, k),
+                                     mon->GetSliceStress33(sl, k)};
+                fwrite(q, 8, 9, fp);
+            }
+        for (long sl = 0; sl < dims[0]; ++sl)
+            for (long k = 0; k < dims[2]; ++k) {
+                const double q[9] = {mon->GetSliceStressBond11(sl, k), mon->GetSliceStressBond12(sl, k),
+                                     mon->GetSliceStressBond13(sl, k), mon->GetSliceStressBond21(sl, k),
+                                     mon->GetSliceStressBond22(sl, k), mon->GetSliceStressBond23(sl, k),
+                                     mon->GetSliceStressBond31(sl, k), mon->GetSliceStressBond32(sl, k),
+                                     mon->GetSliceStressBond33(sl, k)};
+                fwrite(q, 8, 9, fp);
+            }
+        for (long sl = 0; sl < dims[0]; ++sl)
+            for (long k = 0; k < dims[3]; ++k) {
+                const double q[9] = {mon->GetSliceStressBondPair11(sl, k), mon->GetSliceStressBondPair12(sl, k),
+                                     mon->GetSliceStressBondPair13(sl, k), mon->GetSliceStressBondPair21(sl, k),
+                                     mon->GetSliceStressBondPair22(sl, k), mon->GetSliceStressBondPair23(sl, k),
+                                     mon->GetSliceStressBondPair31(sl, k), mon->GetSliceStressBondPair32(sl, k),
+                                     mon->GetSliceStressBondPair33(sl, k)};
+                fwrite(q, 8, 9, fp);
+            }
+        for (size_t i = 0; i < bonds.size(); ++i) {
+            const long long t = bonds[i]->GetType();
+            fwrite(&t, 8, 1, fp);
+        }
+        for (size_t i = 0; i < bps.size(); ++i) {
+            const long long t = bps[i]->GetType();
+            fwrite(&t, 8, 1, fp);
         }
         fclose(fp);
     }

@@ -93,6 +93,8 @@ class DpdSystem:
     angle_second: np.ndarray
     angle_k3: np.ndarray
     angle_phi0: np.ndarray      # radians
+    bond_type: np.ndarray = None    # (nb,) int32: index of the bond's Bond line (CBond::GetType)
+    angle_type: np.ndarray = None   # (na,) int32: index of the pair's BondPair line (CBondPair::GetType)
 
     @property
     def n(self) -> int:
@@ -147,12 +149,12 @@ def _linear_topology(polymers: Sequence[PolymerSpec], bond_specs: Sequence[BondS
     """Bonds and bond pairs of linear polymers in the reference's order and
     head/tail convention (checked against the reference's own topology)."""
     bk = {}
-    for b in bond_specs:
-        bk[(b.name1, b.name2)] = bk[(b.name2, b.name1)] = (b.k2, b.l0)
+    for q, b in enumerate(bond_specs):
+        bk[(b.name1, b.name2)] = bk[(b.name2, b.name1)] = (b.k2, b.l0, q)
     pk = {}
-    for p in bp_specs:
-        pk[(p.name1, p.name2, p.name3)] = pk[(p.name3, p.name2, p.name1)] = (p.k3, math.radians(p.phi0_deg))
-    hs, ts, ks, ls, fs, ss, k3l, phl = [], [], [], [], [], [], [], []
+    for q, p in enumerate(bp_specs):
+        pk[(p.name1, p.name2, p.name3)] = pk[(p.name3, p.name2, p.name1)] = (p.k3, math.radians(p.phi0_deg), q)
+    hs, ts, ks, ls, fs, ss, k3l, phl, bts, ats = [], [], [], [], [], [], [], [], [], []
     next_id = 1
     bond_base = 0
     for poly in polymers:
@@ -176,17 +178,20 @@ def _linear_topology(polymers: Sequence[PolymerSpec], bond_specs: Sequence[BondS
             ts.append((start + np.array([b[1] for b in tb])[None, :]).ravel())
             ks.append(np.tile(np.array([b[2] for b in tb]), c))
             ls.append(np.tile(np.array([b[3] for b in tb]), c))
+            bts.append(np.tile(np.array([b[4] for b in tb]), c))
             if ta:
                 bstart = (bond_base + np.arange(c, dtype=np.int64) * nbp)[:, None]
                 fs.append((bstart + np.array([a[0] for a in ta])[None, :]).ravel())
                 ss.append((bstart + np.array([a[1] for a in ta])[None, :]).ravel())
                 k3l.append(np.tile(np.array([a[2] for a in ta]), c))
                 phl.append(np.tile(np.array([a[3] for a in ta]), c))
+                ats.append(np.tile(np.array([a[4] for a in ta]), c))
             bond_base += c * nbp
         next_id += poly.count * m
     cat = lambda xs, dt: (np.concatenate(xs).astype(dt) if xs else np.zeros(0, dtype=dt))
     return (cat(hs, np.int64), cat(ts, np.int64), cat(ks, np.float64), cat(ls, np.float64),
-            cat(fs, np.int64), cat(ss, np.int64), cat(k3l, np.float64), cat(phl, np.float64))
+            cat(fs, np.int64), cat(ss, np.int64), cat(k3l, np.float64), cat(phl, np.float64),
+            cat(bts, np.int32), cat(ats, np.int32))
 
 
 def _assemble(name, cells, widths, density, dt, lam, kT, seed, type_names, a, gamma,
@@ -194,7 +199,7 @@ def _assemble(name, cells, widths, density, dt, lam, kT, seed, type_names, a, ga
     n = types.shape[0]
     L = np.array([c * w for c, w in zip(cells, widths)], dtype=np.float64)
     x = _wrap(unpbc, L)
-    hb, tb, k2, l0, fa, sa, k3, phi = _linear_topology(polymers, bond_specs, bp_specs, type_names)
+    hb, tb, k2, l0, fa, sa, k3, phi, bty, aty = _linear_topology(polymers, bond_specs, bp_specs, type_names)
     return DpdSystem(
         name=name, cells=tuple(cells), widths=tuple(float(w) for w in widths), density=density,
         dt=dt, lam=lam, kT=kT, seed=seed, type_names=list(type_names), a=a, gamma=gamma,
@@ -203,7 +208,7 @@ def _assemble(name, cells, widths, density, dt, lam, kT, seed, type_names, a, ga
         movable=np.ones(n, dtype=np.uint8), x=x, unpbc=unpbc.astype(np.float64),
         v=v.astype(np.float64), f=np.zeros((n, 3), dtype=np.float64),
         bond_head=hb, bond_tail=tb, bond_k2=k2, bond_l0=l0,
-        angle_first=fa, angle_second=sa, angle_k3=k3, angle_phi0=phi)
+        angle_first=fa, angle_second=sa, angle_k3=k3, angle_phi0=phi, bond_type=bty, angle_type=aty)
 
 
 # ------------------------------------------------------------------ workloads
@@ -384,9 +389,10 @@ def polymer_fractions(system: DpdSystem) -> List[float]:
 
 
 def write_dmpci(system: DpdSystem, path: str, steps: int, kT: float = None, seed: int = None,
-                gamma_scale: float = 1.0, title: str = "synthetic") -> None:
+                gamma_scale: float = 1.0, title: str = "synthetic", grid_z: int = 1) -> None:
     """Osprey-DPD control data file (InputDPDFile.cpp:400-800) for ``system``
-    running ``steps`` steps with sampling, display and restart only at the end."""
+    running ``steps`` steps with sampling, display and restart only at the end;
+    ``grid_z`` analysis-grid slices along z (the slice stress profile's)."""
     T = len(system.type_names)
     lines = ["dpd", "", f'Title\t" {title} "', "Date    03/12/26",
              f'Comment\t" generated {system.name} system "', "", "State\trandom", ""]
@@ -420,7 +426,7 @@ def write_dmpci(system: DpdSystem, path: str, steps: int, kT: float = None, seed
               f"DensityPeriod  {steps}",
               f"DisplayPeriod  {steps}",
               f"RestartPeriod  {steps}",
-              "Grid  1 1 1", ""]
+              f"Grid  1 1 {int(grid_z)}", ""]
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
 
@@ -454,6 +460,21 @@ def read_dump(path: str):
     return {"n": n, "steps": steps, "id": rec["id"].copy(), "type": rec["type"].copy(),
             "x": rec["x"].copy(), "unpbc": rec["u"].copy(), "v": rec["v"].copy(), "f": rec["f"].copy(),
             "stress": rec["stress"].copy()}
+
+
+def read_slices(path: str):
+    """Slice stress dump of the reference harness (--slices)."""
+    with open(path, "rb") as fh:
+        if fh.read(8) != b"DPDSLICE":
+            raise ValueError("not a DPDSLICE file")
+        S, T, nbt, nbpt, nb, na = struct.unpack("<6q", fh.read(48))
+        rd = lambda cnt: np.frombuffer(fh.read(8 * cnt), dtype="<f8").copy()
+        pair = rd(S * T * T * 9).reshape(S, T * T, 9)
+        bond = rd(S * nbt * 9).reshape(S, nbt, 9)
+        bp = rd(S * nbpt * 9).reshape(S, nbpt, 9)
+        btype = np.frombuffer(fh.read(8 * nb), dtype="<i8").copy()
+        atype = np.frombuffer(fh.read(8 * na), dtype="<i8").copy()
+    return {"pair": pair, "bond": bond, "bondpair": bp, "bond_type": btype, "angle_type": atype}
 
 
 def read_topology(path: str):
