@@ -389,6 +389,40 @@ def run_replica_sweep(args, dev, torch, E):
     }
 
 
+def time_slice_profile(engine_mod, system, nslices: int, shape, dev, torch, steps: int = 20):
+    """Cost of the slice stress profile (CMonitor::AddBeadStress & co.) on a
+    sample step: per-kernel CUDA events over ``steps`` steps that all sample,
+    with and without the profile, mixed precision."""
+    from osprey_dpd_b200 import autotune
+    out = {"slices": nslices}
+    for on in (False, True):
+        eng = engine_mod.DpdEngine.from_system(system, precision=engine_mod.MIXED, device=dev.index)
+        if shape:
+            autotune.apply_shape(eng, shape)
+        if on:
+            eng.set_slice_stress_for(system, nslices)
+        eng.set_sample_period(1)
+        eng.step(1, 3)
+        eng.status()
+        eng.profile(True)
+        eng.step(4, steps)
+        eng.status()
+        p = eng.profile_read()
+        per = {k: v["ms"] / v["launches"] for k, v in p.items() if v["launches"]}
+        key = "with" if on else "without"
+        out[f"sample_step_ms_{key}"] = sum(p[k]["ms"] for k in p) / steps
+        if on:
+            out["slice_pairs_ms"] = per.get("slices")
+            out["bonds_ms_with"] = per.get("bonds")
+            out["status"] = eng.status()
+        else:
+            out["bonds_ms_without"] = per.get("bonds")
+        eng.close()
+    out["timing"] = ("CUDA events around every kernel, kernels launched one by one, every step a sample step; "
+                     "the profile is built on sample steps only")
+    return out
+
+
 def read_traffic(n_beads: int, scheme: str = "full"):
     """Per-launch DRAM bytes of the pair kernel (full, half or staged) from the
     committed ncu summary, scaled to the bead count."""
@@ -420,6 +454,8 @@ def main():
     ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged"], default="auto",
                     help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="also time the slice stress profile over this many z slices on sample steps")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -553,6 +589,8 @@ def main():
         "clocks": clocks,
         "status_bits": {k: v["status"] for k, v in results.items()},
     }
+    if args.slices > 0:
+        line["slice_profile"] = time_slice_profile(E, system, args.slices, mixed["shape"], dev, torch)
     print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -66,7 +66,8 @@ extern "C" {
 #define DPD_KERNEL_DOWNLOAD     7   /* slot order -> bead order                */
 #define DPD_KERNEL_KINETIC      8   /* kinetic sums without a step             */
 #define DPD_KERNEL_BONDED       9   /* bond + bond-pair forces (FP64)          */
-#define DPD_NUM_KERNELS         10
+#define DPD_KERNEL_SLICES      10   /* slice stress profile, pair part (sample steps) */
+#define DPD_NUM_KERNELS         11
 
 typedef struct dpd_engine dpd_engine;
 
@@ -198,6 +199,27 @@ DPD_API int dpd_engine_cells(dpd_engine* e, int32_t* cell);
  * step since the upload, the kinetic sums of the current state without a
  * virial (has_virial = 0). */
 DPD_API int dpd_engine_observables(dpd_engine* e, dpd_obs* out);
+
+/* Slice stress profile of the reference's CMonitor (AddBeadStress,
+ * AddBondStress, AddBondPairStress and ZeroSliceStress, Monitor.cpp:1900-2755;
+ * read by the stress-profile analysis, aaStressTensor1d.cpp:150-200).  With
+ * nslices > 0 every sample step splits each pair, bond and bond-pair
+ * contribution (force x separation, 9 components) over nslices z slices of
+ * width L_z/nslices (the analysis grid's GridZCellNo) and keeps it, in FP64,
+ * per type pair [slice][t1*T+t2][9], per bond type [slice][bond_type][9] and
+ * per bond-pair type [slice][bondpair_type][9]; bond_type[i] and
+ * bondpair_type[i] give the type of every uploaded bond and bond pair
+ * (CBond/CBondPair::GetType), nbondtypes/nbptypes their counts.  Bead 1 of a
+ * pair is the reference's for pairs in different cells; inside one cell the
+ * split between t1*T+t2 and t2*T+t1 can differ from the reference's (its
+ * list order), so only their sum is comparable.  A degenerate bond pair
+ * (|b1||b2| <= 1e-4) adds zero.  Single-box engines; call after the topology
+ * upload, which turns the profile off again.  nslices = 0 turns it off. */
+DPD_API int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t nbondtypes, const int32_t* bond_type,
+                                        int32_t nbptypes, const int32_t* bondpair_type);
+/* The slice stress profile of the latest sample step (synchronous); arrays
+ * sized as above, any pointer may be NULL. */
+DPD_API int dpd_engine_slice_stress(dpd_engine* e, double* pair, double* bond, double* bondpair);
 
 /* Queues all further work on the caller's CUDA stream (a cudaStream_t passed
  * as a plain pointer; NULL returns to the engine's own stream).  The stream

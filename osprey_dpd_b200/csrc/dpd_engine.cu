@@ -20,6 +20,7 @@
 #include "dpd_kernels.cuh"
 #include "pair_forces.cuh"
 #include "pair_staged.cuh"
+#include "slice_stress.cuh"
 
 using namespace dpd;
 
@@ -86,6 +87,16 @@ struct dpd_engine {
     double4* d_ubuf = nullptr;            // unPBC position of bonded beads by upload index (FP64)
     int* d_bb = nullptr;                  // bonded beads' upload indices, ascending
     int64_t nbb = 0;
+    int64_t topo_nb = 0, topo_na = 0;     // bonds and bond pairs of the uploaded topology
+
+    // slice stress profile (CMonitor::AddBeadStress & co.), built on sample steps
+    int slice_S = 0, slice_nbt = 0, slice_nbpt = 0;
+    double* d_slice = nullptr;            // pair | bond | bondpair bins, one allocation
+    size_t cap_slice = 0;
+    int* d_slice_bt = nullptr;            // bond type per bond
+    int* d_slice_bpt = nullptr;           // bond-pair type per bond pair
+    size_t cap_slice_bt = 0, cap_slice_bpt = 0;
+    bool slice_sampled = false;           // a sample step has filled the bins
     double4* d_Fb = nullptr;              // bonded force by upload index (FP64)
     double* d_Sb = nullptr;               // bond virial, 9 planes by upload index (sample steps)
     double* d_off = nullptr;
@@ -379,6 +390,32 @@ int set_pair_attributes(dpd_engine* e)
     return DPD_OK;
 }
 
+// Slice-profile parameters of the engine (S = 0 when off).
+SliceParams slice_params(const dpd_engine* e)
+{
+    SliceParams sp{};
+    if (!e->slice_S) return sp;
+    const int S = e->slice_S, KT = e->ntypes * e->ntypes;
+    sp.S = S;
+    sp.width = e->hboxes[0].L[2] / (double)S;   // m_GridZCellWidth, Monitor.cpp:247
+    sp.inv = 1.0 / sp.width;                    // m_invSliceWidth, Monitor.cpp:2185
+    sp.nbt = e->slice_nbt;
+    sp.nbpt = e->slice_nbpt;
+    sp.pair = e->d_slice;
+    sp.bond = e->d_slice + (size_t)S * KT * 9;
+    sp.bondpair = sp.bond + (size_t)S * e->slice_nbt * 9;
+    sp.bond_type = e->d_slice_bt;
+    sp.bondpair_type = e->d_slice_bpt;
+    return sp;
+}
+
+size_t slice_bins(const dpd_engine* e)
+{
+    return (size_t)e->slice_S * 9 * ((size_t)e->ntypes * e->ntypes + e->slice_nbt + e->slice_nbpt);
+}
+
+constexpr size_t kSliceSmemMax = 160 * 1024;   // block-private pair bins up to this size
+
 // One timestep.  The first step of a call starts with k_update_pos; the
 // others had their UpdatePos fused into the k_update_mom before them, which
 // does so for every step but the last of the call.
@@ -423,9 +460,12 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     if ((rc = check_launch(e, "k_gather"))) return rc;
     // bond and bond-pair forces: a branch beside the pair kernel (on the
     // launching stream itself while profiling, so every kernel is timed)
+    const bool slices = sample && e->slice_S > 0;
+    const SliceParams sp = slices ? slice_params(e) : SliceParams{};
+    if (slices) CU(cudaMemsetAsync(e->d_slice, 0, slice_bins(e) * sizeof(double), st));
     const Topology topo{e->d_csr_ptr, e->d_csr_term, e->d_bond_h, e->d_bond_t, e->d_bond_k2, e->d_bond_l0,
                         e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_ang_k3, e->d_ang_cos0,
-                        e->d_ang_sin0, e->d_ubuf};
+                        e->d_ang_sin0, e->d_ubuf, sp};
     const bool fork = e->nbb > 0 && !e->profiling;
     if (e->nbb > 0) {
         cudaStream_t bst = st;
@@ -463,6 +503,17 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
                                                                (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status);
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
+    if (slices) {
+        const size_t smem = (size_t)e->slice_S * e->ntypes * e->ntypes * 9 * sizeof(double);
+        const int sb = smem <= kSliceSmemMax;
+        Timed t(e, DPD_KERNEL_SLICES);
+        k_slice_pairs<real><<<e->sms * 2, 256, sb ? smem : 0, st>>>(n, e->d_K, e->d_boxes, e->d_step,
+                                                                     (const real*)e->d_tab, e->d_cell[b],
+                                                                     e->d_start, (const V4*)e->d_pos4,
+                                                                     (const V4*)e->d_vel4, e->d_x[b], sp, sb);
+        if ((rc = check_launch(e, "k_slice_pairs"))) return rc;
+        e->slice_sampled = true;
+    }
     if (fork) CU(cudaStreamWaitEvent(st, e->ev_join, 0));
     {
         Timed t(e, DPD_KERNEL_UPDATE_MOM);
@@ -535,6 +586,7 @@ int empty_topology(dpd_engine* e)
     CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
     if (moved || e->nbb) drop_graphs(e);
     e->nbb = 0;
+    e->topo_nb = e->topo_na = 0;
     return DPD_OK;
 }
 
@@ -1077,7 +1129,71 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         CU(cudaMemcpy(e->d_ang_cos0, acos0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_ang_sin0, asin0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
     }
+    e->topo_nb = nb;
+    e->topo_na = na;
+    // the slice profile's bond types refer to the previous topology
+    if (e->slice_S) { e->slice_S = 0; drop_graphs(e); }
     if (moved) drop_graphs(e);
+    return DPD_OK;
+}
+
+int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t nbondtypes, const int32_t* bond_type,
+                                int32_t nbptypes, const int32_t* bondpair_type)
+{
+    if (!e) return DPD_E_ARG;
+    if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "the slice stress profile needs a single-box engine");
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads (and the topology) before the slice profile");
+    if (nslices < 0 || nslices > 65536 || nbondtypes < 0 || nbptypes < 0 || nbondtypes > 65536 || nbptypes > 65536)
+        return fail(e, DPD_E_ARG, "slice profile sizes out of range");
+    if (nslices > 0 && ((e->topo_nb > 0 && !bond_type) || (e->topo_na > 0 && !bondpair_type)))
+        return fail(e, DPD_E_ARG, "bond and bond-pair types are required for the uploaded topology");
+    for (int64_t i = 0; nslices > 0 && i < e->topo_nb; ++i)
+        if (bond_type[i] < 0 || bond_type[i] >= nbondtypes) return fail(e, DPD_E_ARG, "bond type out of range");
+    for (int64_t i = 0; nslices > 0 && i < e->topo_na; ++i)
+        if (bondpair_type[i] < 0 || bondpair_type[i] >= nbptypes)
+            return fail(e, DPD_E_ARG, "bond-pair type out of range");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    drop_graphs(e);
+    e->slice_S = 0;
+    e->slice_sampled = false;
+    if (nslices == 0) return DPD_OK;
+    e->slice_nbt = nbondtypes;
+    e->slice_nbpt = nbptypes;
+    e->slice_S = nslices;
+    int rc;
+    bool moved = false;
+    if ((rc = ensure(e, &e->d_slice, e->cap_slice, slice_bins(e), &moved))) { e->slice_S = 0; return rc; }
+    if (e->topo_nb) {
+        if ((rc = ensure(e, &e->d_slice_bt, e->cap_slice_bt, (size_t)e->topo_nb, &moved))) { e->slice_S = 0; return rc; }
+        CU(cudaMemcpy(e->d_slice_bt, bond_type, sizeof(int) * e->topo_nb, cudaMemcpyHostToDevice));
+    }
+    if (e->topo_na) {
+        if ((rc = ensure(e, &e->d_slice_bpt, e->cap_slice_bpt, (size_t)e->topo_na, &moved))) { e->slice_S = 0; return rc; }
+        CU(cudaMemcpy(e->d_slice_bpt, bondpair_type, sizeof(int) * e->topo_na, cudaMemcpyHostToDevice));
+    }
+    CU(cudaMemset(e->d_slice, 0, slice_bins(e) * sizeof(double)));
+    const size_t smem = (size_t)nslices * e->ntypes * e->ntypes * 9 * sizeof(double);
+    if (smem <= kSliceSmemMax) {
+        CU(cudaFuncSetAttribute(k_slice_pairs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CU(cudaFuncSetAttribute(k_slice_pairs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    return DPD_OK;
+}
+
+int dpd_engine_slice_stress(dpd_engine* e, double* pair, double* bond, double* bondpair)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->slice_S) return fail(e, DPD_E_STATE, "the slice stress profile is off");
+    if (!e->slice_sampled) return fail(e, DPD_E_STATE, "no sample step has built the slice stress profile yet");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    const SliceParams sp = slice_params(e);
+    const size_t S = (size_t)e->slice_S;
+    if (pair) CU(cudaMemcpy(pair, sp.pair, S * e->ntypes * e->ntypes * 9 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (bond) CU(cudaMemcpy(bond, sp.bond, S * e->slice_nbt * 9 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (bondpair)
+        CU(cudaMemcpy(bondpair, sp.bondpair, S * e->slice_nbpt * 9 * sizeof(double), cudaMemcpyDeviceToHost));
     return DPD_OK;
 }
 

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256, 6) k_gather(
         double u[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) u[q] = xs[q] + (double)img_get(im, q) * B.L[q] + (off ? off[q * n + b] : 0.0);
-        ubuf[b] = make_double4(u[0], u[1], u[2], 0.0);
+        ubuf[b] = make_double4(u[0], u[1], u[2], xs[2]);   // w: wrapped z, for the slice stress profile
     }
 }
 
@@ -471,6 +471,82 @@ __global__ void __launch_bounds__(128) k_pair_forces_ref(
 
 // -------------------------------------------------------------- UpdateMom
 
+// ------------------------------------------------- slice stress profile
+// CMonitor::AddBeadStress / AddBondStress / AddBondPairStress
+// (Monitor.cpp:1900-2755); see slice_stress.cuh.
+
+struct SliceParams {
+    int S;              // slices (0 = off)
+    double width;       // L_z / S (Monitor.cpp:247)
+    double inv;         // 1 / width (Monitor.cpp:2185)
+    int nbt, nbpt;      // bond and bond-pair types
+    double* pair;       // [S][T*T][9]
+    double* bond;       // [S][nbt][9]
+    double* bondpair;   // [S][nbpt][9]
+    const int* bond_type;       // per bond
+    const int* bondpair_type;   // per bond pair
+};
+
+__device__ __forceinline__ void outer9(const double f[3], const double d[3], double o[9])
+{
+    o[0] = f[0] * d[0]; o[1] = f[0] * d[1]; o[2] = f[0] * d[2];
+    o[3] = f[1] * d[0]; o[4] = f[1] * d[1]; o[5] = f[1] * d[2];
+    o[6] = f[2] * d[0]; o[7] = f[2] * d[1]; o[8] = f[2] * d[2];
+}
+
+__device__ __forceinline__ void slice_put(double* arr, int K, int idx, int sl, const double fdx[9], double fac,
+                                          bool scale)
+{
+    double* q = arr + ((size_t)sl * K + idx) * 9;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) atomicAdd(q + c, scale ? fdx[c] * fac : fdx[c]);
+}
+
+// One contribution over the slices between two beads: za is the z of the
+// bead the separation points to (bead 1, bond head, bead j+1), zb the
+// other's, zDiff the separation's z component.  Same branch structure and
+// arithmetic as the reference's three functions.
+__device__ __forceinline__ void slice_add(const SliceParams& sp, double* arr, int K, int idx, const double fdx[9],
+                                          double zDiff, double za, double zb)
+{
+    double up, lo;
+    if (zDiff > 0.00001) {
+        up = za * sp.inv;
+        lo = zb * sp.inv;
+    } else if (zDiff < -0.00001) {
+        zDiff = -zDiff;
+        up = zb * sp.inv;
+        lo = za * sp.inv;
+    } else {
+        up = za * sp.inv;
+        lo = up;
+    }
+    const int S = sp.S;
+    int ui = (int)up;
+    const double ur = up - (double)ui;
+    int li = (int)lo;
+    const double lr = lo - (double)li;
+    if (ui < 0 || ui >= S || li < 0 || li >= S || idx < 0 || idx >= K) return;   // a z rounded up to L_z
+    if (ui == li) {
+        if (up != lo || ur > 0.00001) {
+            slice_put(arr, K, idx, li, fdx, 1.0, false);
+        } else {
+            slice_put(arr, K, idx, ui, fdx, 0.5, true);
+            if (--li < 0) li += S;
+            slice_put(arr, K, idx, li, fdx, 0.5, true);
+        }
+    } else {
+        const double inner = sp.width / zDiff;
+        if (ui > li) {
+            for (int k = li + 1; k <= ui - 1; ++k) slice_put(arr, K, idx, k, fdx, inner, true);
+        } else {
+            for (int kp = li + 1; kp <= S + ui - 1; ++kp) slice_put(arr, K, idx, kp >= S ? kp - S : kp, fdx, inner, true);
+        }
+        slice_put(arr, K, idx, li, fdx, lr > 0.000001 ? (1.0 - lr) * inner : inner, true);
+        if (ur > 0.000001) slice_put(arr, K, idx, ui, fdx, ur * inner, true);
+    }
+}
+
 struct Topology {
     const int* csr_ptr;     // per bead (upload index): first term
     const int* csr_term;    // term = index * 8 + code
@@ -485,7 +561,8 @@ struct Topology {
     const double* ang_k3;
     const double* ang_cos0; // cos(phi0); 1 when phi0 <= 0
     const double* ang_sin0; // sin(phi0); exactly 0 when phi0 <= 0 (the k3/|b1||b2| branch)
-    const double4* ubuf;    // unPBC position by upload index, written by k_gather for bonded beads
+    const double4* ubuf;    // unPBC position by upload index (w: wrapped z), written by k_gather for bonded beads
+    SliceParams sp;         // slice stress profile on sample steps (sp.S = 0: off)
 };
 
 enum TermCode { kBondHead = 0, kBondTail = 1, kAngle0 = 2, kAngle1 = 3, kAngle2 = 4 };
@@ -536,6 +613,13 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
                         bs[0] += bx * gx; bs[1] += by * gx; bs[2] += bz * gx;
                         bs[3] += bx * gy; bs[4] += by * gy; bs[5] += bz * gy;
                         bs[6] += bx * gz; bs[7] += by * gz; bs[8] += bz * gz;
+                        if (topo.sp.S) {   // CMonitor::AddBondStress, once per bond (its head bead)
+                            const double g[3] = {gx, gy, gz}, bv[3] = {bx, by, bz};
+                            double fdx[9];
+                            outer9(g, bv, fdx);
+                            slice_add(topo.sp, topo.sp.bond, topo.sp.nbt, topo.sp.bond_type[idx], fdx, bz,
+                                      topo.ubuf[h].w, topo.ubuf[tl].w);
+                        }
                     }
                 } else {
                     bf[0] -= gx; bf[1] -= gy; bf[2] -= gz;
@@ -558,6 +642,7 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
                 const double l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
                 const double l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
                 const double mag = l1 * l2;
+                double G0[3] = {0.0, 0.0, 0.0}, G2[3] = {0.0, 0.0, 0.0};
                 if (mag > 0.0001) {
                     const double dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
                     const double o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
@@ -572,9 +657,39 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
                     for (int d = 0; d < 3; ++d) {
                         const double g0 = fm * (o1 * b1[d] - b2[d]);
                         const double g2 = fm * (b1[d] - o2 * b2[d]);
+                        G0[d] = g0;
+                        G2[d] = g2;
                         if (code == kAngle0) bf[d] += g0;
                         else if (code == kAngle2) bf[d] += g2;
                         else bf[d] += -g0 - g2;
+                    }
+                }
+                if (SAMPLE && topo.sp.S && code == kAngle0) {
+                    // CMonitor::AddBondPairStress, once per bond pair (its first tail bead): segments
+                    // first.tail -> first.head -> second.head -> first.tail, force 0.33333333 *
+                    // (F[j+1] - F[j]).  A degenerate pair (|b1||b2| <= 1e-4) adds zero here; the
+                    // reference would reuse the forces of its last non-degenerate step.
+                    const double* U[4] = {u1t, u1h, u2h, u1t};
+                    const double Z[4] = {topo.ubuf[a1t].w, topo.ubuf[a1h].w, topo.ubuf[a2h].w, topo.ubuf[a1t].w};
+                    double FF[4][3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        FF[0][d] = G0[d];
+                        FF[1][d] = -G0[d] - G2[d];
+                        FF[2][d] = G2[d];
+                        FF[3][d] = G0[d];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        double dv[3], fo[3], fdx[9];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            dv[d] = U[j + 1][d] - U[j][d];
+                            fo[d] = 0.33333333 * (FF[j + 1][d] - FF[j][d]);
+                        }
+                        outer9(fo, dv, fdx);
+                        slice_add(topo.sp, topo.sp.bondpair, topo.sp.nbpt, topo.sp.bondpair_type[idx], fdx, dv[2],
+                                  Z[j + 1], Z[j]);
                     }
                 }
             }

@@ -37,10 +37,11 @@ EXPORTED = [
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
+    "dpd_engine_set_slice_stress", "dpd_engine_slice_stress",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
-                "reduce_obs", "download", "kinetic", "bonds"]
+                "reduce_obs", "download", "kinetic", "bonds", "slices"]
 
 
 class DpdParams(C.Structure):
@@ -105,6 +106,8 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
     L.dpd_engine_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
     L.dpd_engine_set_pair_scheme.argtypes = [vp, C.c_int32]
+    L.dpd_engine_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
+    L.dpd_engine_slice_stress.argtypes = [vp, vp, vp, vp]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
     L.dpd_batch_create.argtypes = [C.POINTER(DpdParams), C.c_int32, C.POINTER(DpdBox), C.POINTER(vp)]
@@ -222,6 +225,33 @@ class DpdEngine:
     def set_launch_shape(self, hitcap: int = 32, persistent_blocks_per_sm: int = 0, carveout: int = -1) -> None:
         self._check(load().dpd_engine_set_launch_shape(self.h, int(hitcap), int(persistent_blocks_per_sm),
                                                        int(carveout)), "set_launch_shape")
+
+    def set_slice_stress(self, nslices: int, bond_type=None, nbondtypes: int = 0, bondpair_type=None,
+                         nbptypes: int = 0) -> None:
+        """Slice stress profile over ``nslices`` z slices on sample steps
+        (CMonitor::AddBeadStress & co.); 0 turns it off."""
+        self._sl_bt = np.ascontiguousarray(bond_type if bond_type is not None else [], np.int32)
+        self._sl_bpt = np.ascontiguousarray(bondpair_type if bondpair_type is not None else [], np.int32)
+        self._check(load().dpd_engine_set_slice_stress(self.h, int(nslices), int(nbondtypes), _p(self._sl_bt),
+                                                       int(nbptypes), _p(self._sl_bpt)), "set_slice_stress")
+        self._slice_dims = (int(nslices), int(self._a.shape[0]), int(nbondtypes), int(nbptypes))
+
+    def set_slice_stress_for(self, system, nslices: int) -> None:
+        """set_slice_stress with the bond and bond-pair types of a workloads.DpdSystem."""
+        self.set_slice_stress(nslices, system.bond_type, len(system.bond_specs), system.angle_type,
+                              len(system.bondpair_specs))
+
+    def slice_stress(self) -> dict:
+        """{"pair": [S][T*T][9], "bond": [S][NBT][9], "bondpair": [S][NBPT][9]}
+        of the latest sample step."""
+        dims = getattr(self, "_slice_dims", None)
+        if dims is None or dims[0] == 0:   # off: let the engine report it
+            self._check(load().dpd_engine_slice_stress(self.h, None, None, None), "slice_stress")
+        S, T, nbt, nbpt = dims
+        out = {"pair": np.zeros((S, T * T, 9)), "bond": np.zeros((S, nbt, 9)), "bondpair": np.zeros((S, nbpt, 9))}
+        self._check(load().dpd_engine_slice_stress(self.h, _p(out["pair"]), _p(out["bond"]), _p(out["bondpair"])),
+                    "slice_stress")
+        return out
 
     def set_pair_scheme(self, scheme: int) -> None:
         """PAIR_FULL_SHELL (reproducible), PAIR_HALF_SHELL (each pair once) or
