@@ -75,6 +75,13 @@ struct dpd_engine {
     int* d_tf[2] = {nullptr, nullptr};
     uint32_t* d_img[2] = {nullptr, nullptr};
     int* d_cell[2] = {nullptr, nullptr};
+    // UpdatePos of the next call's first step, done by the last k_update_mom of
+    // a call into these buffers (the visible state keeps the step's own x, img, cell)
+    double* d_xa = nullptr;
+    uint32_t* d_imga = nullptr;
+    int* d_cella = nullptr;
+    bool ahead_valid = false;    // d_xa/d_imga/d_cella and the arrival counts hold the next drift
+    bool ahead_enabled = true;
     void* d_F = nullptr;        // current force, slot order (real)
     void* d_Fold = nullptr;     // previous force, slot order (real)
     void* d_stress = nullptr;   // per-bead virial of the last sample step (real, 9 planes)
@@ -146,6 +153,7 @@ struct dpd_engine {
     // captured multi-step sequences (DPD_GRAPHS=0 disables)
     struct Graph {
         int nsteps, parity;
+        bool from_ahead, to_ahead;
         std::vector<char> samples;
         cudaStream_t stream;
         cudaGraphExec_t exec;
@@ -227,8 +235,21 @@ int check_launch(dpd_engine* e, const char* what)
 // Host mirror of StepConst, the box table and the pair tables
 // (CCNTCell::SetTimeStepConstants, CNTCell.cpp:180-203;
 // sigma_ij = sqrt(gamma_ij) * sqrt(24 kT / dt), CNTCell.cpp:190,1220).
+// Forget a drift done ahead by the last call (its arrival counts included),
+// before anything that changes what that drift computed.
+int drop_ahead(dpd_engine* e)
+{
+    if (!e->ahead_valid) return DPD_OK;
+    CU(cudaMemsetAsync(e->d_count, 0, sizeof(int) * (size_t)e->ncell, e->s()));
+    CU(cudaMemsetAsync(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk, e->s()));
+    e->ahead_valid = false;
+    return DPD_OK;
+}
+
 int push_constants(dpd_engine* e)
 {
+    int rc0;
+    if ((rc0 = drop_ahead(e))) return rc0;   // the drift done ahead used the old constants
     const dpd_params& p = e->params;
     StepConst K{};
     K.dt = p.dt;
@@ -420,7 +441,7 @@ constexpr size_t kSliceSmemMax = 160 * 1024;   // block-private pair bins up to 
 // others had their UpdatePos fused into the k_update_mom before them, which
 // does so for every step but the last of the call.
 template <typename real>
-int queue_step(dpd_engine* e, bool sample, bool first, bool last)
+int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahead, bool to_ahead)
 {
     typedef typename Vec4<real>::type V4;
     const int n = (int)e->n;
@@ -428,7 +449,13 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     const int nb = blocks_for(n, kThreads);
     cudaStream_t st = e->s();
     int rc;
-    if (first) {
+    // the first step of a call drifts here unless the previous call's last
+    // k_update_mom did it already (from_ahead: x, img, cell from the ahead buffers)
+    const bool ahead_in = first && from_ahead;
+    double* x_in = ahead_in ? e->d_xa : e->d_x[a];
+    uint32_t* img_in = ahead_in ? e->d_imga : e->d_img[a];
+    int* cell_in = ahead_in ? e->d_cella : e->d_cell[a];
+    if (first && !from_ahead) {
         {
             Timed t(e, DPD_KERNEL_UPDATE_POS);
             k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
@@ -446,14 +473,14 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     {
         Timed t(e, DPD_KERNEL_PERMUTE);
         k_permute<<<blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st>>>(
-            n, e->nchunk, e->d_cell[a], e->d_rank, e->d_start, e->d_perm, e->d_block_count);
+            n, e->nchunk, cell_in, e->d_rank, e->d_start, e->d_perm, e->d_block_count);
     }
     if ((rc = check_launch(e, "k_permute"))) return rc;
     {
         Timed t(e, DPD_KERNEL_GATHER);
         k_gather<real><<<nb, kThreads, 0, st>>>(
-            n, e->d_K, e->d_boxes, e->d_perm, e->d_start, e->d_x[a], e->d_v[a], (const real*)e->d_F, e->d_bid[a],
-            e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
+            n, e->d_K, e->d_boxes, e->d_perm, e->d_start, x_in, e->d_v[a], (const real*)e->d_F, e->d_bid[a],
+            e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
             e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b], (V4*)e->d_pos4, (V4*)e->d_vel4,
             e->d_ubuf, e->off_active ? e->d_off : nullptr);
     }
@@ -517,12 +544,18 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last)
     if (fork) CU(cudaStreamWaitEvent(st, e->ev_join, 0));
     {
         Timed t(e, DPD_KERNEL_UPDATE_MOM);
-        auto kern = sample ? (last ? k_update_mom<real, true, false> : k_update_mom<real, true, true>)
-                           : (last ? k_update_mom<real, false, false> : k_update_mom<real, false, true>);
+        // the next step's drift: in place between the steps of a call, into
+        // the ahead buffers after the last one (or not at all)
+        const bool pos = !last || to_ahead;
+        auto kern = sample ? (pos ? k_update_mom<real, true, true> : k_update_mom<real, true, false>)
+                           : (pos ? k_update_mom<real, false, true> : k_update_mom<real, false, false>);
+        double* xo = last ? e->d_xa : e->d_x[b];
+        uint32_t* imgo = last ? e->d_imga : e->d_img[b];
+        int* cello = last ? e->d_cella : e->d_cell[b];
         kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
                                        (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_Fb, e->d_Sb,
                                        (real*)e->d_stress, e->d_partials, e->d_img[b], e->d_cell[b], e->d_rank,
-                                       e->d_count, e->d_block_count, e->d_status);
+                                       e->d_count, e->d_block_count, e->d_status, xo, imgo, cello);
     }
     if ((rc = check_launch(e, "k_update_mom"))) return rc;
     if (sample) {
@@ -556,6 +589,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
             else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
+            else if (key == "ahead") e->ahead_enabled = val != 0;
         }
         pos = end + 1;
     }
@@ -831,6 +865,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
     if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
     CU(cudaSetDevice(e->device));
+    if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
     CU(cudaStreamSynchronize(e->s()));
     // CSimBox::AssignBeadstoCells (SimBox.cpp:715-762): ix = (long)(x/w), box-local coordinates
     std::vector<int> cell(n);
@@ -898,10 +933,14 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
                          &e->d_F, &e->d_Fold, &e->d_stress, &e->d_pos4, &e->d_vel4, (void**)&e->d_rank,
                          (void**)&e->d_perm, (void**)&e->d_pid[0], (void**)&e->d_pid[1], (void**)&e->d_pid_of,
                          (void**)&e->d_partials,
-                         (void**)&e->d_out, (void**)&e->d_out_cell};
+                         (void**)&e->d_out, (void**)&e->d_out_cell, (void**)&e->d_xa, (void**)&e->d_imga,
+                         (void**)&e->d_cella};
         for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
         const size_t rs = real_size(e);
         int rc;
+        if ((rc = dalloc(e, &e->d_xa, 3 * (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_imga, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_cella, (size_t)n))) return rc;
         for (int k = 0; k < 2; ++k) {
             if ((rc = dalloc(e, &e->d_x[k], 3 * (size_t)n))) return rc;
             if ((rc = dalloc(e, &e->d_v[k], 3 * (size_t)n))) return rc;
@@ -1269,6 +1308,7 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     CU(cudaGetLastError());
     e->launches += 1;
     std::vector<char> samples(nsteps);
+    const bool from_ahead = e->ahead_valid, to_ahead = e->ahead_enabled;
     for (int32_t k = 0; k < nsteps; ++k) {
         const int64_t t = first_step + k;
         // ISimState::TimeToSample (ISimState.cpp:468-471): m_SimTime % SamplePeriod == 0
@@ -1277,8 +1317,9 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     auto queue_all = [&](void) -> int {
         for (int32_t k = 0; k < nsteps; ++k) {
             const bool first = k == 0, last = k == nsteps - 1;
-            const int rc = (e->precision == DPD_PRECISION_FP64) ? queue_step<double>(e, samples[k], first, last)
-                                                                 : queue_step<float>(e, samples[k], first, last);
+            const int rc = (e->precision == DPD_PRECISION_FP64)
+                               ? queue_step<double>(e, samples[k], first, last, from_ahead, to_ahead)
+                               : queue_step<float>(e, samples[k], first, last, from_ahead, to_ahead);
             if (rc) return rc;
         }
         return DPD_OK;
@@ -1288,7 +1329,8 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
         // one captured graph per (step count, buffer parity, sample pattern, stream)
         dpd_engine::Graph* g = nullptr;
         for (auto& cand : e->graphs)
-            if (cand.nsteps == nsteps && cand.parity == parity && cand.samples == samples && cand.stream == e->s())
+            if (cand.nsteps == nsteps && cand.parity == parity && cand.samples == samples && cand.stream == e->s() &&
+                cand.from_ahead == from_ahead && cand.to_ahead == to_ahead)
                 g = &cand;
         if (!g) {
             if (e->graphs.size() >= 16) drop_graphs(e);
@@ -1311,7 +1353,7 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
             ce = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             if (ce != cudaSuccess) return fail(e, DPD_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-            e->graphs.push_back({nsteps, parity, samples, e->s(), exec, e->launches - launches0});
+            e->graphs.push_back({nsteps, parity, from_ahead, to_ahead, samples, e->s(), exec, e->launches - launches0});
             g = &e->graphs.back();
             e->launches = launches0;   // counted per replay below
             e->cur = parity;
@@ -1329,6 +1371,7 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
             e->last_sample_step = first_step + k;
             break;
         }
+    e->ahead_valid = to_ahead;
     e->stepped = true;
     e->obs_valid = false;
     e->box_obs_valid = false;

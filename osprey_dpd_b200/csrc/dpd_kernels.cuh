@@ -708,15 +708,19 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
 // them), keep accumulating force.  On sample steps the FP64 single-bead sums
 // are reduced per block.  With POS the same thread goes on with the next
 // step's UpdatePos (drift, cell move, arrival counts), which saves a launch
-// and a second pass over x, v, F and the flags.
+// and a second pass over x, v, F and the flags; the drifted x, img and cell
+// go to xo, imgo, cello -- the state arrays themselves between the steps of
+// a call, separate buffers after its last step (the state the caller sees
+// stays the step's own).  Each thread reads slot s before it writes it.
 template <typename real, bool SAMPLE, bool POS>
 __global__ void __launch_bounds__(256, 4) k_update_mom(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, int64_t* __restrict__ step_ptr,
-    double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
+    const double* x, double* __restrict__ v, real* __restrict__ F,
     const real* __restrict__ Fold, const int* __restrict__ bid, const int* __restrict__ tf,
     const double4* __restrict__ Fb, const double* __restrict__ Sb,
-    real* __restrict__ stress, double* __restrict__ partials, uint32_t* __restrict__ img, int* __restrict__ cell,
-    int* __restrict__ rank, int* __restrict__ count, int* __restrict__ block_count, unsigned* __restrict__ status)
+    real* __restrict__ stress, double* __restrict__ partials, const uint32_t* img, const int* cell,
+    int* __restrict__ rank, int* __restrict__ count, int* __restrict__ block_count, unsigned* __restrict__ status,
+    double* xo, uint32_t* imgo, int* cello)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = s < n;
@@ -777,7 +781,7 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
         if (POS) {
             // UpdatePos of the next step (the drift uses this step's v and F)
             const double f0[3] = {(double)f[0], (double)f[1], (double)f[2]};
-            cnew = drift_and_move(K, boxes, n, s, c, tfl, xs, vn, f0, im0, x, img, cell, bad);
+            cnew = drift_and_move(K, boxes, n, s, c, tfl, xs, vn, f0, im0, xo, imgo, cello, bad);
         }
         if (SAMPLE) {
 #pragma unroll
