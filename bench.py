@@ -423,6 +423,28 @@ def time_slice_profile(engine_mod, system, nslices: int, shape, dev, torch, step
     return out
 
 
+def time_monitor(engine_mod, system, dev, reps: int = 10):
+    """Wall time of one synchronous dpd_engine_monitor call (CMonitor sample
+    data on the device) and of the full state download a host-side monitor
+    would need instead, mixed precision, after 20 steps."""
+    eng = engine_mod.DpdEngine.from_system(system, precision=engine_mod.MIXED, device=dev.index)
+    eng.set_monitor_for(system)
+    eng.step(1, 20)
+    eng.status()
+    eng.monitor()
+    eng.download()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        eng.monitor()
+    t1 = time.perf_counter()
+    for _ in range(reps):
+        eng.download()
+    t2 = time.perf_counter()
+    eng.close()
+    return {"monitor_ms": 1000.0 * (t1 - t0) / reps, "download_ms": 1000.0 * (t2 - t1) / reps,
+            "timing": "host wall clock around synchronous calls"}
+
+
 def read_traffic(n_beads: int, scheme: str = "full"):
     """Per-launch DRAM bytes of the pair kernel (full, half or staged) from the
     committed ncu summary, scaled to the bead count."""
@@ -454,6 +476,8 @@ def main():
     ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged"], default="auto",
                     help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
+    ap.add_argument("--monitor", action="store_true",
+                    help="also time dpd_engine_monitor against the state download it replaces")
     ap.add_argument("--slices", type=int, default=0,
                     help="also time the slice stress profile over this many z slices on sample steps")
     args = ap.parse_args()
@@ -591,6 +615,8 @@ def main():
     }
     if args.slices > 0:
         line["slice_profile"] = time_slice_profile(E, system, args.slices, mixed["shape"], dev, torch)
+    if args.monitor:
+        line["monitor"] = time_monitor(E, system, dev)
     print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -221,6 +221,42 @@ DPD_API int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t 
  * sized as above, any pointer may be NULL. */
 DPD_API int dpd_engine_slice_stress(dpd_engine* e, double* pair, double* bond, double* bondpair);
 
+/* CMonitor sample data beyond dpd_obs, computed on the device from the
+ * current state when dpd_engine_monitor is called (so a sample needs no state
+ * download):
+ *   CalculateSingleBeadData     Monitor.cpp:790-1040  inertia tensor / N,
+ *                               per-type MSD / (6 dt t N_type) from the initial
+ *                               unPBC positions (at t = 0: / N_type)
+ *   CalculateSinglePolymerData  Monitor.cpp:708-788   mean end-to-end distance
+ *                               per polymer type (head - tail, minimum image)
+ *   CalculateSingleBondData     Monitor.cpp:1052-1174 mean bond length per bond
+ *                               type, global mean and mean square
+ *   CalculateSingleBondPairData Monitor.cpp:1176-1273 per bond-pair type: P2,
+ *                               first and second bond length, phi - phi0, its
+ *                               square, and the ratio <dphi^2>/<dphi>^2
+ * dpd_engine_set_monitor gives the bond and bond-pair types of the uploaded
+ * topology, the polymers (head and tail bead ids, type) and the initial
+ * unPBC positions (3 per bead in upload order; NULL = the current ones).
+ * Call it after the topology upload; an upload of beads or topology clears it.
+ * Single-box engines. */
+typedef struct dpd_monitor {
+    int64_t step;             /* m_SimTime of the state                             */
+    int64_t n;
+    double  inertia[9];       /* m_totalInertia / N, row-major (symmetric)          */
+    int64_t bonds;
+    double  mean_bond_length; /* over all bonds                                     */
+    double  mean_sq_bond_length;
+} dpd_monitor;
+DPD_API int dpd_engine_set_monitor(dpd_engine* e, int32_t nbondtypes, const int32_t* bond_type, int32_t nbptypes,
+                                   const int32_t* bondpair_type, int64_t npoly, const int64_t* poly_head_id,
+                                   const int64_t* poly_tail_id, const int32_t* poly_type, int32_t npolytypes,
+                                   const double* initial_unpbc3);
+/* Synchronous.  msd[ntypes], bond_length[nbondtypes], end_to_end[npolytypes],
+ * bondpair[6 * nbptypes] (P2, first length, second length, dphi, dphi^2,
+ * dphi ratio); any array may be NULL. */
+DPD_API int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bond_length,
+                               double* end_to_end, double* bondpair);
+
 /* Queues all further work on the caller's CUDA stream (a cudaStream_t passed
  * as a plain pointer; NULL returns to the engine's own stream).  The stream
  * must belong to the engine's device and outlive its use. */

@@ -21,6 +21,7 @@
 #include "pair_forces.cuh"
 #include "pair_staged.cuh"
 #include "slice_stress.cuh"
+#include "monitor.cuh"
 
 using namespace dpd;
 
@@ -104,6 +105,16 @@ struct dpd_engine {
     int* d_slice_bpt = nullptr;           // bond-pair type per bond pair
     size_t cap_slice_bt = 0, cap_slice_bpt = 0;
     bool slice_sampled = false;           // a sample step has filled the bins
+
+    // CMonitor sample data on request (dpd_engine_set_monitor / dpd_engine_monitor)
+    std::vector<int64_t> type_count;      // beads per type at the last upload
+    std::vector<double> h_ang_phi0;       // bond-pair phi0 of the uploaded topology
+    bool mon_set = false;
+    int mon_nbt = 0, mon_npt = 0, mon_nbpt = 0;
+    int64_t mon_np = 0;
+    std::vector<int64_t> mon_bcount, mon_pcount, mon_bpcount;
+    int *d_mon_bt = nullptr, *d_mon_bpt = nullptr, *d_mon_ph = nullptr, *d_mon_pt = nullptr, *d_mon_ptype = nullptr;
+    double *d_mon_phi0 = nullptr, *d_mon_u0 = nullptr, *d_mon_xu = nullptr, *d_mon_sums = nullptr;
     double4* d_Fb = nullptr;              // bonded force by upload index (FP64)
     double* d_Sb = nullptr;               // bond virial, 9 planes by upload index (sample steps)
     double* d_off = nullptr;
@@ -1014,6 +1025,9 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     int rc = empty_topology(e);
     if (rc) return rc;
     e->uploaded = true;
+    e->type_count.assign((size_t)e->ntypes, 0);
+    for (int64_t b = 0; b < n; ++b) e->type_count[(size_t)type[b]]++;
+    e->mon_set = false;   // the monitor's polymers and initial positions refer to the old beads
     e->stepped = false;
     e->sampled = false;
     e->obs_valid = false;
@@ -1167,9 +1181,11 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         CU(cudaMemcpy(e->d_ang_k3, k3, na * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_ang_cos0, acos0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(e->d_ang_sin0, asin0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
+        e->h_ang_phi0.assign(phi0, phi0 + na);
     }
     e->topo_nb = nb;
     e->topo_na = na;
+    e->mon_set = false;   // the monitor's bond types refer to the previous topology
     // the slice profile's bond types refer to the previous topology
     if (e->slice_S) { e->slice_S = 0; drop_graphs(e); }
     if (moved) drop_graphs(e);
@@ -1233,6 +1249,178 @@ int dpd_engine_slice_stress(dpd_engine* e, double* pair, double* bond, double* b
     if (bond) CU(cudaMemcpy(bond, sp.bond, S * e->slice_nbt * 9 * sizeof(double), cudaMemcpyDeviceToHost));
     if (bondpair)
         CU(cudaMemcpy(bondpair, sp.bondpair, S * e->slice_nbpt * 9 * sizeof(double), cudaMemcpyDeviceToHost));
+    return DPD_OK;
+}
+
+int dpd_engine_set_monitor(dpd_engine* e, int32_t nbondtypes, const int32_t* bond_type, int32_t nbptypes,
+                           const int32_t* bondpair_type, int64_t npoly, const int64_t* poly_head_id,
+                           const int64_t* poly_tail_id, const int32_t* poly_type, int32_t npolytypes,
+                           const double* initial_unpbc3)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads (and the topology) before the monitor");
+    if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "the monitor needs a single-box engine");
+    if (nbondtypes < 0 || nbptypes < 0 || npolytypes < 0 || npoly < 0 || nbondtypes > 65536 || nbptypes > 65536 ||
+        npolytypes > 65536 || (e->topo_nb && !bond_type) || (e->topo_na && !bondpair_type) ||
+        (npoly && (!poly_head_id || !poly_tail_id || !poly_type)))
+        return fail(e, DPD_E_ARG, "bad monitor arrays");
+    std::vector<int64_t> bc(nbondtypes, 0), bpc(nbptypes, 0), pc(npolytypes, 0);
+    for (int64_t i = 0; i < e->topo_nb; ++i) {
+        if (bond_type[i] < 0 || bond_type[i] >= nbondtypes) return fail(e, DPD_E_ARG, "bond type out of range");
+        bc[bond_type[i]]++;
+    }
+    for (int64_t i = 0; i < e->topo_na; ++i) {
+        if (bondpair_type[i] < 0 || bondpair_type[i] >= nbptypes) return fail(e, DPD_E_ARG, "bond-pair type out of range");
+        bpc[bondpair_type[i]]++;
+    }
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    const int64_t n = e->n;
+    // bead id -> upload index, as in the topology upload
+    std::vector<int> hpid(n);
+    CU(cudaMemcpy(hpid.data(), e->d_pid_of, n * sizeof(int), cudaMemcpyDeviceToHost));
+    std::unordered_map<int64_t, int> by_id;
+    by_id.reserve((size_t)n);
+    for (int64_t b = 0; b < n; ++b) by_id.emplace((int64_t)hpid[b], (int)b);
+    std::vector<int> ph(npoly), pt(npoly), pty(npoly);
+    for (int64_t k = 0; k < npoly; ++k) {
+        const auto ih = by_id.find(poly_head_id[k]), it = by_id.find(poly_tail_id[k]);
+        if (ih == by_id.end() || it == by_id.end()) return fail(e, DPD_E_ARG, "polymer refers to an unknown bead id");
+        if (poly_type[k] < 0 || poly_type[k] >= npolytypes) return fail(e, DPD_E_ARG, "polymer type out of range");
+        ph[k] = ih->second;
+        pt[k] = it->second;
+        pty[k] = poly_type[k];
+        pc[poly_type[k]]++;
+    }
+    int rc;
+    auto upload_ints = [&](int** d, const int* h, int64_t cnt) -> int {
+        dfree(e, *d);
+        *d = nullptr;
+        if ((rc = dalloc(e, d, (size_t)std::max<int64_t>(cnt, 1)))) return rc;
+        if (cnt) CU(cudaMemcpy(*d, h, sizeof(int) * cnt, cudaMemcpyHostToDevice));
+        return DPD_OK;
+    };
+    if ((rc = upload_ints(&e->d_mon_bt, bond_type, e->topo_nb))) return rc;
+    if ((rc = upload_ints(&e->d_mon_bpt, bondpair_type, e->topo_na))) return rc;
+    if ((rc = upload_ints(&e->d_mon_ph, ph.data(), npoly))) return rc;
+    if ((rc = upload_ints(&e->d_mon_pt, pt.data(), npoly))) return rc;
+    if ((rc = upload_ints(&e->d_mon_ptype, pty.data(), npoly))) return rc;
+    double** dd[] = {&e->d_mon_phi0, &e->d_mon_u0, &e->d_mon_xu, &e->d_mon_sums};
+    for (auto q : dd) { dfree(e, *q); *q = nullptr; }
+    if ((rc = dalloc(e, &e->d_mon_phi0, (size_t)std::max<int64_t>(e->topo_na, 1)))) return rc;
+    if (e->topo_na) CU(cudaMemcpy(e->d_mon_phi0, e->h_ang_phi0.data(), sizeof(double) * e->topo_na, cudaMemcpyHostToDevice));
+    if ((rc = dalloc(e, &e->d_mon_u0, 3 * (size_t)n))) return rc;
+    if ((rc = dalloc(e, &e->d_mon_xu, 6 * (size_t)n))) return rc;
+    const size_t nsums = 6 + (size_t)e->ntypes + nbondtypes + 2 + npolytypes + 5 * (size_t)nbptypes;
+    if ((rc = dalloc(e, &e->d_mon_sums, nsums))) return rc;
+    if (initial_unpbc3) {
+        CU(cudaMemcpy(e->d_mon_u0, initial_unpbc3, 3 * sizeof(double) * n, cudaMemcpyHostToDevice));
+    } else {   // the current unPBC positions, as k_download forms them
+        const int c = e->cur;
+        const int nbk = blocks_for(n, kThreads);
+        if (e->precision == DPD_PRECISION_FP64)
+            k_download<double><<<nbk, kThreads, 0, e->s()>>>((int)n, e->d_boxes, e->d_tf[c], e->d_bid[c], e->d_x[c],
+                                                             e->d_v[c], (const double*)e->d_F, e->d_img[c],
+                                                             e->off_active ? e->d_off : nullptr, nullptr, e->d_cell[c],
+                                                             nullptr, e->d_mon_u0, nullptr, nullptr, nullptr, nullptr);
+        else
+            k_download<float><<<nbk, kThreads, 0, e->s()>>>((int)n, e->d_boxes, e->d_tf[c], e->d_bid[c], e->d_x[c],
+                                                            e->d_v[c], (const float*)e->d_F, e->d_img[c],
+                                                            e->off_active ? e->d_off : nullptr, nullptr, e->d_cell[c],
+                                                            nullptr, e->d_mon_u0, nullptr, nullptr, nullptr, nullptr);
+        if ((rc = check_launch(e, "k_download"))) return rc;
+        CU(cudaStreamSynchronize(e->s()));
+    }
+    e->mon_nbt = nbondtypes;
+    e->mon_nbpt = nbptypes;
+    e->mon_npt = npolytypes;
+    e->mon_np = npoly;
+    e->mon_bcount = bc;
+    e->mon_bpcount = bpc;
+    e->mon_pcount = pc;
+    e->mon_set = true;
+    return DPD_OK;
+}
+
+int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bond_length, double* end_to_end,
+                       double* bondpair)
+{
+    if (!e) return DPD_E_ARG;
+    if (!out) return fail(e, DPD_E_ARG, "null output");
+    if (!e->mon_set) return fail(e, DPD_E_STATE, "dpd_engine_set_monitor has not been called for these beads");
+    CU(cudaSetDevice(e->device));
+    const int n = (int)e->n, T = e->ntypes;
+    const size_t nsums = 6 + (size_t)T + e->mon_nbt + 2 + e->mon_npt + 5 * (size_t)e->mon_nbpt;
+    CU(cudaMemsetAsync(e->d_mon_sums, 0, nsums * sizeof(double), e->s()));
+    const int c = e->cur;
+    k_monitor_beads<<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>(n, T, e->d_boxes, e->d_tf[c], e->d_bid[c],
+                                                                       e->d_x[c], e->d_img[c],
+                                                                       e->off_active ? e->d_off : nullptr,
+                                                                       e->d_mon_u0, e->d_mon_xu, e->d_mon_sums);
+    int rc;
+    if ((rc = check_launch(e, "k_monitor_beads"))) return rc;
+    MonitorTerms M{};
+    M.nb = (int)e->topo_nb;
+    M.np = (int)e->mon_np;
+    M.na = (int)e->topo_na;
+    M.bond_h = e->d_bond_h; M.bond_t = e->d_bond_t; M.bond_type = e->d_mon_bt;
+    M.poly_h = e->d_mon_ph; M.poly_t = e->d_mon_pt; M.poly_type = e->d_mon_ptype;
+    M.ang_b1h = e->d_ang[0]; M.ang_b1t = e->d_ang[1]; M.ang_b2h = e->d_ang[2]; M.ang_b2t = e->d_ang[3];
+    M.ang_type = e->d_mon_bpt; M.ang_phi0 = e->d_mon_phi0; M.ang_cos0 = e->d_ang_cos0; M.ang_sin0 = e->d_ang_sin0;
+    M.nbt = e->mon_nbt; M.npt = e->mon_npt; M.nbpt = e->mon_nbpt;
+    for (int d = 0; d < 3; ++d) M.L[d] = e->hboxes[0].L[d];
+    M.sums = e->d_mon_sums + 6 + T;
+    const int64_t terms = (int64_t)M.nb + M.np + M.na;
+    const size_t tsm = (M.nbt + 2 + M.npt + 5 * (size_t)M.nbpt) * sizeof(double);
+    if (terms > 0) {
+        if (tsm > 48 * 1024) return fail(e, DPD_E_LIMIT, "too many bond, polymer and bond-pair types for the monitor");
+        k_monitor_terms<<<blocks_for(terms, kThreads), kThreads, tsm, e->s()>>>(M, e->d_mon_xu, n);
+        if ((rc = check_launch(e, "k_monitor_terms"))) return rc;
+    }
+    std::vector<double> h(nsums);
+    CU(cudaMemcpyAsync(h.data(), e->d_mon_sums, nsums * sizeof(double), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    memset(out, 0, sizeof *out);
+    out->step = e->stepped ? e->last_step : 0;
+    out->n = e->n;
+    // m_totalInertia / N (Monitor.cpp:999-1007), symmetric completion
+    const double N = (double)e->n;
+    const int idx[6] = {0, 1, 2, 4, 5, 8};
+    for (int k = 0; k < 6; ++k) out->inertia[idx[k]] = h[k] / N;
+    out->inertia[3] = out->inertia[1];
+    out->inertia[6] = out->inertia[2];
+    out->inertia[7] = out->inertia[5];
+    // m_vBeadMSD / (6 dt t N_type) (Monitor.cpp:943-964); at step 0 only / N_type
+    const double pre = 6.0 * e->params.dt * (double)out->step;
+    for (int t = 0; t < T && msd; ++t) {
+        const double cnt = (double)e->type_count[t];
+        msd[t] = cnt > 0 ? h[6 + t] / ((pre > 0 ? pre : 1.0) * cnt) : 0.0;
+    }
+    const double* hb = h.data() + 6 + T;
+    int64_t nbt = 0;
+    for (int k = 0; k < e->mon_nbt; ++k) nbt += e->mon_bcount[k];
+    for (int k = 0; k < e->mon_nbt && bond_length; ++k)
+        bond_length[k] = e->mon_bcount[k] ? hb[k] / (double)e->mon_bcount[k] : 0.0;
+    out->bonds = nbt;
+    out->mean_bond_length = nbt ? hb[e->mon_nbt] / (double)nbt : 0.0;
+    out->mean_sq_bond_length = nbt ? hb[e->mon_nbt + 1] / (double)nbt : 0.0;
+    const double* hp = hb + e->mon_nbt + 2;
+    for (int k = 0; k < e->mon_npt && end_to_end; ++k)
+        end_to_end[k] = e->mon_pcount[k] ? hp[k] / (double)e->mon_pcount[k] : 0.0;
+    const double* ha = hp + e->mon_npt;
+    for (int k = 0; k < e->mon_nbpt && bondpair; ++k) {
+        const int64_t cnt = e->mon_bpcount[k];
+        double* o = bondpair + 6 * k;
+        for (int q = 0; q < 6; ++q) o[q] = 0.0;
+        if (!cnt) continue;
+        const double inv = 1.0 / (double)cnt;   // Monitor.cpp:1210-1222
+        o[0] = ha[5 * k] * inv;       // P2
+        o[1] = ha[5 * k + 1] * inv;   // first bond length
+        o[2] = ha[5 * k + 2] * inv;   // second bond length
+        o[3] = ha[5 * k + 3] * inv;   // phi - phi0
+        o[4] = ha[5 * k + 4] * inv;   // (phi - phi0)^2
+        o[5] = o[3] > 0.0 ? o[4] / (o[3] * o[3]) : 0.0;   // m_vBondPairPhiRatio
+    }
     return DPD_OK;
 }
 

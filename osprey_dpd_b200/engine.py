@@ -37,7 +37,7 @@ EXPORTED = [
     "dpd_engine_last_error", "dpd_engine_destroy", "dpd_engine_set_stream", "dpd_engine_profile",
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
-    "dpd_engine_set_slice_stress", "dpd_engine_slice_stress",
+    "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -56,6 +56,11 @@ class DpdBox(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("wx", C.c_double), ("wy", C.c_double), ("wz", C.c_double),
                 ("a", C.POINTER(C.c_double)), ("gamma", C.POINTER(C.c_double)), ("seed", C.c_uint64)]
+
+
+class DpdMonitor(C.Structure):
+    _fields_ = [("step", C.c_int64), ("n", C.c_int64), ("inertia", C.c_double * 9), ("bonds", C.c_int64),
+                ("mean_bond_length", C.c_double), ("mean_sq_bond_length", C.c_double)]
 
 
 class DpdObs(C.Structure):
@@ -107,6 +112,8 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
     L.dpd_engine_set_pair_scheme.argtypes = [vp, C.c_int32]
     L.dpd_engine_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
+    L.dpd_engine_set_monitor.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, C.c_int64, vp, vp, vp, C.c_int32, vp]
+    L.dpd_engine_monitor.argtypes = [vp, C.POINTER(DpdMonitor), vp, vp, vp, vp]
     L.dpd_engine_slice_stress.argtypes = [vp, vp, vp, vp]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
@@ -121,6 +128,22 @@ def load(path: Optional[str] = None) -> C.CDLL:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def polymer_table(system):
+    """(head id, tail id, polymer type) of every polymer of a workloads.DpdSystem:
+    ids are 1..N in polymer order, each polymer's beads consecutive."""
+    heads, tails, types = [], [], []
+    nxt = 1
+    for t, p in enumerate(system.polymers):
+        m = len(p.beads)
+        start = nxt + m * np.arange(p.count, dtype=np.int64)
+        heads.append(start)
+        tails.append(start + m - 1)
+        types.append(np.full(p.count, t, dtype=np.int32))
+        nxt += m * p.count
+    cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dt)
+    return cat(heads, np.int64), cat(tails, np.int64), cat(types, np.int32)
 
 
 class DpdEngine:
@@ -235,6 +258,31 @@ class DpdEngine:
         self._check(load().dpd_engine_set_slice_stress(self.h, int(nslices), int(nbondtypes), _p(self._sl_bt),
                                                        int(nbptypes), _p(self._sl_bpt)), "set_slice_stress")
         self._slice_dims = (int(nslices), int(self._a.shape[0]), int(nbondtypes), int(nbptypes))
+
+    def set_monitor_for(self, system, initial_unpbc=None) -> None:
+        """CMonitor sample data (dpd_engine_set_monitor) for a workloads.DpdSystem;
+        initial unPBC positions in upload order, default the current ones."""
+        ph, pt, pty = polymer_table(system)
+        self._mon = dict(bt=np.ascontiguousarray(system.bond_type if system.bond_type is not None else [], np.int32),
+                         at=np.ascontiguousarray(system.angle_type if system.angle_type is not None else [], np.int32),
+                         ph=ph, pt=pt, pty=pty,
+                         u0=None if initial_unpbc is None else np.ascontiguousarray(initial_unpbc, np.float64))
+        m = self._mon
+        self._mon_dims = (int(self._a.shape[0]), len(system.bond_specs), len(system.polymers),
+                          len(system.bondpair_specs))
+        self._check(load().dpd_engine_set_monitor(self.h, len(system.bond_specs), _p(m["bt"]),
+                                                  len(system.bondpair_specs), _p(m["at"]), len(ph), _p(ph), _p(pt),
+                                                  _p(pty), len(system.polymers), _p(m["u0"])), "set_monitor")
+
+    def monitor(self) -> dict:
+        """dpd_engine_monitor as a dict (see include/dpd_engine.h)."""
+        T, nbt, npt, nbpt = getattr(self, "_mon_dims", (int(self._a.shape[0]), 0, 0, 0))
+        o = DpdMonitor()
+        msd, bl, ee, bp = np.zeros(T), np.zeros(nbt), np.zeros(npt), np.zeros((nbpt, 6))
+        self._check(load().dpd_engine_monitor(self.h, C.byref(o), _p(msd), _p(bl), _p(ee), _p(bp)), "monitor")
+        return {"step": o.step, "n": o.n, "inertia": np.array(o.inertia[:]).reshape(3, 3), "bonds": o.bonds,
+                "mean_bond_length": o.mean_bond_length, "mean_sq_bond_length": o.mean_sq_bond_length,
+                "msd": msd, "bond_length": bl, "end_to_end": ee, "bondpair": bp}
 
     def set_slice_stress_for(self, system, nslices: int) -> None:
         """set_slice_stress with the bond and bond-pair types of a workloads.DpdSystem."""
