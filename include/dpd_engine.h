@@ -257,6 +257,21 @@ DPD_API int dpd_engine_set_monitor(dpd_engine* e, int32_t nbondtypes, const int3
 DPD_API int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bond_length,
                                double* end_to_end, double* bondpair);
 
+/* Restart state in the reference's text format (CRestartState::Serialize,
+ * RestartState.cpp:100-163), written from the device state without a round
+ * trip through bead objects.  The layout is registered once: order[k] is the
+ * upload index of the k-th bead of the file (the reference writes polymer by
+ * polymer, beads in polymer order), poly_id[k] / poly_type[k] its polymer's
+ * id and type, radius_by_type the bead radii.  An upload clears it.  The
+ * file holds the constraint flags, then per bead: polymer id, polymer type,
+ * bead id, bead type, radius, x[3], unPBC[3], v[3], F[3], with the stream's
+ * default 6-significant-digit formatting; coordinates within 0.001 of a box
+ * face are written as 0.001 and one outside the box is an error
+ * (CheckBeadWithinBox, RestartState.cpp:488-530).  Synchronous. */
+DPD_API int dpd_engine_set_restart_layout(dpd_engine* e, int64_t n, const int64_t* order, const int64_t* poly_id,
+                                          const int32_t* poly_type, const double* radius_by_type);
+DPD_API int dpd_engine_write_restart(dpd_engine* e, const char* path, int32_t wall, int32_t gravity, int32_t shear);
+
 /* Queues all further work on the caller's CUDA stream (a cudaStream_t passed
  * as a plain pointer; NULL returns to the engine's own stream).  The stream
  * must belong to the engine's device and outlive its use. */

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -108,6 +109,12 @@ struct dpd_engine {
 
     // CMonitor sample data on request (dpd_engine_set_monitor / dpd_engine_monitor)
     std::vector<int64_t> type_count;      // beads per type at the last upload
+    std::vector<int64_t> h_id;            // bead ids and types by upload index (restart files)
+    std::vector<int32_t> h_type;
+    // restart-file layout: file order of the beads (upload indices), their polymer id and type
+    std::vector<int64_t> rs_order, rs_poly_id;
+    std::vector<int32_t> rs_poly_type;
+    std::vector<double> rs_radius;        // per bead type
     std::vector<double> h_ang_phi0;       // bond-pair phi0 of the uploaded topology
     bool mon_set = false;
     int mon_nbt = 0, mon_npt = 0, mon_nbpt = 0;
@@ -1027,6 +1034,9 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     e->uploaded = true;
     e->type_count.assign((size_t)e->ntypes, 0);
     for (int64_t b = 0; b < n; ++b) e->type_count[(size_t)type[b]]++;
+    e->h_id.assign(id, id + n);
+    e->h_type.assign(type, type + n);
+    e->rs_order.clear();   // the restart layout refers to the old beads
     e->mon_set = false;   // the monitor's polymers and initial positions refer to the old beads
     e->stepped = false;
     e->sampled = false;
@@ -1421,6 +1431,87 @@ int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bon
         o[4] = ha[5 * k + 4] * inv;   // (phi - phi0)^2
         o[5] = o[3] > 0.0 ? o[4] / (o[3] * o[3]) : 0.0;   // m_vBondPairPhiRatio
     }
+    return DPD_OK;
+}
+
+static int run_download(dpd_engine* e, double* x3, double* u3, double* v3, double* f3, double* st9, int32_t* cell);
+
+int dpd_engine_set_restart_layout(dpd_engine* e, int64_t n, const int64_t* order, const int64_t* poly_id,
+                                  const int32_t* poly_type, const double* radius_by_type)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads before the restart layout");
+    if (n != e->n || !order || !poly_id || !poly_type || !radius_by_type)
+        return fail(e, DPD_E_ARG, "the restart layout needs every bead, its polymer id and type, and the radii");
+    std::vector<char> seen((size_t)n, 0);
+    for (int64_t k = 0; k < n; ++k) {
+        if (order[k] < 0 || order[k] >= n || seen[(size_t)order[k]])
+            return fail(e, DPD_E_ARG, "restart order is not a permutation of the upload indices");
+        seen[(size_t)order[k]] = 1;
+    }
+    e->rs_order.assign(order, order + n);
+    e->rs_poly_id.assign(poly_id, poly_id + n);
+    e->rs_poly_type.assign(poly_type, poly_type + n);
+    e->rs_radius.assign(radius_by_type, radius_by_type + e->ntypes);
+    return DPD_OK;
+}
+
+int dpd_engine_write_restart(dpd_engine* e, const char* path, int32_t wall, int32_t gravity, int32_t shear)
+{
+    if (!e) return DPD_E_ARG;
+    if (!path) return fail(e, DPD_E_ARG, "null path");
+    if (e->rs_order.empty() || (int64_t)e->rs_order.size() != e->n)
+        return fail(e, DPD_E_STATE, "dpd_engine_set_restart_layout has not been called for these beads");
+    if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "restart files are written for single-box engines");
+    const int64_t n = e->n;
+    std::vector<double> x(3 * n), u(3 * n), v(3 * n), f(3 * n);
+    int rc = run_download(e, x.data(), u.data(), v.data(), f.data(), nullptr, nullptr);
+    if (rc) return rc;
+    const double* L = e->hboxes[0].L;
+    // CRestartState::CheckBeadWithinBox (RestartState.cpp:488-530): a
+    // coordinate past the box length is an error, one within 0.001 of a face
+    // is written as 0.001
+    const double lim = 0.001;
+    for (int64_t b = 0; b < n; ++b)
+        for (int d = 0; d < 3; ++d) {
+            double& c = x[3 * b + d];
+            if (c > L[d]) return fail(e, DPD_E_BOX, "bead coordinate outside the box writing a restart state");
+            if (c > L[d] - lim || c < lim) c = lim;
+        }
+    // CRestartState::Serialize (RestartState.cpp:113-163): the constraint
+    // flags, then one line per bead in polymer order with the stream's default
+    // 6-significant-digit formatting; lines formatted in parallel chunks
+    const int nth = (int)std::max<unsigned>(1, std::min<unsigned>(16, std::thread::hardware_concurrency()));
+    std::vector<std::string> parts(nth);
+    auto work = [&](int t) {
+        const int64_t k0 = n * t / nth, k1 = n * (t + 1) / nth;
+        std::string& out = parts[t];
+        out.reserve((size_t)(k1 - k0) * 200);
+        char line[512];
+        for (int64_t k = k0; k < k1; ++k) {
+            const int64_t b = e->rs_order[k];
+            const double* X = &x[3 * b];
+            const double* U = &u[3 * b];
+            const double* V = &v[3 * b];
+            const double* F = &f[3 * b];
+            const int len = snprintf(line, sizeof line,
+                                     "%lld %d %lld %d %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g %.6g\n",
+                                     (long long)e->rs_poly_id[k], e->rs_poly_type[k], (long long)e->h_id[b],
+                                     e->h_type[b], e->rs_radius[e->h_type[b]], X[0], X[1], X[2], U[0], U[1], U[2],
+                                     V[0], V[1], V[2], F[0], F[1], F[2]);
+            out.append(line, (size_t)len);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return fail(e, DPD_E_ARG, std::string("cannot open ") + path);
+    bool ok = fprintf(fp, "%d %d %d\n", wall ? 1 : 0, gravity ? 1 : 0, shear ? 1 : 0) > 0;
+    for (auto& pstr : parts) ok = ok && fwrite(pstr.data(), 1, pstr.size(), fp) == pstr.size();
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) return fail(e, DPD_E_ARG, std::string("write failed: ") + path);
     return DPD_OK;
 }
 

@@ -38,6 +38,7 @@ EXPORTED = [
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
     "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
+    "dpd_engine_set_restart_layout", "dpd_engine_write_restart",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -114,6 +115,8 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
     L.dpd_engine_set_monitor.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, C.c_int64, vp, vp, vp, C.c_int32, vp]
     L.dpd_engine_monitor.argtypes = [vp, C.POINTER(DpdMonitor), vp, vp, vp, vp]
+    L.dpd_engine_set_restart_layout.argtypes = [vp, C.c_int64, vp, vp, vp, vp]
+    L.dpd_engine_write_restart.argtypes = [vp, C.c_char_p, C.c_int32, C.c_int32, C.c_int32]
     L.dpd_engine_slice_stress.argtypes = [vp, vp, vp, vp]
     L.dpd_engine_profile.argtypes = [vp, C.c_int32]
     L.dpd_engine_profile_read.argtypes = [vp, vp, vp]
@@ -128,6 +131,21 @@ def load(path: Optional[str] = None) -> C.CDLL:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def restart_layout(system):
+    """(order, polymer id, polymer type) per bead of a workloads.DpdSystem in
+    the reference's restart order: polymer by polymer, ids 1..N already in that
+    order, polymer ids from 1."""
+    pid, pty = [], []
+    k = 1
+    for t, p in enumerate(system.polymers):
+        m = len(p.beads)
+        pid.append(np.repeat(np.arange(k, k + p.count, dtype=np.int64), m))
+        pty.append(np.full(p.count * m, t, dtype=np.int32))
+        k += p.count
+    order = np.arange(system.n, dtype=np.int64)
+    return order, np.concatenate(pid), np.concatenate(pty)
 
 
 def polymer_table(system):
@@ -283,6 +301,18 @@ class DpdEngine:
         return {"step": o.step, "n": o.n, "inertia": np.array(o.inertia[:]).reshape(3, 3), "bonds": o.bonds,
                 "mean_bond_length": o.mean_bond_length, "mean_sq_bond_length": o.mean_sq_bond_length,
                 "msd": msd, "bond_length": bl, "end_to_end": ee, "bondpair": bp}
+
+    def set_restart_layout_for(self, system, radius: float = 0.5) -> None:
+        """dpd_engine_set_restart_layout for a workloads.DpdSystem (bead radius
+        0.5 for every type, as the workloads' input files declare)."""
+        order, pid, pty = restart_layout(system)
+        self._rs = (order, pid, pty, np.full(self._a.shape[0], float(radius)))
+        self._check(load().dpd_engine_set_restart_layout(self.h, len(order), *[_p(a) for a in self._rs]),
+                    "set_restart_layout")
+
+    def write_restart(self, path: str, wall: bool = False, gravity: bool = False, shear: bool = False) -> None:
+        self._check(load().dpd_engine_write_restart(self.h, os.fsencode(path), int(wall), int(gravity), int(shear)),
+                    "write_restart")
 
     def set_slice_stress_for(self, system, nslices: int) -> None:
         """set_slice_stress with the bond and bond-pair types of a workloads.DpdSystem."""
