@@ -23,6 +23,8 @@
 #include "pair_staged.cuh"
 #include "slice_stress.cuh"
 #include "monitor.cuh"
+#include "upload.cuh"
+#include <climits>
 
 using namespace dpd;
 
@@ -83,6 +85,15 @@ struct dpd_engine {
     uint32_t* d_imga = nullptr;
     int* d_cella = nullptr;
     bool ahead_valid = false;    // d_xa/d_imga/d_cella and the arrival counts hold the next drift
+    // upload staging: the caller's arrays as given, and per-bead scratch by upload index
+    double* d_up = nullptr;
+    size_t cap_up = 0;
+    int* d_up_cell = nullptr;
+    uint32_t* d_up_img = nullptr;
+    double* d_up_off = nullptr;
+    int* d_up_perm = nullptr;
+    int* d_up_err = nullptr;
+    size_t cap_up_cell = 0, cap_up_img = 0, cap_up_off = 0, cap_up_perm = 0, cap_up_err = 0;
     bool ahead_enabled = true;
     void* d_F = nullptr;        // current force, slot order (real)
     void* d_Fold = nullptr;     // previous force, slot order (real)
@@ -629,15 +640,20 @@ void release_topology(dpd_engine* e)
     e->cap_csr_ptr = e->cap_csr_term = e->cap_bond = e->cap_ang = 0;
 }
 
-// Empty topology: csr_ptr all zero.
-int empty_topology(dpd_engine* e)
+// Empty topology: csr_ptr all zero.  With keep_bonded (same bead count as
+// before) the bonded branch keeps its bead list and stays in the captured
+// graphs: with no terms it writes zero bonded forces, which k_update_mom
+// ignores for beads without kFlagBonded (all of them after a bead upload).
+int empty_topology(dpd_engine* e, bool keep_bonded)
 {
     bool moved = false;
     int rc;
     if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved))) return rc;
     CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
-    if (moved || e->nbb) drop_graphs(e);
-    e->nbb = 0;
+    if (moved || (e->nbb && !keep_bonded)) {
+        drop_graphs(e);
+        e->nbb = 0;
+    }
     e->topo_nb = e->topo_na = 0;
     return DPD_OK;
 }
@@ -885,63 +901,70 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     CU(cudaSetDevice(e->device));
     if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
     CU(cudaStreamSynchronize(e->s()));
-    // CSimBox::AssignBeadstoCells (SimBox.cpp:715-762): ix = (long)(x/w), box-local coordinates
-    std::vector<int> cell(n);
-    std::vector<double> off;
-    bool any_off = false;
-    std::vector<uint32_t> img(n);
-    for (int64_t b = 0; b < n; ++b) {
-        if (type[b] < 0 || type[b] >= e->ntypes) return fail(e, DPD_E_ARG, "bead type out of range");
-        if (id[b] < 1 || id[b] > 0x7fffffff) return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
-        const int bxi = box ? box[b] : 0;
-        if (bxi < 0 || bxi >= (int)e->hboxes.size()) return fail(e, DPD_E_ARG, "bead box index out of range");
-        const Box& B = e->hboxes[bxi];
-        const double* L = B.L;
-        const double* w = B.w;
-        const int* nc = B.nc;
-        int64_t ci[3];
-        for (int d = 0; d < 3; ++d) {
-            const double xv = x3[3 * b + d];
-            if (!std::isfinite(xv) || !std::isfinite(v3[3 * b + d])) return fail(e, DPD_E_BOX, "non-finite bead state");
-            ci[d] = (int64_t)(xv / w[d]);
-            if (xv < 0.0 || ci[d] < 0 || ci[d] >= nc[d]) {
+    cudaStream_t st = e->s();
+    // the caller's arrays, copied as they are (pinned buffers make these DMA
+    // copies); staging layout in doubles: x, unPBC, v, F (3n each), id (n
+    // int64), then int type[n], box[n] and the movable bytes
+    int rc;
+    bool smoved = false;
+    if ((rc = ensure(e, &e->d_up, e->cap_up, 15 * (size_t)n + 8, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_cell, e->cap_up_cell, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 1, &smoved))) return rc;
+    double* up = e->d_up;
+    int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
+    unsigned char* upm = reinterpret_cast<unsigned char*>(upi + 2 * (size_t)n);
+    const size_t v3b = 3 * sizeof(double) * (size_t)n;
+    UploadIn in{};
+    in.x = up;
+    CU(cudaMemcpyAsync(up, x3, v3b, cudaMemcpyHostToDevice, st));
+    if (unpbc3) { in.u = up + 3 * (size_t)n; CU(cudaMemcpyAsync(up + 3 * (size_t)n, unpbc3, v3b, cudaMemcpyHostToDevice, st)); }
+    in.v = up + 6 * (size_t)n;
+    CU(cudaMemcpyAsync(up + 6 * (size_t)n, v3, v3b, cudaMemcpyHostToDevice, st));
+    if (f3) { in.f = up + 9 * (size_t)n; CU(cudaMemcpyAsync(up + 9 * (size_t)n, f3, v3b, cudaMemcpyHostToDevice, st)); }
+    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)n);
+    CU(cudaMemcpyAsync(up + 12 * (size_t)n, id, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    in.type = upi;
+    CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    if (box) { in.box = upi + n; CU(cudaMemcpyAsync(upi + n, box, sizeof(int) * n, cudaMemcpyHostToDevice, st)); }
+    if (movable) { in.movable = upm; CU(cudaMemcpyAsync(upm, movable, (size_t)n, cudaMemcpyHostToDevice, st)); }
+    // validation and binning (CSimBox::AssignBeadstoCells, SimBox.cpp:715-762:
+    // ix = (long)(x/w), box-local coordinates); nothing of the state changes yet
+    int herr[kUpErrors + 1];
+    for (int k = 0; k < kUpErrors; ++k) herr[k] = INT_MAX;
+    herr[kUpErrors] = 0;   // any residual unPBC offset
+    CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
+    k_up_check<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, (int)e->hboxes.size(), e->ntypes, e->d_boxes, in,
+                                                            e->d_up_cell, e->d_up_img, e->d_up_off, e->d_count,
+                                                            e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors);
+    if ((rc = check_launch(e, "k_up_check"))) return rc;
+    CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    int bad = INT_MAX, kind = -1;
+    for (int k = 0; k < kUpErrors; ++k)
+        if (herr[k] < bad) { bad = herr[k]; kind = k; }
+    if (kind >= 0) {
+        CU(cudaMemset(e->d_count, 0, sizeof(int) * (size_t)e->ncell));
+        CU(cudaMemset(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk));
+        switch (kind) {
+            case kUpType: return fail(e, DPD_E_ARG, "bead type out of range");
+            case kUpId: return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
+            case kUpBox: return fail(e, DPD_E_ARG, "bead box index out of range");
+            case kUpNonFinite: return fail(e, DPD_E_BOX, "non-finite bead state");
+            case kUpOutside: {
                 char msg[160];
-                snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)b, (long long)id[b]);
+                snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)bad,
+                         (long long)id[bad]);
                 return fail(e, DPD_E_BOX, msg);
             }
-        }
-        cell[b] = (int)(B.cell_base + ci[0] + (int64_t)nc[0] * (ci[1] + (int64_t)nc[1] * ci[2]));
-        int ii[3] = {0, 0, 0};
-        if (unpbc3) {
-            for (int d = 0; d < 3; ++d) {
-                const double du = unpbc3[3 * b + d] - x3[3 * b + d];
-                const double k = std::nearbyint(du / L[d]);
-                if (!(std::fabs(k) <= 511.0)) return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
-                ii[d] = (int)k;
-                const double r = du - k * L[d];
-                if (r != 0.0) any_off = true;
-            }
-        }
-        img[b] = img_pack(ii[0], ii[1], ii[2]);
-    }
-    if (any_off) {
-        off.assign(3 * (size_t)n, 0.0);
-        for (int64_t b = 0; b < n; ++b) {
-            const double* L = e->hboxes[box ? box[b] : 0].L;
-            for (int d = 0; d < 3; ++d) {
-                const double du = unpbc3[3 * b + d] - x3[3 * b + d];
-                off[(size_t)d * n + b] = du - (double)img_get(img[b], d) * L[d];
-            }
+            default: return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
         }
     }
-    // slot order: by cell, then by upload index (stable counting sort)
-    std::vector<int64_t> start(e->ncell + 1, 0);
-    for (int64_t b = 0; b < n; ++b) start[cell[b] + 1]++;
-    for (int64_t c = 0; c < e->ncell; ++c) start[c + 1] += start[c];
-    std::vector<int64_t> fill(start.begin(), start.end() - 1);
-    std::vector<int> order(n);
-    for (int64_t b = 0; b < n; ++b) order[fill[cell[b]]++] = (int)b;
+    const bool any_off = herr[kUpErrors] != 0;
     // (re)allocate per-bead buffers; new addresses invalidate the captured graphs
+    const bool same_n = e->n == n;
     if (e->n != n) {
         drop_graphs(e);
         release_topology(e);
@@ -981,55 +1004,37 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
         if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
         e->n = n;
     }
+    // cell starts, then the slot order: by cell, inside a cell by upload index
+    k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start);
+    if ((rc = check_launch(e, "k_scan_cells"))) return rc;
+    CU(cudaMemsetAsync(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk, st));
+    k_up_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, e->d_up_cell, e->d_start, e->d_count,
+                                                              e->d_up_perm);
+    if ((rc = check_launch(e, "k_up_scatter"))) return rc;
+    const int c = e->cur;
+    if (e->precision == DPD_PRECISION_FP64)
+        k_up_place<double><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            (int)n, in, e->d_up_cell, e->d_up_img, e->d_start, e->d_up_perm, e->d_x[c], e->d_v[c], (double*)e->d_F,
+            e->d_bid[c], e->d_tf[c], e->d_cell[c], e->d_img[c], e->d_pid[c], e->d_pid_of);
+    else
+        k_up_place<float><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            (int)n, in, e->d_up_cell, e->d_up_img, e->d_start, e->d_up_perm, e->d_x[c], e->d_v[c], (float*)e->d_F,
+            e->d_bid[c], e->d_tf[c], e->d_cell[c], e->d_img[c], e->d_pid[c], e->d_pid_of);
+    if ((rc = check_launch(e, "k_up_place"))) return rc;
+    CU(cudaMemsetAsync(e->d_count, 0, sizeof(int) * (size_t)e->ncell, st));
     if (any_off) {
         bool moved = false;
-        int rc;
         if ((rc = ensure(e, &e->d_off, e->cap_off, 3 * (size_t)n, &moved))) return rc;
-        CU(cudaMemcpy(e->d_off, off.data(), off.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(e->d_off, e->d_up_off, 3 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
         if (moved || !e->off_active) drop_graphs(e);
     } else if (e->off_active) {
         drop_graphs(e);        // the kernels' offset pointer becomes null
     }
     e->off_active = any_off;
-    // host staging in slot order
-    std::vector<double> hx(3 * n), hv(3 * n), hf(3 * n);
-    std::vector<int> hbid(n), htf(n), hcell(n), hpid(n), hpids(n);
-    std::vector<uint32_t> himg(n);
-    for (int64_t s = 0; s < n; ++s) {
-        const int b = order[s];
-        for (int d = 0; d < 3; ++d) {
-            hx[(size_t)d * n + s] = x3[3 * b + d];
-            hv[(size_t)d * n + s] = v3[3 * b + d];
-            hf[(size_t)d * n + s] = f3 ? f3[3 * b + d] : 0.0;
-        }
-        hbid[s] = b;
-        htf[s] = type[b] | ((box ? box[b] : 0) << 8) | ((movable && !movable[b]) ? kFlagFrozen : 0);
-        hcell[s] = cell[b];
-        himg[s] = img[b];
-        hpids[s] = (int)id[b];
-    }
-    for (int64_t b = 0; b < n; ++b) hpid[b] = (int)id[b];
-    const int c = e->cur;
-    CU(cudaMemcpy(e->d_x[c], hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_v[c], hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice));
-    if (e->precision == DPD_PRECISION_FP64) {
-        CU(cudaMemcpy(e->d_F, hf.data(), hf.size() * sizeof(double), cudaMemcpyHostToDevice));
-    } else {
-        std::vector<float> ff(hf.begin(), hf.end());
-        CU(cudaMemcpy(e->d_F, ff.data(), ff.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
-    CU(cudaMemcpy(e->d_bid[c], hbid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_tf[c], htf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_cell[c], hcell.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_img[c], himg.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_pid[c], hpids.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(e->d_pid_of, hpid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    std::vector<int> st32(e->ncell + 1);
-    for (int64_t k = 0; k <= e->ncell; ++k) st32[k] = (int)start[k];
-    CU(cudaMemcpy(e->d_start, st32.data(), st32.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CU(cudaMemset(e->d_stress, 0, 9 * real_size(e) * (size_t)n));
-    CU(cudaMemset(e->d_status, 0, sizeof(unsigned)));
-    int rc = empty_topology(e);
+    CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)n, st));
+    CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
+    CU(cudaStreamSynchronize(st));
+    rc = empty_topology(e, same_n);
     if (rc) return rc;
     e->uploaded = true;
     e->type_count.assign((size_t)e->ntypes, 0);

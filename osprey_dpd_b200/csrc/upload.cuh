@@ -1,0 +1,122 @@
+// upload.cuh -- bead upload on the device (CSimBox::AssignBeadstoCells,
+// SimBox.cpp:715-762): the caller's arrays are copied once as they are
+// (bead order, xyz interleaved), then
+//   k_up_check   validates every bead, files it in its CNT cell
+//                (ix = (long)(x/w)), splits unPBC - x into periodic images
+//                and a residual offset, and counts the beads per cell;
+//   k_scan_cells (dpd_kernels.cuh) turns the counts into cell starts;
+//   k_up_scatter drops every bead into its cell's slot range;
+//   k_up_place   orders each cell's beads by upload index (the slot order the
+//                host counting sort used: by cell, then by upload index) and
+//                writes the structure-of-arrays state in slot order.
+// Nothing of the engine's state is written before k_up_check has passed.
+#pragma once
+#include "dpd_kernels.cuh"
+
+namespace dpd {
+
+// Error kinds of k_up_check, each recording the lowest failing bead index.
+enum UploadError { kUpType = 0, kUpId, kUpBox, kUpNonFinite, kUpOutside, kUpImage, kUpErrors };
+
+struct UploadIn {
+    const double* x;        // 3 per bead, bead order
+    const double* u;        // unPBC, or null
+    const double* v;
+    const double* f;        // or null
+    const int64_t* id;
+    const int* type;
+    const int* box;         // or null (single box)
+    const unsigned char* movable;   // or null
+};
+
+__global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes, const Box* __restrict__ boxes,
+                                                  UploadIn in, int* __restrict__ cell, uint32_t* __restrict__ img,
+                                                  double* __restrict__ off, int* __restrict__ count,
+                                                  int* __restrict__ block_count, int* __restrict__ err,
+                                                  int* __restrict__ any_off)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const int t = in.type[b];
+    if (t < 0 || t >= ntypes) { atomicMin(&err[kUpType], b); return; }
+    const int64_t idv = in.id[b];
+    if (idv < 1 || idv > 0x7fffffff) { atomicMin(&err[kUpId], b); return; }
+    const int bx = in.box ? in.box[b] : 0;
+    if (bx < 0 || bx >= nboxes) { atomicMin(&err[kUpBox], b); return; }
+    const Box& B = boxes[bx];
+    long long ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double xv = in.x[3 * b + d];
+        if (!isfinite(xv) || !isfinite(in.v[3 * b + d])) { atomicMin(&err[kUpNonFinite], b); return; }
+        ci[d] = (long long)(xv / B.w[d]);
+        if (xv < 0.0 || ci[d] < 0 || ci[d] >= B.nc[d]) { atomicMin(&err[kUpOutside], b); return; }
+    }
+    int ii[3] = {0, 0, 0};
+    bool residual = false;
+    double r[3] = {0.0, 0.0, 0.0};
+    if (in.u) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double du = in.u[3 * b + d] - in.x[3 * b + d];
+            const double k = nearbyint(du / B.L[d]);
+            if (!(fabs(k) <= 511.0)) { atomicMin(&err[kUpImage], b); return; }
+            ii[d] = (int)k;
+            r[d] = du - k * B.L[d];
+            residual |= r[d] != 0.0;
+        }
+    }
+    const int c = (int)(B.cell_base + ci[0] + (long long)B.nc[0] * (ci[1] + (long long)B.nc[1] * ci[2]));
+    cell[b] = c;
+    img[b] = img_pack(ii[0], ii[1], ii[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) off[(size_t)d * n + b] = r[d];
+    if (residual) *any_off = 1;
+    atomicAdd(&count[c], 1);
+    atomicAdd(&block_count[c / kScanChunk], 1);
+}
+
+// Any slot of the bead's cell range, taken with an atomic cursor (count, zero
+// on entry); k_up_place fixes the order inside the cell.
+__global__ void __launch_bounds__(256) k_up_scatter(int n, const int* __restrict__ cell,
+                                                    const int* __restrict__ start, int* __restrict__ cursor,
+                                                    int* __restrict__ perm)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const int c = cell[b];
+    perm[start[c] + atomicAdd(&cursor[c], 1)] = b;
+}
+
+template <typename real>
+__global__ void __launch_bounds__(256) k_up_place(int n, UploadIn in, const int* __restrict__ cell,
+                                                  const uint32_t* __restrict__ img, const int* __restrict__ start,
+                                                  const int* __restrict__ perm, double* __restrict__ x,
+                                                  double* __restrict__ v, real* __restrict__ F, int* __restrict__ bid,
+                                                  int* __restrict__ tf, int* __restrict__ ocell,
+                                                  uint32_t* __restrict__ oimg, int* __restrict__ pid,
+                                                  int* __restrict__ pid_of)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int b = perm[s];
+    const int c = cell[b];
+    const int beg = start[c], end = start[c + 1];
+    int k = 0;
+    for (int q = beg; q < end; ++q) k += perm[q] < b;
+    const int o = beg + k;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        x[(size_t)d * n + o] = in.x[3 * b + d];
+        v[(size_t)d * n + o] = in.v[3 * b + d];
+        F[(size_t)d * n + o] = in.f ? (real)in.f[3 * b + d] : real(0);
+    }
+    bid[o] = b;
+    tf[o] = in.type[b] | ((in.box ? in.box[b] : 0) << 8) | ((in.movable && !in.movable[b]) ? kFlagFrozen : 0);
+    ocell[o] = c;
+    oimg[o] = img[b];
+    pid[o] = (int)in.id[b];
+    pid_of[b] = (int)in.id[b];
+}
+
+}  // namespace dpd
