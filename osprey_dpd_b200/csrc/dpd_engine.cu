@@ -1079,15 +1079,14 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
     const int64_t n = e->n;
-    // bead id -> upload index
-    std::vector<int> hpid(n);
-    CU(cudaMemcpy(hpid.data(), e->d_pid_of, n * sizeof(int), cudaMemcpyDeviceToHost));
+    // bead id -> upload index (the ids kept from the bead upload)
+    const std::vector<int64_t>& hpid = e->h_id;
     bool identity = true;
     for (int64_t b = 0; b < n && identity; ++b) identity = (hpid[b] == b + 1);
     std::unordered_map<int64_t, int> by_id;
     if (!identity && (nb || na)) {
         by_id.reserve((size_t)n);
-        for (int64_t b = 0; b < n; ++b) by_id.emplace((int64_t)hpid[b], (int)b);
+        for (int64_t b = 0; b < n; ++b) by_id.emplace(hpid[b], (int)b);
     }
     auto index_of = [&](int64_t idv) -> int {
         if (identity) return (idv >= 1 && idv <= n) ? (int)(idv - 1) : -1;
@@ -1132,20 +1131,6 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         terms[fillp[a4[0][i]]++] = (int)(i * 8 + kAngle1);   // middle bead:       force [1]
         terms[fillp[a4[2][i]]++] = (int)(i * 8 + kAngle2);   // second bond's head: force [2]
     }
-    // mark the beads that have terms (kFlagBonded) so k_update_mom skips the
-    // topology lookup for all others, and k_gather writes their unPBC
-    // position into the FP64 buffer the bonded terms read
-    {
-        std::vector<int> tf(n), bid(n);
-        const int c = e->cur;
-        CU(cudaMemcpy(tf.data(), e->d_tf[c], n * sizeof(int), cudaMemcpyDeviceToHost));
-        CU(cudaMemcpy(bid.data(), e->d_bid[c], n * sizeof(int), cudaMemcpyDeviceToHost));
-        for (int64_t sl = 0; sl < n; ++sl) {
-            const int b = bid[sl];
-            tf[sl] = (tf[sl] & ~kFlagBonded) | (cnt[b + 1] > cnt[b] ? kFlagBonded : 0);
-        }
-        CU(cudaMemcpy(e->d_tf[c], tf.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    }
     bool moved = false;
     int rc;
     std::vector<int> bbl;
@@ -1164,6 +1149,13 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, terms.size(), &moved))) return rc;
     CU(cudaMemcpy(e->d_csr_ptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
     if (!terms.empty()) CU(cudaMemcpy(e->d_csr_term, terms.data(), terms.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // mark the beads that have terms (kFlagBonded) so k_update_mom skips the
+    // topology lookup for all others, and k_gather writes their unPBC
+    // position into the FP64 buffer the bonded terms read
+    k_mark_bonded<<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>((int)n, e->d_bid[e->cur], e->d_csr_ptr,
+                                                                    e->d_tf[e->cur]);
+    if ((rc = check_launch(e, "k_mark_bonded"))) return rc;
+    CU(cudaStreamSynchronize(e->s()));
     if (nb) {
         size_t c = e->cap_bond;
         if ((rc = ensure(e, &e->d_bond_h, c, nb, &moved))) return rc;

@@ -119,4 +119,15 @@ __global__ void __launch_bounds__(256) k_up_place(int n, UploadIn in, const int*
     pid_of[b] = (int)in.id[b];
 }
 
+// kFlagBonded for the beads with bond or bond-pair terms (csr_ptr by upload
+// index), in slot order.
+__global__ void __launch_bounds__(256) k_mark_bonded(int n, const int* __restrict__ bid,
+                                                     const int* __restrict__ csr_ptr, int* __restrict__ tf)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int b = bid[s];
+    tf[s] = (tf[s] & ~kFlagBonded) | (csr_ptr[b + 1] > csr_ptr[b] ? kFlagBonded : 0);
+}
+
 }  // namespace dpd
