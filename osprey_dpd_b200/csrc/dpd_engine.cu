@@ -95,6 +95,7 @@ struct dpd_engine {
     int* d_up_err = nullptr;
     size_t cap_up_cell = 0, cap_up_img = 0, cap_up_off = 0, cap_up_perm = 0, cap_up_err = 0;
     bool ahead_enabled = true;
+    bool pdl = true;             // programmatic dependent launch of the step kernels
     void* d_F = nullptr;        // current force, slot order (real)
     void* d_Fold = nullptr;     // previous force, slot order (real)
     void* d_stress = nullptr;   // per-bead virial of the last sample step (real, 9 planes)
@@ -440,6 +441,26 @@ int set_pair_attributes(dpd_engine* e)
     return DPD_OK;
 }
 
+// A step kernel launched with programmatic stream serialization (when the
+// engine allows it): it may be scheduled while its predecessor drains and
+// waits in pdl_wait() for that predecessor's results.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_step(const dpd_engine* e, void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                        cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = e->pdl ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Slice-profile parameters of the engine (S = 0 when off).
 SliceParams slice_params(const dpd_engine* e)
 {
@@ -487,31 +508,33 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
     if (first && !from_ahead) {
         {
             Timed t(e, DPD_KERNEL_UPDATE_POS);
-            k_update_pos<real><<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
-                                                        (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a],
-                                                        e->d_rank, e->d_count, e->d_block_count, e->d_status);
+            CU(launch_step(e, k_update_pos<real>, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
+                           (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
+                           e->d_block_count, e->d_status));
         }
         if ((rc = check_launch(e, "k_update_pos"))) return rc;
     }
     {
         Timed t(e, DPD_KERNEL_SCAN_CELLS);
-        k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, n, e->d_count, e->d_block_count,
-                                                          e->d_start);
+        CU(launch_step(e, k_scan_cells, e->nchunk, kScanThreads, 0, st, (int)e->ncell, n, e->d_count,
+                       e->d_block_count, e->d_start));
     }
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
     {
         Timed t(e, DPD_KERNEL_PERMUTE);
-        k_permute<<<blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st>>>(
-            n, e->nchunk, cell_in, e->d_rank, e->d_start, e->d_perm, e->d_block_count);
+        CU(launch_step(e, k_permute, blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st, n,
+                       e->nchunk, cell_in, e->d_rank, e->d_start, e->d_perm, e->d_block_count));
     }
     if ((rc = check_launch(e, "k_permute"))) return rc;
     {
         Timed t(e, DPD_KERNEL_GATHER);
-        k_gather<real><<<nb, kThreads, 0, st>>>(
-            n, e->d_K, e->d_boxes, e->d_perm, e->d_start, x_in, e->d_v[a], (const real*)e->d_F, e->d_bid[a],
-            e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b], (real*)e->d_Fold, e->d_bid[b],
-            e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b], (V4*)e->d_pos4, (V4*)e->d_vel4,
-            e->d_ubuf, e->off_active ? e->d_off : nullptr);
+        // the half-shell schemes accumulate into F with atomics: k_gather clears it
+        const int zero_F = e->pair_scheme != DPD_PAIR_FULL_SHELL ? 1 : 0;
+        CU(launch_step(e, k_gather<real>, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_perm, e->d_start, x_in,
+                       e->d_v[a], (real*)e->d_F, e->d_bid[a], e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b],
+                       (real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b],
+                       (V4*)e->d_pos4, (V4*)e->d_vel4, e->d_ubuf, (const double*)(e->off_active ? e->d_off : nullptr),
+                       zero_F));
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
     // bond and bond-pair forces: a branch beside the pair kernel (on the
@@ -544,7 +567,6 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         const size_t dyn = pair_dyn_bytes<real>(e, multi);
         if ((rc = set_pair_attributes<real>(e))) return rc;
         // the half shell accumulates into F with atomics
-        if (e->pair_scheme != DPD_PAIR_FULL_SHELL) CU(cudaMemsetAsync(e->d_F, 0, (size_t)3 * n * sizeof(real), st));
         // the half-shell kernels add each owner's pair virial in pieces
         if (sample && e->pair_scheme != DPD_PAIR_FULL_SHELL)
             CU(cudaMemsetAsync(e->d_stress, 0, (size_t)9 * n * sizeof(real), st));
@@ -553,20 +575,18 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         const int tiles = blocks_for(n, kPairBlock);
         const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
-        kern<<<blocks_for(tiles, tpb), kPairBlock, dyn, st>>>(n, e->d_K, e->d_boxes, e->d_step, (const real*)e->d_tab,
-                                                               e->d_cell[b], e->d_start, (const V4*)e->d_pos4,
-                                                               (const V4*)e->d_vel4, (real*)e->d_F,
-                                                               (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status);
+        CU(launch_step(e, kern, blocks_for(tiles, tpb), kPairBlock, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
+                       (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
+                       (real*)e->d_F, (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status));
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
     if (slices) {
         const size_t smem = (size_t)e->slice_S * e->ntypes * e->ntypes * 9 * sizeof(double);
         const int sb = smem <= kSliceSmemMax;
         Timed t(e, DPD_KERNEL_SLICES);
-        k_slice_pairs<real><<<e->sms * 2, 256, sb ? smem : 0, st>>>(n, e->d_K, e->d_boxes, e->d_step,
-                                                                     (const real*)e->d_tab, e->d_cell[b],
-                                                                     e->d_start, (const V4*)e->d_pos4,
-                                                                     (const V4*)e->d_vel4, e->d_x[b], sp, sb);
+        CU(launch_step(e, k_slice_pairs<real>, e->sms * 2, 256, sb ? smem : 0, st, n, e->d_K, e->d_boxes, e->d_step,
+                       (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
+                       (const double*)e->d_x[b], sp, sb));
         if ((rc = check_launch(e, "k_slice_pairs"))) return rc;
         e->slice_sampled = true;
     }
@@ -581,16 +601,17 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         double* xo = last ? e->d_xa : e->d_x[b];
         uint32_t* imgo = last ? e->d_imga : e->d_img[b];
         int* cello = last ? e->d_cella : e->d_cell[b];
-        kern<<<nb, kThreads, 0, st>>>(n, e->d_K, e->d_boxes, e->d_step, e->d_x[b], e->d_v[b], (real*)e->d_F,
-                                       (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_Fb, e->d_Sb,
-                                       (real*)e->d_stress, e->d_partials, e->d_img[b], e->d_cell[b], e->d_rank,
-                                       e->d_count, e->d_block_count, e->d_status, xo, imgo, cello);
+        CU(launch_step(e, kern, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_step, (const double*)e->d_x[b],
+                       e->d_v[b], (real*)e->d_F, (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b],
+                       (const double4*)e->d_Fb, (const double*)e->d_Sb, (real*)e->d_stress, e->d_partials,
+                       (const uint32_t*)e->d_img[b], (const int*)e->d_cell[b], e->d_rank, e->d_count,
+                       e->d_block_count, e->d_status, xo, imgo, cello));
     }
     if ((rc = check_launch(e, "k_update_mom"))) return rc;
     if (sample) {
         {
             Timed t(e, DPD_KERNEL_REDUCE_OBS);
-            k_reduce_obs<<<1, 32 * kObsTerms, 0, st>>>(nb, e->d_partials, e->d_obs);
+            CU(launch_step(e, k_reduce_obs, 1, 32 * kObsTerms, 0, st, nb, (const double*)e->d_partials, e->d_obs));
         }
         if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
     }
@@ -619,6 +640,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
             else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
             else if (key == "ahead") e->ahead_enabled = val != 0;
+            else if (key == "pdl") e->pdl = val != 0;
         }
         pos = end + 1;
     }

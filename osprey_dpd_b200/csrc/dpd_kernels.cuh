@@ -29,6 +29,16 @@
 
 namespace dpd {
 
+// Programmatic dependent launch (sm_90 and later): a kernel launched with the
+// programmatic-serialization attribute may be scheduled while the kernel
+// ahead of it in the stream is still running.  pdl_wait() blocks until that
+// kernel has completed and its writes are visible; pdl_launch() lets the next
+// kernel be scheduled once every block of this one has started.  Both are
+// no-ops for an ordinary launch.  Every step kernel calls both first thing,
+// before it reads any global memory.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 constexpr int kMaxTypes = 32;
 constexpr int kScanThreads = 256;
 constexpr int kScanPerThread = 4;
@@ -191,6 +201,8 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
     int* __restrict__ cell, int* __restrict__ rank, int* __restrict__ count,
     int* __restrict__ block_count, unsigned* __restrict__ status)
 {
+    pdl_wait();
+    pdl_launch();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = s < n;
     int cnew = 0;
@@ -222,6 +234,8 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     int ncell, int n, int* __restrict__ count, const int* __restrict__ block_count,
     int* __restrict__ start)
 {
+    pdl_wait();
+    pdl_launch();
     __shared__ int warp_sum[kScanThreads / 32];
     __shared__ int base_s;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, wid = t >> 5;
@@ -277,27 +291,33 @@ static __global__ void __launch_bounds__(256) k_permute(
     int n, int nchunk, const int* __restrict__ cell, const int* __restrict__ rank,
     const int* __restrict__ start, int* __restrict__ perm, int* __restrict__ block_count)
 {
+    pdl_wait();
+    pdl_launch();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < nchunk) block_count[s] = 0;
     if (s < n) perm[start[cell[s]] + rank[s]] = s;
 }
 
-// Stable order inside each cell (by previous slot), state permutation, and
-// the force kernel's shadows: position relative to the bead's own cell origin
+// Stable order inside each cell (by previous slot), state permutation, the
+// force kernel's shadows (position relative to the bead's own cell origin
 // and intermediate velocity v~ = v + lambda*dt*F_old (CNTCell.cpp:1743-1747),
-// with the bead type and the noise id in the fourth component.
+// with the bead type and the noise id in the fourth component) and, with
+// zero_F, the cleared force accumulator.
 template <typename real>
 __global__ void __launch_bounds__(256, 6) k_gather(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int* __restrict__ perm,
     const int* __restrict__ start,
-    const double* __restrict__ x_in, const double* __restrict__ v_in, const real* __restrict__ F_in,
+    const double* __restrict__ x_in, const double* __restrict__ v_in, real* __restrict__ F_in,
     const int* __restrict__ bid_in, const int* __restrict__ tf_in, const uint32_t* __restrict__ img_in,
     const int* __restrict__ cell_in, double* __restrict__ x_out, double* __restrict__ v_out,
     real* __restrict__ Fold_out, int* __restrict__ bid_out, int* __restrict__ tf_out,
     uint32_t* __restrict__ img_out, int* __restrict__ cell_out, const int* __restrict__ pid_in,
     int* __restrict__ pid_out, typename Vec4<real>::type* __restrict__ pos4,
-    typename Vec4<real>::type* __restrict__ vel4, double4* __restrict__ ubuf, const double* __restrict__ off)
+    typename Vec4<real>::type* __restrict__ vel4, double4* __restrict__ ubuf, const double* __restrict__ off,
+    int zero_F)
 {
+    pdl_wait();
+    pdl_launch();
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
     const int s = perm[d];
@@ -355,6 +375,12 @@ __global__ void __launch_bounds__(256, 6) k_gather(
 #pragma unroll
         for (int q = 0; q < 3; ++q) u[q] = xs[q] + (double)img_get(im, q) * B.L[q] + (off ? off[q * n + b] : 0.0);
         ubuf[b] = make_double4(u[0], u[1], u[2], xs[2]);   // w: wrapped z, for the slice stress profile
+    }
+    // the half-shell pair kernels add into F: each old slot was read above by
+    // exactly one thread, which clears it last (no separate memset)
+    if (zero_F) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) F_in[q * n + s] = real(0);
     }
 }
 
@@ -586,6 +612,8 @@ template <bool SAMPLE>
 __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __restrict__ bb, Topology topo,
                                                double4* __restrict__ Fb, double* __restrict__ Sb)
 {
+    pdl_wait();
+    pdl_launch();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < nbb) {
         const int b = bb[k];
@@ -722,6 +750,8 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
     int* __restrict__ rank, int* __restrict__ count, int* __restrict__ block_count, unsigned* __restrict__ status,
     double* xo, uint32_t* imgo, int* cello)
 {
+    pdl_wait();
+    pdl_launch();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = s < n;
     double acc[kObsTerms];
@@ -833,6 +863,8 @@ static __global__ void k_set_step(int64_t* __restrict__ step_ptr, int64_t value)
 static __global__ void __launch_bounds__(32 * kObsTerms) k_reduce_obs(int nblocks, const double* __restrict__ partials,
                                                                        double* __restrict__ out)
 {
+    pdl_wait();
+    pdl_launch();
     const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double* p = partials + (size_t)q * nblocks;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;

@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
     unsigned* __restrict__ status)
 {
+    pdl_wait();
+    pdl_launch();
     typedef typename Vec4<real>::type V4;
     extern __shared__ __align__(16) unsigned char pair_dyn[];
     const int nt = K->ntypes;
@@ -792,6 +794,8 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
     unsigned* __restrict__ status)
 {
+    pdl_wait();
+    pdl_launch();
     extern __shared__ __align__(16) unsigned char pair_dyn[];
     const int nt = K->ntypes;
     real* Tsh = reinterpret_cast<real*>(pair_dyn);

@@ -81,6 +81,8 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
     unsigned* __restrict__ status)
 {
+    pdl_wait();
+    pdl_launch();
     typedef typename Vec4<real>::type V4;
     extern __shared__ __align__(16) unsigned char pair_dyn[];
     __shared__ int key_s[kPairBlock];

@@ -35,6 +35,8 @@ __global__ void __launch_bounds__(256) k_slice_pairs(
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     const double* __restrict__ x, SliceParams sp, int sbins)
 {
+    pdl_wait();
+    pdl_launch();
     typedef typename Vec4<real>::type V4;
     extern __shared__ double sbin[];
     const int nt = K->ntypes, KT = nt * nt;
