@@ -32,6 +32,9 @@ template <typename real, bool MULTI = false> struct PairOcc {
     static constexpr int value = sizeof(real) == 8 ? 6 : 8;
 };
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
+// Cell pruning threshold on the squared distance to a cell's nearest point:
+// the cut-off (1) plus a margin far above the FP32 rounding of r2.
+constexpr float kPruneR2 = 1.0f + 1e-5f;
 
 template <typename real> struct RealOps;
 template <> struct RealOps<float> {
@@ -432,8 +435,9 @@ __device__ __forceinline__ void balanced_force_pass(
             const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
                              T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
             // the staged test decides pairs at the cut-off from rounded
-            // window coordinates: re-apply the exact cut-off here
-            const real m = (!STAGED || (r2 < real(1) && r2 > real(1e-18))) ? mag * inv : real(0);
+            // window coordinates: re-apply the exact cut-off here; the
+            // unstaged test leaves coincident beads (r2 <= 1e-18) to this pass
+            const real m = ((STAGED ? r2 < real(1) : true) && r2 > real(1e-18)) ? mag * inv : real(0);
             const real gx = m * dx, gy = m * dy, gz = m * dz;
             acc[0] += gx; acc[1] += gy; acc[2] += gz;
             atomicAdd(F + j, -gx);
@@ -637,7 +641,8 @@ __device__ __forceinline__ void half_shell_tile_lanes(
 }
 
 // Dynamic shared memory of k_pair_forces_half: pair tables (single box), hit
-// lists, then the balanced pass's per-thread scratch.
+// lists (hitcap rows plus the spare row of the branch-free test loop), then
+// the balanced pass's per-thread scratch.
 template <typename real>
 __host__ __device__ constexpr size_t half_scratch_bytes()
 {
@@ -646,7 +651,7 @@ __host__ __device__ constexpr size_t half_scratch_bytes()
 template <typename real>
 __host__ __device__ constexpr size_t half_smem_bytes(int nt, int hitcap, bool multi)
 {
-    return pair_smem_bytes<real>(nt, hitcap, multi) + half_scratch_bytes<real>();
+    return pair_smem_bytes<real>(nt, hitcap + 1, multi) + half_scratch_bytes<real>();
 }
 template <typename real>
 __device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
@@ -720,6 +725,19 @@ __device__ __forceinline__ void half_shell_tile(
         const int rb = B.cell_base + nx * (y2 + ny * z2);
         const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
         const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
+        const uint32_t code_m = rowbits, code_0 = rowbits | (1u << 26), code_p = rowbits | (2u << 26);
+        // Cell pruning: the nearest point of a row cell lies g_yz away in y-z
+        // (0 where the row spans the bead's own y or z) and, for the cells at
+        // x-1 and x+1, a further pi.x or wx - pi.x in x.  A cell whose nearest
+        // point is at or beyond the cut-off (with a margin far above the FP32
+        // rounding of r2) holds no partner and is cut from the window.
+        const real gy = dy > 0 ? wy - pi.y : (dy < 0 ? pi.y : real(0));
+        const real gz = dz > 0 ? wz - pi.z : real(0);
+        const real gyz = gy * gy + gz * gz;
+        const real gxp = wx - pi.x;
+        const bool keep_0 = gyz < kPruneR2;
+        const bool keep_m = pi.x * pi.x + gyz < kPruneR2;
+        const bool keep_p = gxp * gxp + gyz < kPruneR2;
         for (int seg = 0; seg < 2; ++seg) {
             int lo, hi, b1, b2;
             if (r > 0) {
@@ -735,7 +753,11 @@ __device__ __forceinline__ void half_shell_tile(
                 if (seg == 0) { lo = b1 = i + 1; b2 = hi = start[rb + cx + 1]; }
                 else { lo = b1 = b2 = start[rb]; hi = start[rb + 1]; }
             }
-            const int len = hi - lo;
+            // [lo, b1) is cell x-1, [b1, b2) cell x, [b2, hi) cell x+1
+            lo = keep_m ? lo : b1;
+            hi = keep_p ? hi : b2;
+            hi = keep_0 ? hi : lo;
+            const int len = max(hi - lo, 0);
             const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
             // chunks of at most hitcap candidates, so a list can never overflow
             for (int base = 0; base < trip; base += hitcap) {
@@ -747,29 +769,31 @@ __device__ __forceinline__ void half_shell_tile(
                     cnt = 0;
                 }
                 const int tend = base + min(trip - base, hitcap);
-                // Four candidates per iteration: their loads are issued
-                // together, so four L1/L2 round trips overlap.  The bead
-                // itself (r2 = 0) fails r2 > 1e-18, the reference's dr > 1e-9
-                // test (CNTCell.cpp:1202), so no separate j != i test.
-                // cnt + clen <= hitcap holds here, so the stores stay in range.
+                const int lim = min(len, tend);
+                // Four candidates per iteration, without branches: every lane
+                // runs all four (a lane past the end of its window loads a
+                // clamped slot and its result is masked), so their loads are
+                // issued together and four L1/L2 round trips overlap.  The
+                // entry is stored whether or not the candidate passes and kept
+                // by advancing cnt: cnt + clen <= hitcap holds here, so the
+                // store goes at most to the list's spare row (index hitcap).
+                // The own-cell window starts after i; coincident beads (the
+                // reference's dr > 1e-9 test, CNTCell.cpp:1202) are left to
+                // the force pass.
                 for (int t = base; t < tend; t += 4) {
+                    const int j0 = lo + t, rem = lim - t;
                     V4 p[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (t + q < len && t + q < tend) p[q] = pos4[lo + t + q];
+                    for (int q = 0; q < 4; ++q) p[q] = pos4[min(j0 + q, n - 1)];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const int jq = lo + t + q;
-                        if (t + q < len && t + q < tend) {
-                            const bool ge1 = jq >= b1, ge2 = jq >= b2;
-                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
-                            const real ddy = piy - p[q].y, ddz = piz - p[q].z;
-                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
-                                list[cnt * kPairBlock] = (uint32_t)jq | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
-                                ++cnt;
-                            }
-                        }
+                        const int jq = j0 + q;
+                        const bool ge1 = jq >= b1, ge2 = jq >= b2;
+                        const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
+                        const real ddy = piy - p[q].y, ddz = piz - p[q].z;
+                        const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                        list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                        cnt += (r2 < real(1) && q < rem) ? 1 : 0;
                     }
                 }
             }
@@ -801,7 +825,7 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     real* Tsh = reinterpret_cast<real*>(pair_dyn);
     unsigned char* lbase = pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt));
     uint32_t* lists = reinterpret_cast<uint32_t*>(lbase);
-    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)hitcap * kPairBlock);
+    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)(hitcap + 1) * kPairBlock);
     if (!MULTI)
         for (int k = threadIdx.x; k < 3 * nt * nt; k += kPairBlock) Tsh[k] = tab[k];
     const int64_t step = *step_ptr;

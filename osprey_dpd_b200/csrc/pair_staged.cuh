@@ -67,7 +67,7 @@ struct StgLayout {
         hpos = o; o += v4 * kPairBlock;
         hvel = o; o += v4 * kPairBlock;
         hxw = o; o += ((sizeof(real) * kPairBlock + 15) / 16) * 16;
-        lists = o; o += sizeof(uint32_t) * (size_t)hitcap * kPairBlock;
+        lists = o; o += sizeof(uint32_t) * (size_t)(hitcap + 1) * kPairBlock;   // + the spare row of half_shell_tile
         coff = o; o += sizeof(int) * kStgCells;
         total = o;
     }
