@@ -123,6 +123,25 @@ DPD_API int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id,
                             const uint8_t* movable, const double* x3, const double* unpbc3,
                             const double* v3, const double* f3);
 
+/* Builds the random initial state of CRandomBuilder::Assemble
+ * (RandomBuilder.cpp:71-361, no walls, 3-d) on the device and uploads it as
+ * dpd_engine_upload_beads would (unPBC = x, F = 0, all movable).  Replaces
+ * the builder's loop over the beads in CInitialState (InitialState.cpp:
+ * 451-520): id[i], type[i] are the i-th bead the reference creates; the
+ * reference's generator (CCNTCell::Randf) starts at rng_seed (the |RNGSeed|
+ * of the control file, CNTCell.cpp:134-137) and rng_skip draws are consumed
+ * first (0 for the reference's random state); bond_head/bond_tail are bead
+ * indices (0-based, into id) in the reference's polymer order, used for its
+ * bond shortening.  kT is the engine's.  Positions equal the reference's bit
+ * for bit; velocities agree to a few ulps (device acos/sin/cos, tree sums).
+ * x3_out / v3_out (3 per bead, bead order) receive the built state when not
+ * NULL.  Single-box engines only.  (Bond shortening moves a tail
+ * coordinate to a point between the head's and its own, so every bead stays
+ * in the box.) */
+DPD_API int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
+                                    uint64_t rng_seed, int64_t rng_skip, int64_t nb, const int64_t* bond_head,
+                                    const int64_t* bond_tail, double* x3_out, double* v3_out);
+
 /* Bonds (CBond: head id, tail id, k2, l0; Bond.h:45-52) and bond pairs
  * (CBondPair: indices of its first and second bond in this bond list, k3,
  * phi0 in radians; BondPair.h:23-30). */

@@ -734,3 +734,92 @@ int dpdo_get_cells(const dpdo_sim* s, int32_t* cell)
 
 int64_t dpdo_cell_errors(const dpdo_sim* s) { return s ? s->cell_errors : -1; }
 int64_t dpdo_pair_count(const dpdo_sim* s) { return s ? s->pairs : -1; }
+
+/* ---------------------------------------------------------------- random initial state
+ *
+ * CRandomBuilder::Assemble (RandomBuilder.cpp:71-361) for a box without
+ * walls, in three dimensions, restated operation by operation:
+ *   - the velocity-magnitude table CBuilder::MaxwellDist (Builder.cpp:104-126):
+ *     max(n, 10^7) entries from the recurrence vel = sqrt(2 log(M f/(M - f))),
+ *     f = exp(vel^2/2), the last entry repeating the one before;
+ *   - per bead i in bead order, six draws of the reference's LCG
+ *     (CCNTCell::Randf / lcg, CNTCell.cpp:2454-2466; state' = 6364136223846793005
+ *     state + 1, draw = (state' >> 32) / 2^32): table index, x, y, z (each
+ *     L * u, set to 0 when within 1e-4 of the upper face, RandomBuilder.cpp:
+ *     139-191), then theta = acos(1 - 2u), phi = 2 pi u, v = vmag (sin theta
+ *     cos phi, sin theta sin phi, cos theta) (RandomBuilder.cpp:201-208);
+ *   - bonds in polymer order: where a component of tail - head exceeds 1 in
+ *     magnitude the tail's coordinate becomes head + the unit vector's
+ *     component (RandomBuilder.cpp:241-311); the unPBC position equals x;
+ *   - centre-of-mass velocity removed and the velocities scaled to kT with
+ *     the 3N normalisation (RandomBuilder.cpp:315-361), sums in bead order.
+ * `skip` draws of the generator are consumed first (the reference's draws
+ * before the builder runs).  Returns 0, or -1 - i for bead i drawn outside
+ * the box (the reference's "coord outside box" error). */
+static double rb_draw(uint64_t* st)
+{
+    *st = 6364136223846793005ull * *st + 1ull;
+    return (double)(uint32_t)(*st >> 32) * (1.0 / 4294967296.0);
+}
+
+int dpdo_random_state(int64_t n, const double L[3], double kT, uint64_t seed, int64_t skip, int64_t nb,
+                      const int64_t* bond_head, const int64_t* bond_tail, double* x3, double* v3)
+{
+    const int64_t M = n > 10000000 ? n : 10000000;
+    double* tab = (double*)malloc(sizeof(double) * (size_t)M);
+    if (!tab) return -1000000000;
+    const double dM = (double)M;
+    double factor = 1.0;
+    for (int64_t j = 0; j < M - 1; ++j) {
+        const double vel = sqrt(2.0 * log(dM * factor / (dM - factor)));
+        factor = exp(0.5 * vel * vel);
+        tab[j] = vel;
+    }
+    tab[M - 1] = tab[M - 2];
+    uint64_t st = seed;
+    for (int64_t k = 0; k < skip; ++k) (void)rb_draw(&st);
+    const double twopi = 2.0 * 3.141592653589793238;   /* xxBase::m_globalTwoPI, xxBase.cpp:30-31 */
+    double vcm[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t index = (int64_t)((double)(size_t)M * rb_draw(&st));
+        const double vmag = tab[index];
+        double xp[3];
+        for (int d = 0; d < 3; ++d) {
+            xp[d] = 0.0 + L[d] * rb_draw(&st);
+            if (xp[d] > L[d]) { free(tab); return (int)(-1 - i); }
+            if (L[d] - xp[d] < 0.0001) xp[d] = 0.0;
+        }
+        const double vtheta = acos(1.0 - 2.0 * rb_draw(&st));
+        const double vphi = twopi * rb_draw(&st);
+        double* v = v3 + 3 * i;
+        v[0] = vmag * sin(vtheta) * cos(vphi);
+        v[1] = vmag * sin(vtheta) * sin(vphi);
+        v[2] = vmag * cos(vtheta);
+        vcm[0] += v[0];
+        vcm[1] += v[1];
+        vcm[2] += v[2];
+        for (int d = 0; d < 3; ++d) x3[3 * i + d] = xp[d];
+    }
+    free(tab);
+    for (int64_t k = 0; k < nb; ++k) {
+        double* h = x3 + 3 * bond_head[k];
+        double* t = x3 + 3 * bond_tail[k];
+        const double rd[3] = {t[0] - h[0], t[1] - h[1], t[2] - h[2]};
+        const double rmag = sqrt(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+        const double ru[3] = {rd[0] / rmag, rd[1] / rmag, rd[2] / rmag};
+        for (int d = 0; d < 3; ++d)
+            if (fabs(rd[d]) > 1.0) t[d] = h[d] + ru[d];
+    }
+    for (int d = 0; d < 3; ++d) vcm[d] /= (double)n;
+    double vtotal = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        double* v = v3 + 3 * i;
+        v[0] -= vcm[0];
+        v[1] -= vcm[1];
+        v[2] -= vcm[2];
+        vtotal = vtotal + v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    }
+    vtotal = sqrt(vtotal / (double)(3 * n));
+    for (int64_t i = 0; i < 3 * n; ++i) v3[i] = sqrt(kT) * v3[i] / vtotal;
+    return 0;
+}

@@ -102,6 +102,15 @@ int dpdo_set_dt(dpdo_sim* s, double dt);
 /* a_ij / gamma_ij update (CNTCell.cpp:434-456 sets both (i,j) and (j,i)). */
 int dpdo_set_pair(dpdo_sim* s, int32_t ti, int32_t tj, double a, double gamma);
 
+/* Random initial state of CRandomBuilder::Assemble (RandomBuilder.cpp:71-361,
+ * no walls, 3-d): positions x3 and velocities v3 (3 per bead, bead order) for
+ * n beads in a box of lengths L at temperature kT, from the reference's LCG
+ * seeded with `seed` after `skip` draws; bonds (bead indices, polymer order)
+ * shorten long bonds as the reference does.  The unPBC position equals x3.
+ * Returns 0, or -1 - i when bead i falls outside the box. */
+int dpdo_random_state(int64_t n, const double L[3], double kT, uint64_t seed, int64_t skip, int64_t nb,
+                      const int64_t* bond_head, const int64_t* bond_tail, double* x3, double* v3);
+
 #ifdef __cplusplus
 }
 #endif

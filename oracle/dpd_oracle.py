@@ -65,6 +65,8 @@ def lib() -> C.CDLL:
         L.dpdo_get_slice_stress.argtypes = [vp, vp, vp, vp]
         L.dpdo_slice_errors.argtypes = [vp]
         L.dpdo_slice_errors.restype = C.c_int64
+        L.dpdo_random_state.argtypes = [C.c_int64, vp, C.c_double, C.c_uint64, C.c_int64, C.c_int64, vp, vp,
+                                        vp, vp]
         _lib = L
     return _lib
 
@@ -169,18 +171,34 @@ class Oracle:
             self.h = None
 
 
+def random_state(n: int, L, kT: float, seed: int, skip: int = 0, bond_head=None, bond_tail=None):
+    """CRandomBuilder::Assemble restated (dpdo_random_state): (x, v), each
+    (n, 3) in bead order, for ``n`` beads in a box of lengths ``L``; bonds as
+    bead indices in the reference's polymer order."""
+    x = np.zeros((n, 3))
+    v = np.zeros((n, 3))
+    Lv = np.ascontiguousarray(L, dtype=np.float64)
+    bh = np.ascontiguousarray(bond_head if bond_head is not None else [], dtype=np.int64)
+    bt = np.ascontiguousarray(bond_tail if bond_tail is not None else [], dtype=np.int64)
+    rc = lib().dpdo_random_state(n, _p(Lv), kT, seed, skip, len(bh), _p(bh), _p(bt), _p(x), _p(v))
+    if rc != 0:
+        raise ValueError(f"bead {-1 - rc} drawn outside the box")
+    return x, v
+
+
 def philox_pair(seed: int, step: int, id_lo: int, id_hi: int) -> int:
     return int(lib().dpdo_philox_pair(seed, step, id_lo, id_hi))
 
 
 def run_reference(system, steps: int, workdir: str = None, kT: float = None, gamma_scale: float = 1.0,
                   inject: bool = True, dump: bool = True, topology: bool = False, timeout: float = None,
-                  rng_seed: int = None, slices: int = 0):
+                  rng_seed: int = None, slices: int = 0, initial: bool = False):
     """Runs the unmodified reference (oracle/_ref/osprey_ref_driver) on
     ``system`` for ``steps`` steps; ``rng_seed`` restarts its pair-noise LCG
     at that value just before the step loop; ``slices`` > 0 sets the analysis
     grid to that many z slices and also returns the last step's slice stress
-    profile.  Returns (json summary, dump dict or None, topology dict or None)
+    profile; ``initial`` adds the builder's state before any step as
+    summary["initial"].  Returns (json summary, dump dict or None, topology dict or None)
     or, with ``slices``, (summary, dump, topology, slice dict)."""
     from osprey_dpd_b200 import workloads  # local import: test-side helper
 
@@ -204,6 +222,8 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     if slices:
         dims = f"{int(slices)},{len(system.type_names)},{len(system.bond_specs)},{len(system.bondpair_specs)}"
         args += ["--slices", "slices.bin", "--slice-dims", dims]
+    if initial:
+        args += ["--dump-initial", "init.bin"]
     cp = subprocess.run(args, cwd=wd, capture_output=True, text=True, timeout=timeout)
     if cp.returncode != 0:
         raise RuntimeError(f"reference driver failed: {cp.stderr.strip()} {cp.stdout.strip()}")
@@ -212,6 +232,8 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     d = workloads.read_dump(os.path.join(wd, "out.bin")) if dump else None
     t = workloads.read_topology(os.path.join(wd, "topo.bin")) if topology else None
     sl = workloads.read_slices(os.path.join(wd, "slices.bin")) if slices else None
+    if initial:
+        summary["initial"] = workloads.read_dump(os.path.join(wd, "init.bin"))
     if own:
         import shutil
         shutil.rmtree(wd, ignore_errors=True)

@@ -22,7 +22,7 @@
 //
 // Usage (run inside the directory that holds dmpci.<runId>):
 //   osprey_ref_driver <runId> [--inject state.bin] [--topology topo.bin]
-//                             [--dump out.bin] [--rng-seed S]
+//                             [--dump out.bin] [--rng-seed S] [--dump-initial init.bin]
 // Prints one JSON line: {"beads":N,"steps":T,"run_seconds":s,...}
 //
 // Binary formats (little endian):
@@ -82,6 +82,30 @@ int fail(const char* msg) {
 
 }  // namespace
 
+// out.bin format (see the header comment), beads by id.
+static bool write_dump(const char* path, const std::vector<CBead*>& byId, long n, long steps)
+{
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return false;
+    fwrite("DPDDUMP1", 1, 8, fp);
+    long long nn = n, ss = steps;
+    fwrite(&nn, 8, 1, fp);
+    fwrite(&ss, 8, 1, fp);
+    for (long id = 1; id <= n; ++id) {
+        const CBead* b = byId[id];
+        long long it[2] = {b->GetId(), b->GetType()};
+        double d[21] = {b->GetXPos(), b->GetYPos(), b->GetZPos(),
+                        b->GetunPBCXPos(), b->GetunPBCYPos(), b->GetunPBCZPos(),
+                        b->GetXMom(), b->GetYMom(), b->GetZMom(),
+                        b->GetXForce(), b->GetYForce(), b->GetZForce()};
+        for (int k = 0; k < 9; ++k) d[12 + k] = b->m_Stress[k];
+        fwrite(it, 8, 2, fp);
+        fwrite(d, 8, 21, fp);
+    }
+    fclose(fp);
+    return true;
+}
+
 int main(int argc, char** argv)
 {
     if (argc < 2) return fail("usage: osprey_ref_driver <runId> [--inject f] [--topology f] [--dump f]");
@@ -92,6 +116,7 @@ int main(int argc, char** argv)
     const char* rngSeed = 0;
     const char* slicePath = 0;
     const char* sliceDims = 0;
+    const char* initialPath = 0;
     for (int a = 2; a + 1 < argc; a += 2) {
         if (!strcmp(argv[a], "--inject")) injectPath = argv[a + 1];
         else if (!strcmp(argv[a], "--topology")) topoPath = argv[a + 1];
@@ -99,6 +124,7 @@ int main(int argc, char** argv)
         else if (!strcmp(argv[a], "--rng-seed")) rngSeed = argv[a + 1];
         else if (!strcmp(argv[a], "--slices")) slicePath = argv[a + 1];
         else if (!strcmp(argv[a], "--slice-dims")) sliceDims = argv[a + 1];
+        else if (!strcmp(argv[a], "--dump-initial")) initialPath = argv[a + 1];
         else return fail("unknown option");
     }
 
@@ -118,6 +144,11 @@ int main(int argc, char** argv)
         if (id < 1 || id > n || byId[id]) return fail("unexpected bead id layout");
         byId[id] = beads[i];
     }
+
+    // The builder's output (CSimState::Assemble -> CInitialState -> e.g.
+    // CRandomBuilder::Assemble, RandomBuilder.cpp:71-361), before any
+    // injection or step: the dump format with steps = 0.
+    if (initialPath && !write_dump(initialPath, byId, n, 0)) return fail("cannot write initial dump");
 
     if (injectPath) {
         FILE* fp = fopen(injectPath, "rb");
@@ -176,26 +207,7 @@ int main(int argc, char** argv)
     pBox->Run();
     auto tRun1 = std::chrono::steady_clock::now();
 
-    if (dumpPath) {
-        FILE* fp = fopen(dumpPath, "wb");
-        if (!fp) return fail("cannot open dump file");
-        fwrite("DPDDUMP1", 1, 8, fp);
-        long long nn = n, ss = steps;
-        fwrite(&nn, 8, 1, fp);
-        fwrite(&ss, 8, 1, fp);
-        for (long id = 1; id <= n; ++id) {
-            const CBead* b = byId[id];
-            long long it[2] = {b->GetId(), b->GetType()};
-            double d[21] = {b->GetXPos(), b->GetYPos(), b->GetZPos(),
-                            b->GetunPBCXPos(), b->GetunPBCYPos(), b->GetunPBCZPos(),
-                            b->GetXMom(), b->GetYMom(), b->GetZMom(),
-                            b->GetXForce(), b->GetYForce(), b->GetZForce()};
-            for (int k = 0; k < 9; ++k) d[12 + k] = b->m_Stress[k];
-            fwrite(it, 8, 2, fp);
-            fwrite(d, 8, 21, fp);
-        }
-        fclose(fp);
-    }
+    if (dumpPath && !write_dump(dumpPath, byId, n, steps)) return fail("cannot open dump file");
 
     if (slicePath) {
         long long dims[4] = {0, 0, 0, 0};

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -24,6 +25,7 @@
 #include "slice_stress.cuh"
 #include "monitor.cuh"
 #include "upload.cuh"
+#include "builder.cuh"
 #include <climits>
 
 using namespace dpd;
@@ -913,6 +915,25 @@ int dpd_engine_profile_read(dpd_engine* e, double* total_ms, int64_t* launches)
 
 int64_t dpd_engine_launch_count(const dpd_engine* e) { return e ? e->launches : -1; }
 
+// Staging buffers of a bead upload; layout in doubles: x, unPBC, v, F (3n
+// each, xyz interleaved, bead order), id (n int64), then int type[n], box[n]
+// and the movable bytes.
+static int stage_buffers(dpd_engine* e, int64_t n)
+{
+    int rc;
+    bool smoved = false;
+    if ((rc = ensure(e, &e->d_up, e->cap_up, 15 * (size_t)n + 8, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_cell, e->cap_up_cell, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, (size_t)n, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 1, &smoved))) return rc;
+    return DPD_OK;
+}
+
+static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                         const UploadIn& in);
+
 static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
                        const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
                        const double* f3)
@@ -925,16 +946,9 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     CU(cudaStreamSynchronize(e->s()));
     cudaStream_t st = e->s();
     // the caller's arrays, copied as they are (pinned buffers make these DMA
-    // copies); staging layout in doubles: x, unPBC, v, F (3n each), id (n
-    // int64), then int type[n], box[n] and the movable bytes
+    // copies) into the staging buffers
     int rc;
-    bool smoved = false;
-    if ((rc = ensure(e, &e->d_up, e->cap_up, 15 * (size_t)n + 8, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_cell, e->cap_up_cell, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 1, &smoved))) return rc;
+    if ((rc = stage_buffers(e, n))) return rc;
     double* up = e->d_up;
     int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
     unsigned char* upm = reinterpret_cast<unsigned char*>(upi + 2 * (size_t)n);
@@ -952,6 +966,16 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
     CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
     if (box) { in.box = upi + n; CU(cudaMemcpyAsync(upi + n, box, sizeof(int) * n, cudaMemcpyHostToDevice, st)); }
     if (movable) { in.movable = upm; CU(cudaMemcpyAsync(upm, movable, (size_t)n, cudaMemcpyHostToDevice, st)); }
+    return upload_staged(e, n, box, id, type, in);
+}
+
+// Validation, binning and placement of a staged bead set (in: device arrays
+// in the staging buffers; id and type: the same beads on the host).
+static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                         const UploadIn& in)
+{
+    cudaStream_t st = e->s();
+    int rc;
     // validation and binning (CSimBox::AssignBeadstoCells, SimBox.cpp:715-762:
     // ix = (long)(x/w), box-local coordinates); nothing of the state changes yet
     int herr[kUpErrors + 1];
@@ -1085,6 +1109,140 @@ int dpd_batch_upload_beads(dpd_engine* e, int64_t n, const int32_t* box, const i
 {
     if (!box) return fail(e, DPD_E_ARG, "null box array");
     return upload_impl(e, n, box, id, type, movable, x3, unpbc3, v3, f3);
+}
+
+// CBuilder::MaxwellDist (Builder.cpp:104-126): max(n, 10^7) magnitudes from a
+// sequential recurrence through the C library's log and exp, computed on the
+// host the way the reference does (same operations, same order) and kept for
+// the process.
+static const std::vector<double>& maxwell_table(int64_t n)
+{
+    static std::mutex mu;
+    static std::vector<double> tab;
+    std::lock_guard<std::mutex> lock(mu);
+    const int64_t M = std::max<int64_t>(n, 10000000);
+    if ((int64_t)tab.size() != M) {
+        tab.assign((size_t)M, 0.0);
+        const double dM = (double)M;
+        double factor = 1.0;
+        for (int64_t j = 0; j < M - 1; ++j) {
+            const double vel = std::sqrt(2.0 * std::log(dM * factor / (dM - factor)));
+            factor = std::exp(0.5 * vel * vel);
+            tab[(size_t)j] = vel;
+        }
+        tab[(size_t)(M - 1)] = tab[(size_t)(M - 2)];
+    }
+    return tab;
+}
+
+int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type, uint64_t rng_seed,
+                            int64_t rng_skip, int64_t nb, const int64_t* bond_head, const int64_t* bond_tail,
+                            double* x3_out, double* v3_out)
+{
+    if (!e) return DPD_E_ARG;
+    if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || rng_skip < 0 || nb < 0 ||
+        (nb > 0 && (!bond_head || !bond_tail)))
+        return fail(e, DPD_E_ARG, "bad arguments");
+    if (e->hboxes.size() != 1) return fail(e, DPD_E_ARG, "the random builder fills a single box");
+    for (int64_t k = 0; k < nb; ++k)
+        if (bond_head[k] < 0 || bond_head[k] >= n || bond_tail[k] < 0 || bond_tail[k] >= n ||
+            bond_head[k] == bond_tail[k])
+            return fail(e, DPD_E_ARG, "bond bead index out of range");
+    // connected components of the bond graph (union-find on bead indices);
+    // each component's bonds keep their order
+    std::vector<int64_t> comp_ptr(1, 0), comp_bonds;
+    if (nb > 0) {
+        std::vector<int64_t> parent((size_t)n);
+        for (int64_t b = 0; b < n; ++b) parent[(size_t)b] = b;
+        auto find = [&](int64_t a) {
+            while (parent[(size_t)a] != a) {
+                parent[(size_t)a] = parent[(size_t)parent[(size_t)a]];
+                a = parent[(size_t)a];
+            }
+            return a;
+        };
+        for (int64_t k = 0; k < nb; ++k) {
+            const int64_t ra = find(bond_head[k]), rb = find(bond_tail[k]);
+            if (ra != rb) parent[(size_t)std::max(ra, rb)] = std::min(ra, rb);
+        }
+        std::vector<int64_t> root((size_t)nb), count;
+        std::unordered_map<int64_t, int64_t> slot;
+        for (int64_t k = 0; k < nb; ++k) {
+            const int64_t r = find(bond_head[k]);
+            auto it = slot.find(r);
+            if (it == slot.end()) { it = slot.emplace(r, (int64_t)count.size()).first; count.push_back(0); }
+            root[(size_t)k] = it->second;
+            count[(size_t)it->second]++;
+        }
+        comp_ptr.assign(count.size() + 1, 0);
+        for (size_t c = 0; c < count.size(); ++c) comp_ptr[c + 1] = comp_ptr[c] + count[c];
+        std::vector<int64_t> fill(comp_ptr.begin(), comp_ptr.end() - 1);
+        comp_bonds.resize((size_t)nb);
+        for (int64_t k = 0; k < nb; ++k) comp_bonds[(size_t)fill[(size_t)root[(size_t)k]]++] = k;
+    }
+    const int ncomp = (int)comp_ptr.size() - 1;
+    const std::vector<double>& tab = maxwell_table(n);
+    CU(cudaSetDevice(e->device));
+    if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
+    CU(cudaStreamSynchronize(e->s()));
+    cudaStream_t st = e->s();
+    int rc;
+    if ((rc = stage_buffers(e, n))) return rc;
+    double* up = e->d_up;
+    int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
+    const int nblk = blocks_for(n, kRbThreads);
+    // scratch of the build, released at the end: table, partial sums, bonds
+    double* d_tab = nullptr;
+    double* d_part = nullptr;
+    int64_t* d_bonds = nullptr;
+    auto release = [&]() { dfree(e, d_tab); dfree(e, d_part); dfree(e, d_bonds); };
+    const size_t nbw = nb > 0 ? 2 * (size_t)nb + (size_t)ncomp + 1 + (size_t)nb : 1;
+    if ((rc = dalloc(e, &d_tab, tab.size())) || (rc = dalloc(e, &d_part, 3 * (size_t)nblk + 8)) ||
+        (rc = dalloc(e, &d_bonds, nbw))) {
+        release();
+        return rc;
+    }
+    UploadIn in{};
+    in.x = up;
+    in.v = up + 6 * (size_t)n;
+    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)n);
+    in.type = upi;
+    auto run = [&]() -> int {
+        CU(cudaMemcpyAsync(up + 12 * (size_t)n, id, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st));
+        const Box& B = e->hboxes[0];
+        k_rb_beads<<<nblk, kRbThreads, 0, st>>>((int)n, rng_seed, (uint64_t)rng_skip, B.L[0], B.L[1], B.L[2], d_tab,
+                                                (int64_t)tab.size(), up, up + 6 * (size_t)n, d_part);
+        if (int r = check_launch(e, "k_rb_beads")) return r;
+        if (nb > 0) {
+            int64_t* dh = d_bonds;
+            int64_t* dt = dh + nb;
+            int64_t* dp = dt + nb;
+            int64_t* dc = dp + ncomp + 1;
+            CU(cudaMemcpyAsync(dh, bond_head, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dt, bond_tail, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dp, comp_ptr.data(), sizeof(int64_t) * (ncomp + 1), cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dc, comp_bonds.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
+            k_rb_bonds<<<blocks_for(ncomp, kRbThreads), kRbThreads, 0, st>>>(ncomp, dp, dc, dh, dt, up);
+            if (int r = check_launch(e, "k_rb_bonds")) return r;
+        }
+        double* stats = d_part + 3 * (size_t)nblk;   // vcm[3], vtotal
+        k_rb_vcm<<<1, 32, 0, st>>>(nblk, (int)n, d_part, stats);
+        k_rb_center<<<nblk, kRbThreads, 0, st>>>((int)n, stats, up + 6 * (size_t)n, d_part);
+        k_rb_vtotal<<<1, 32, 0, st>>>(nblk, (int)n, d_part, stats);
+        k_rb_scale<<<blocks_for(3 * n, kRbThreads), kRbThreads, 0, st>>>((int)n, std::sqrt(e->params.kT), stats,
+                                                                         up + 6 * (size_t)n);
+        if (int r = check_launch(e, "k_rb_scale")) return r;
+        if (x3_out) CU(cudaMemcpyAsync(x3_out, up, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        if (v3_out) CU(cudaMemcpyAsync(v3_out, up + 6 * (size_t)n, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        return DPD_OK;
+    };
+    rc = run();
+    release();
+    if (rc) return rc;
+    return upload_staged(e, n, nullptr, id, type, in);
 }
 
 int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_head_id, const int64_t* bond_tail_id,

@@ -795,9 +795,11 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
 #pragma unroll
             for (int d = 0; d < 3; ++d) f[d] = (real)((double)f[d] + bf[d]);
         }
-        F[s] = f[0];
-        F[n + s] = f[1];
-        F[2 * n + s] = f[2];
+        if (frozen || bonded) {   // otherwise F holds the pair force, the total already
+            F[s] = f[0];
+            F[n + s] = f[1];
+            F[2 * n + s] = f[2];
+        }
         if (!isfinite((double)f[0]) || !isfinite((double)f[1]) || !isfinite((double)f[2])) bad |= 0x2u;
         double vn[3];
 #pragma unroll

@@ -38,7 +38,7 @@ EXPORTED = [
     "dpd_engine_profile_read", "dpd_engine_set_sample_period", "dpd_batch_create", "dpd_batch_upload_beads",
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
     "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
-    "dpd_engine_set_restart_layout", "dpd_engine_write_restart",
+    "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -94,6 +94,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     vp = C.c_void_p
     L.dpd_engine_create.argtypes = [C.POINTER(DpdParams), C.POINTER(vp)]
     L.dpd_engine_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 7
+    L.dpd_engine_build_random.argtypes = [vp, C.c_int64, vp, vp, C.c_uint64, C.c_int64, C.c_int64, vp, vp, vp, vp]
     L.dpd_engine_upload_topology.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
     L.dpd_engine_set_pair_params.argtypes = [vp, C.c_int32, vp, vp]
     L.dpd_engine_set_dt.argtypes = [vp, C.c_double]
@@ -210,6 +211,23 @@ class DpdEngine:
                 np.ascontiguousarray(v, np.float64), None if f is None else np.ascontiguousarray(f, np.float64)]
         self._check(load().dpd_engine_upload_beads(self.h, n, *[_p(a) for a in arrs]), "upload_beads")
         self.n = n
+
+    def build_random(self, ids, types, seed: int, skip: int = 0, bond_head=None, bond_tail=None):
+        """The random initial state of CRandomBuilder::Assemble built on the
+        device and uploaded (dpd_engine_build_random); beads in the
+        reference's creation order, bonds as bead indices in its polymer
+        order.  Returns the built (x, v), each (n, 3), in that order."""
+        n = len(ids)
+        idv = np.ascontiguousarray(ids, np.int64)
+        tv = np.ascontiguousarray(types, np.int32)
+        bh = np.ascontiguousarray(bond_head if bond_head is not None else [], np.int64)
+        bt = np.ascontiguousarray(bond_tail if bond_tail is not None else [], np.int64)
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        self._check(load().dpd_engine_build_random(self.h, n, _p(idv), _p(tv), int(seed), int(skip), len(bh), _p(bh),
+                                                   _p(bt), _p(x), _p(v)), "build_random")
+        self.n = n
+        return x, v
 
     def upload_topology(self, head, tail, k2, l0, first, second, k3, phi0) -> None:
         t = [np.ascontiguousarray(head, np.int64), np.ascontiguousarray(tail, np.int64),

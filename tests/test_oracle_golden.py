@@ -24,8 +24,9 @@ def _cases():
 
 
 FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("stats_", "restart_")))
-# stats_*: tests/golden/make_stats.py; restart_*: tests/golden/make_restart_golden.py
+                  if not os.path.basename(p).startswith(("stats_", "restart_", "random_")))
+# stats_*: tests/golden/make_stats.py; restart_*: tests/golden/make_restart_golden.py;
+# random_*: tests/golden/make_random_golden.py
 
 
 @pytest.mark.parametrize("name", FIXTURES)
