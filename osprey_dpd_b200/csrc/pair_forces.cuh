@@ -714,6 +714,9 @@ __device__ __forceinline__ void half_shell_tile(
     const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
     const int tile_base = tile * kPairBlock;
     int cnt = 0;
+    // a row's second segment (the cell across the periodic x boundary) exists
+    // only for beads in the first or last cell column: warps with none skip it
+    const int nseg = __any_sync(0xffffffffu, live && (cx == 0 || cx == nx - 1)) ? 2 : 1;
     __syncwarp();   // home shadows visible to the warp
     for (int r = 0; r < 5; ++r) {
         const int dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
@@ -738,7 +741,7 @@ __device__ __forceinline__ void half_shell_tile(
         const bool keep_0 = gyz < kPruneR2;
         const bool keep_m = pi.x * pi.x + gyz < kPruneR2;
         const bool keep_p = gxp * gxp + gyz < kPruneR2;
-        for (int seg = 0; seg < 2; ++seg) {
+        for (int seg = 0; seg < nseg; ++seg) {
             int lo, hi, b1, b2;
             if (r > 0) {
                 row_segment(live, seg, rb, cx, nx, start, lo, hi, b1, b2);
