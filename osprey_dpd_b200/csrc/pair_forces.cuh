@@ -562,6 +562,9 @@ __device__ __forceinline__ void half_shell_tile_lanes(
 #pragma unroll
         for (int q = 0; q < NACC; ++q) acc[q] = real(0);
         int cnt = 0;
+        // the periodic-boundary segment of a row only for warps with a bead in
+        // the first or last cell column (as in half_shell_tile)
+        const int nseg = __any_sync(0xffffffffu, live && (cx == 0 || cx == nx - 1)) ? 2 : 1;
         for (int r = 0; r < 5; ++r) {
             const int dy = r == 0 ? 0 : (r == 1 ? 1 : r - 3);
             const int dz = r < 2 ? 0 : 1;
@@ -572,7 +575,16 @@ __device__ __forceinline__ void half_shell_tile_lanes(
             const int rb = B.cell_base + nx * (y2 + ny * z2);
             const real piy = pi.y - (real)dy * wy, piz = pi.z - (real)dz * wz;
             const uint32_t rowbits = ((uint32_t)(dy + 1) << 28) | ((uint32_t)(dz + 1) << 30);
-            for (int seg = 0; seg < 2; ++seg) {
+            const uint32_t code_m = rowbits, code_0 = rowbits | (1u << 26), code_p = rowbits | (2u << 26);
+            // cell pruning as in half_shell_tile
+            const real gy = dy > 0 ? wy - pi.y : (dy < 0 ? pi.y : real(0));
+            const real gz = dz > 0 ? wz - pi.z : real(0);
+            const real gyz = gy * gy + gz * gz;
+            const real gxp = wx - pi.x;
+            const bool keep_0 = gyz < kPruneR2;
+            const bool keep_m = pi.x * pi.x + gyz < kPruneR2;
+            const bool keep_p = gxp * gxp + gyz < kPruneR2;
+            for (int seg = 0; seg < nseg; ++seg) {
                 int lo, hi, b1, b2;
                 if (r > 0) {
                     row_segment(live, seg, rb, cx, nx, start, lo, hi, b1, b2);
@@ -587,7 +599,10 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                     if (seg == 0) { lo = b1 = i + 1; b2 = hi = start[rb + cx + 1]; }
                     else { lo = b1 = b2 = start[rb]; hi = start[rb + 1]; }
                 }
-                const int len = hi - lo;
+                lo = keep_m ? lo : b1;
+                hi = keep_p ? hi : b2;
+                hi = keep_0 ? hi : lo;
+                const int len = max(hi - lo, 0);
                 const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
                 for (int base = 0; base < trip; base += hitcap) {
                     const int clen = min(max(len - base, 0), hitcap);
@@ -597,32 +612,38 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                         cnt = 0;
                     }
                     const int tend = base + min(trip - base, hitcap);
-                    for (int t = base; t < tend; t += 2) {
-                        const int j0 = lo + t, j1 = j0 + 1;
-                        const bool h0 = t < len, h1 = t + 1 < len && t + 1 < tend;
-                        V4 p0, p1;
-                        if (h0) p0 = pos4[j0];
-                        if (h1) p1 = pos4[j1];
-                        if (h0) {
-                            const bool ge1 = j0 >= b1, ge2 = j0 >= b2;
-                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p0.x;
-                            const real ddy = piy - p0.y, ddz = piz - p0.z;
+                    const int lim = min(len, tend);
+                    // two candidates per iteration, then the last one singly,
+                    // without branches (clamped loads, masked results, the
+                    // entry stored at the list's count, which stays within the
+                    // spare row: cnt + clen <= hitcap)
+                    const int tend2 = base + ((tend - base) & ~1);
+                    int t = base;
+                    for (; t < tend2; t += 2) {
+                        const int j0 = lo + t, rem = lim - t;
+                        V4 p[2];
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) p[q] = pos4[min(j0 + q, n - 1)];
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            const int jq = j0 + q;
+                            const bool ge1 = jq >= b1, ge2 = jq >= b2;
+                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
+                            const real ddy = piy - p[q].y, ddz = piz - p[q].z;
                             const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
-                                list[cnt * kPairBlock] = (uint32_t)j0 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
-                                ++cnt;
-                            }
+                            list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                            cnt += (r2 < real(1) && r2 > real(1e-18) && q < rem) ? 1 : 0;
                         }
-                        if (h1) {
-                            const bool ge1 = j1 >= b1, ge2 = j1 >= b2;
-                            const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p1.x;
-                            const real ddy = piy - p1.y, ddz = piz - p1.z;
-                            const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            if ((r2 < real(1)) && (r2 > real(1e-18))) {
-                                list[cnt * kPairBlock] = (uint32_t)j1 | ((uint32_t)(ge1 + ge2) << 26) | rowbits;
-                                ++cnt;
-                            }
-                        }
+                    }
+                    if (t < tend) {
+                        const int jq = lo + t;
+                        const V4 pq = pos4[min(jq, n - 1)];
+                        const bool ge1 = jq >= b1, ge2 = jq >= b2;
+                        const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - pq.x;
+                        const real ddy = piy - pq.y, ddz = piz - pq.z;
+                        const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                        list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                        cnt += (r2 < real(1) && r2 > real(1e-18) && t < lim) ? 1 : 0;
                     }
                 }
             }
@@ -773,17 +794,20 @@ __device__ __forceinline__ void half_shell_tile(
                 }
                 const int tend = base + min(trip - base, hitcap);
                 const int lim = min(len, tend);
-                // Four candidates per iteration, without branches: every lane
-                // runs all four (a lane past the end of its window loads a
-                // clamped slot and its result is masked), so their loads are
-                // issued together and four L1/L2 round trips overlap.  The
-                // entry is stored whether or not the candidate passes and kept
+                // Four candidates per iteration (then the last 1-3 singly, so
+                // no group runs past the warp's longest window), without
+                // branches: every lane runs all four (a lane past the end of
+                // its window loads a clamped slot and its result is masked),
+                // so their loads are issued together and four L1/L2 round
+                // trips overlap.  The entry is stored whether or not the candidate passes and kept
                 // by advancing cnt: cnt + clen <= hitcap holds here, so the
                 // store goes at most to the list's spare row (index hitcap).
                 // The own-cell window starts after i; coincident beads (the
                 // reference's dr > 1e-9 test, CNTCell.cpp:1202) are left to
                 // the force pass.
-                for (int t = base; t < tend; t += 4) {
+                const int tend4 = base + ((tend - base) & ~3);
+                int t = base;
+                for (; t < tend4; t += 4) {
                     const int j0 = lo + t, rem = lim - t;
                     V4 p[4];
 #pragma unroll
@@ -798,6 +822,16 @@ __device__ __forceinline__ void half_shell_tile(
                         list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
                         cnt += (r2 < real(1) && q < rem) ? 1 : 0;
                     }
+                }
+                for (; t < tend; ++t) {   // the last 1-3 candidates of the warp's longest window
+                    const int jq = lo + t;
+                    const V4 pq = pos4[min(jq, n - 1)];
+                    const bool ge1 = jq >= b1, ge2 = jq >= b2;
+                    const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - pq.x;
+                    const real ddy = piy - pq.y, ddz = piz - pq.z;
+                    const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                    list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                    cnt += (r2 < real(1) && t < lim) ? 1 : 0;
                 }
             }
         }
