@@ -69,10 +69,8 @@ def workload(name: str, seed_offset: int = 0):
 
 
 def dist_info():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from osprey_dpd_b200 import ranks
+    return ranks.layout()
 
 
 def load_peaks():
@@ -488,40 +486,24 @@ def main():
         return run_reference_arm(args)
 
     import torch
+    from osprey_dpd_b200 import ranks as R
     ws, rank, local = dist_info()
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+    group = R.open_ranks("nccl", dev)
     from osprey_dpd_b200 import engine as E
 
     if args.workload == "replicas":
         line = run_replica_sweep(args, dev, torch, __import__("osprey_dpd_b200.engine", fromlist=["x"]))
         if rank == 0:
             print(json.dumps(line), flush=True)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        group.close()
         return 0
-    system, desc = workload(args.workload, seed_offset=rank)
+    system, desc = workload(args.workload, seed_offset=R.replica_seed_offset(rank))
     peaks, peak_kind = load_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        tt = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+    barrier = group.barrier
+    max_over_ranks = group.max
 
     results = {}
     clocks = None
@@ -545,7 +527,7 @@ def main():
         total_ms = max_over_ranks(sum(ms))
         results[prec_name] = {"ms": ms, "total_ms": total_ms, "prof": prof, "launches": launches,
                               "status": status, "shape": tuned["shape"] if tuned else None,
-                              "value": ws * system.n * args.steps / (total_ms / 1000.0)}
+                              "value": R.aggregate_rate(ws, system.n, args.steps, total_ms)}
 
     e2e_value = h2d_step = d2h_step = None
     e2e_times = []
@@ -553,7 +535,7 @@ def main():
         mshape = (results.get("mixed") or {}).get("shape")
         e2e_times, h2d_step, d2h_step = e2e_run(E, system, E.MIXED, args.e2e_reps, dev, torch, mshape)
         e2e_t = max_over_ranks(sum(e2e_times))
-        e2e_value = ws * system.n * E2E_PERIOD * len(e2e_times) / e2e_t
+        e2e_value = R.aggregate_rate(ws, system.n, E2E_PERIOD * len(e2e_times), 1000.0 * e2e_t)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -564,9 +546,7 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
 
     if rank != 0:
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        group.close()
         return 0
 
     mixed = results.get("mixed") or results["fp64"]
@@ -618,9 +598,7 @@ def main():
     if args.monitor:
         line["monitor"] = time_monitor(E, system, dev)
     print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    group.close()
     return 0
 
 
