@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "bead-steps/s, 393k-bead bilayer: FP32/FP64-mixed vs all-FP64, 1 B200"
+REPLICA_METRIC = "bead-steps/s, 512-replica A/B sweep: one batch vs replicas one at a time, 1 B200"
 UNIT = "bead-steps/s"
 SAMPLE_PERIOD = 100       # SamplePeriod of the reference's bilayer example (examples/dmpci.bilayer)
 E2E_PERIOD = SAMPLE_PERIOD
@@ -154,9 +155,48 @@ def cpu_reference_sample(system, steps: int, timeout: float = 600.0) -> dict:
             "run_seconds": dt}
 
 
+def reference_replica_aggregate(nrep: int, cores: int, seconds: float = 15.0) -> dict:
+    """The reference on the replica sweep with all host cores: the first
+    min(cores, nrep) replicas run at once, one reference process each, every
+    process for about `seconds` of its own step loop; the aggregate is the sum
+    of the processes' bead-steps/s (each measured while the others run)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from osprey_dpd_b200 import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import dpd_oracle
+    if not os.path.exists(dpd_oracle.REF_DRIVER):
+        raise FileNotFoundError(dpd_oracle.REF_DRIVER)
+    p = max(1, min(cores, nrep))
+    systems = [W.replica(r, nrep) for r in range(p)]
+    steps = [max(5, min(2000, int(seconds * 5e5 / s.n))) for s in systems]
+
+    def one(k):
+        summary, _, _ = dpd_oracle.run_reference(systems[k], steps[k], dump=False, timeout=20 * seconds + 300)
+        return summary["bead_steps_per_s"], summary["run_seconds"]
+
+    with ThreadPoolExecutor(max_workers=p) as pool:
+        res = list(pool.map(one, range(p)))
+    agg = sum(r[0] for r in res)
+    return {"value": agg, "unit": UNIT, "cores": p, "kind": "reference",
+            "sample": f"replicas 0..{p - 1} of {nrep} ({sum(s.n for s in systems)} beads), one reference process "
+                      f"each, {min(steps)}-{max(steps)} steps, run at once; sum of the processes' rates",
+            "run_seconds": max(r[1] for r in res)}
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_info()
     if rank != 0:
+        return 0
+    if args.workload == "replicas":
+        cb = reference_replica_aggregate(args.replicas, os.cpu_count() or 1)
+        line = {"impl": "reference", "metric": REPLICA_METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded replica table)",
+                "config": {"workload": f"{args.replicas} A/B replicas, edges 8..24 (all-cores sample)",
+                           "precision": "reference FP64"},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return 0
     system, desc = workload(args.workload)
     # bounded sample: about a minute of the serial reference at most
@@ -373,7 +413,7 @@ def run_replica_sweep(args, dev, torch, E):
         e.close()
     work = ntot * K * args.steps
     return {
-        "metric": "bead-steps/s, 512-replica A/B sweep: one batch vs replicas one at a time, 1 B200",
+        "metric": REPLICA_METRIC,
         "value": work / (batch_ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": args.steps * K,
         "warmup": args.warmup * K, "ms_per_step": batch_ms / (args.steps * K), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 state",
