@@ -1,0 +1,117 @@
+"""The z-slab decomposition (osprey_dpd_b200.slabs) on the CPU: two and three
+gloo ranks, each stepping its slab plus ghost layers with the oracle (Philox
+pair noise), exchange ghosts and migrants every step; the gathered box
+equals the single-box oracle run to rounding (the summation order inside a
+cell list differs).  A polymer solution, so bonds cross the slab faces."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+STEPS = 10
+
+
+def _system():
+    sys.path.insert(0, ROOT)
+    from osprey_dpd_b200 import workloads as W
+    return W.polymer_solution(cells=(6, 6, 12))
+
+
+def _oracle_engine(s):
+    import dpd_oracle as O
+    return O.Oracle(s, noise=O.NOISE_PHILOX)
+
+
+def _single_box():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    s = _system()
+    o = _oracle_engine(s)
+    o.step(1, STEPS)
+    st = o.state()
+    order = np.argsort(s.ids)
+    return {k: st[k][order] for k in ("x", "unpbc", "v", "f")}, s.ids[order]
+
+
+def _free_port() -> int:
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        from osprey_dpd_b200 import ranks as R, slabs
+        g = R.open_ranks("gloo", "cpu", timeout_s=120)
+        dec = slabs.SlabDecomposition(_system(), g, ghost=2)
+        counts = []
+        for t in range(1, STEPS + 1):
+            dec.step(t, _oracle_engine, lambda e: e.state())
+            counts.append(len(dec.owned))
+        out = dec.gather()
+        g.close()
+        q.put((rank, out, counts))
+    except Exception as exc:
+        import traceback
+        q.put((rank, "error", traceback.format_exc()))
+
+
+def _run(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(world):
+        item = q.get(timeout=600)
+        res[item[0]] = item
+    for p in procs:
+        p.join(timeout=60)
+    for r in range(world):
+        assert res[r][1] != "error", res[r][2]
+    return res
+
+
+def _compare(got, ref, ids):
+    assert np.array_equal(got["id"], ids)
+    np.testing.assert_allclose(got["x"], ref["x"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(got["unpbc"], ref["unpbc"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(got["v"], ref["v"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(got["f"], ref["f"], rtol=0, atol=1e-7)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slabs_equal_single_box(world):
+    ref, ids = _single_box()
+    res = _run(world)
+    _compare(res[0][1], ref, ids)
+    assert sum(res[r][2][-1] for r in range(world)) == len(ids)   # every bead owned once
+
+
+def test_single_rank_is_the_box(monkeypatch):
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from osprey_dpd_b200 import ranks as R, slabs
+    ref, ids = _single_box()
+    dec = slabs.SlabDecomposition(_system(), R.open_ranks("gloo", "cpu"), ghost=2)
+    for t in range(1, STEPS + 1):
+        dec.step(t, _oracle_engine, lambda e: e.state())
+    _compare(dec.gather(), ref, ids)
+
+
+def test_slab_bounds_and_limits():
+    sys.path.insert(0, ROOT)
+    from osprey_dpd_b200 import slabs
+    assert [slabs.slab_bounds(10, 3, r) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
+    assert slabs.slab_bounds(12, 1, 0) == (0, 12)
