@@ -2,7 +2,9 @@
 gloo ranks, each stepping its slab plus ghost layers with the oracle (Philox
 pair noise), exchange ghosts and migrants every step; the gathered box
 equals the single-box oracle run to rounding (the summation order inside a
-cell list differs).  A polymer solution, so bonds cross the slab faces."""
+cell list differs).  A polymer solution (bonds across the slab faces and the
+global z face) and a bilayer centred on a slab face (bonds and angles across
+it)."""
 import os
 import socket
 import sys
@@ -14,9 +16,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STEPS = 10
 
 
-def _system():
+def _system(kind="polymer"):
     sys.path.insert(0, ROOT)
     from osprey_dpd_b200 import workloads as W
+    if kind == "bilayer":
+        return W.bilayer(cells=(6, 6, 12), nlipids=40)
     return W.polymer_solution(cells=(6, 6, 12))
 
 
@@ -25,9 +29,9 @@ def _oracle_engine(s):
     return O.Oracle(s, noise=O.NOISE_PHILOX)
 
 
-def _single_box():
+def _single_box(kind="polymer"):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    s = _system()
+    s = _system(kind)
     o = _oracle_engine(s)
     o.step(1, STEPS)
     st = o.state()
@@ -41,7 +45,7 @@ def _free_port() -> int:
         return sk.getsockname()[1]
 
 
-def _worker(rank, world, port, q):
+def _worker(rank, world, port, q, kind="polymer"):
     os.environ.update(WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
                       MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
@@ -49,7 +53,7 @@ def _worker(rank, world, port, q):
     try:
         from osprey_dpd_b200 import ranks as R, slabs
         g = R.open_ranks("gloo", "cpu", timeout_s=120)
-        dec = slabs.SlabDecomposition(_system(), g, ghost=2)
+        dec = slabs.SlabDecomposition(_system(kind), g, ghost=2)
         counts = []
         for t in range(1, STEPS + 1):
             dec.step(t, _oracle_engine, lambda e: e.state())
@@ -62,12 +66,12 @@ def _worker(rank, world, port, q):
         q.put((rank, "error", traceback.format_exc()))
 
 
-def _run(world):
+def _run(world, kind="polymer"):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, kind)) for r in range(world)]
     for p in procs:
         p.start()
     res = {}
@@ -89,10 +93,10 @@ def _compare(got, ref, ids):
     np.testing.assert_allclose(got["f"], ref["f"], rtol=0, atol=1e-7)
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_slabs_equal_single_box(world):
-    ref, ids = _single_box()
-    res = _run(world)
+@pytest.mark.parametrize("world,kind", [(2, "polymer"), (3, "polymer"), (2, "bilayer")])
+def test_slabs_equal_single_box(world, kind):
+    ref, ids = _single_box(kind)
+    res = _run(world, kind)
     _compare(res[0][1], ref, ids)
     assert sum(res[r][2][-1] for r in range(world)) == len(ids)   # every bead owned once
 
