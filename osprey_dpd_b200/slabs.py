@@ -158,9 +158,7 @@ class SlabDecomposition:
         u = rec[:, 6:9].copy()
         x[:, 2] += shift
         u[:, 2] += self._u_shift()
-        present = set(ids.tolist())
-        keep_b = np.array([h in present and t in present for h, t in zip(self.bond_head, self.bond_tail)],
-                          dtype=bool)
+        keep_b = np.isin(self.bond_head, ids) & np.isin(self.bond_tail, ids)
         bmap = -np.ones(len(keep_b), np.int64)
         bmap[keep_b] = np.arange(int(keep_b.sum()))
         keep_a = keep_b[self.angle_first] & keep_b[self.angle_second] if len(self.angle_first) else np.zeros(0, bool)
