@@ -633,6 +633,12 @@ def main():
         "clocks": clocks,
         "status_bits": {k: v["status"] for k, v in results.items()},
     }
+    # the same fraction against the SM clock seen during the timed region,
+    # when it sat below the maximum
+    sm_seen = (clocks or {}).get("sm_mhz")
+    if sm_seen:
+        line["roofline"]["frac_at_observed_clock"] = achieved / (sms * 128 * float(sm_seen) * 1e6)
+        line["roofline"]["observed_sm_mhz"] = float(sm_seen)
     if args.slices > 0:
         line["slice_profile"] = time_slice_profile(E, system, args.slices, mixed["shape"], dev, torch)
     if args.monitor:
