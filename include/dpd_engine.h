@@ -137,7 +137,9 @@ DPD_API int dpd_engine_upload_beads(dpd_engine* e, int64_t n, const int64_t* id,
  * x3_out / v3_out (3 per bead, bead order) receive the built state when not
  * NULL.  Single-box engines only.  (Bond shortening moves a tail
  * coordinate to a point between the head's and its own, so every bead stays
- * in the box.) */
+ * in the box.)  The first call computes the reference's velocity-magnitude
+ * table (CBuilder::MaxwellDist, max(n, 10^7) entries) on the host, about
+ * half a second, and keeps it (8 bytes per entry) for the process. */
 DPD_API int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
                                     uint64_t rng_seed, int64_t rng_skip, int64_t nb, const int64_t* bond_head,
                                     const int64_t* bond_tail, double* x3_out, double* v3_out);
