@@ -293,6 +293,27 @@ DPD_API int dpd_engine_set_restart_layout(dpd_engine* e, int64_t n, const int64_
                                           const int32_t* poly_type, const double* radius_by_type);
 DPD_API int dpd_engine_write_restart(dpd_engine* e, const char* path, int32_t wall, int32_t gravity, int32_t shear);
 
+/* Writes a Paraview snapshot of n beads given in file order, from host
+ * arrays (no device work): the file CCurrentState::Serialize writes with
+ * CParaviewFormat (CurrentState.cpp:163-244, ParaviewFormat.cpp:72-112) --
+ * header, one "x y z" line per bead at 6 significant digits, the vertex
+ * list, one display id per bead.  Returns DPD_E_ARG when the file cannot be
+ * written. */
+DPD_API int dpd_write_paraview(const char* path, int64_t n, const double* x3, const int32_t* display_id);
+
+/* The engine's current state as that Paraview snapshot, replacing
+ * CCurrentState::Serialize for the Paraview format (from one position
+ * download, no bead objects).  Beads are written by CNT cell in index order,
+ * as CSimBox::GetAllBeadsInCNTCells lists them (SimBox.cpp:5883-5895); inside
+ * a cell the reference follows its cell-list history and the engine the
+ * upload order, so the files agree cell by cell.  type_visible (one byte per
+ * bead type, NULL = all visible) leaves out invisible types as
+ * CCurrentState does; display_id (per bead in upload order, NULL = the bead
+ * type, the reference's default display map, Monitor.cpp:277) sets the
+ * ptype column.  Single-box engines. */
+DPD_API int dpd_engine_write_paraview(dpd_engine* e, const char* path, const uint8_t* type_visible,
+                                      const int32_t* display_id);
+
 /* Queues all further work on the caller's CUDA stream (a cudaStream_t passed
  * as a plain pointer; NULL returns to the engine's own stream).  The stream
  * must belong to the engine's device and outlive its use. */

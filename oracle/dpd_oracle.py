@@ -192,13 +192,14 @@ def philox_pair(seed: int, step: int, id_lo: int, id_hi: int) -> int:
 
 def run_reference(system, steps: int, workdir: str = None, kT: float = None, gamma_scale: float = 1.0,
                   inject: bool = True, dump: bool = True, topology: bool = False, timeout: float = None,
-                  rng_seed: int = None, slices: int = 0, initial: bool = False):
+                  rng_seed: int = None, slices: int = 0, initial: bool = False, paraview: bool = False):
     """Runs the unmodified reference (oracle/_ref/osprey_ref_driver) on
     ``system`` for ``steps`` steps; ``rng_seed`` restarts its pair-noise LCG
     at that value just before the step loop; ``slices`` > 0 sets the analysis
     grid to that many z slices and also returns the last step's slice stress
     profile; ``initial`` adds the builder's state before any step as
-    summary["initial"].  Returns (json summary, dump dict or None, topology dict or None)
+    summary["initial"]; ``paraview`` the bytes of the reference's Paraview
+    snapshot of the last step as summary["paraview"].  Returns (json summary, dump dict or None, topology dict or None)
     or, with ``slices``, (summary, dump, topology, slice dict)."""
     from osprey_dpd_b200 import workloads  # local import: test-side helper
 
@@ -224,6 +225,8 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
         args += ["--slices", "slices.bin", "--slice-dims", dims]
     if initial:
         args += ["--dump-initial", "init.bin"]
+    if paraview:
+        args += ["--paraview", "1"]
     cp = subprocess.run(args, cwd=wd, capture_output=True, text=True, timeout=timeout)
     if cp.returncode != 0:
         raise RuntimeError(f"reference driver failed: {cp.stderr.strip()} {cp.stdout.strip()}")
@@ -234,6 +237,12 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     sl = workloads.read_slices(os.path.join(wd, "slices.bin")) if slices else None
     if initial:
         summary["initial"] = workloads.read_dump(os.path.join(wd, "init.bin"))
+    if paraview:
+        vtk = [f for f in os.listdir(wd) if f.endswith(".vtk")]
+        if len(vtk) != 1:
+            raise RuntimeError(f"expected one Paraview file, found {vtk}")
+        with open(os.path.join(wd, vtk[0]), "rb") as fh:
+            summary["paraview"] = fh.read()
     if own:
         import shutil
         shutil.rmtree(wd, ignore_errors=True)

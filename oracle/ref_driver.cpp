@@ -23,6 +23,7 @@
 // Usage (run inside the directory that holds dmpci.<runId>):
 //   osprey_ref_driver <runId> [--inject state.bin] [--topology topo.bin]
 //                             [--dump out.bin] [--rng-seed S] [--dump-initial init.bin]
+//                             [--paraview 1]
 // Prints one JSON line: {"beads":N,"steps":T,"run_seconds":s,...}
 //
 // Binary formats (little endian):
@@ -42,6 +43,9 @@
 
 #include "StdAfx.h"
 #include "SimDefs.h"
+
+#include "CurrentState.h"
+#include "ParaviewFormat.h"
 
 #include <chrono>
 #include <cstdio>
@@ -117,6 +121,7 @@ int main(int argc, char** argv)
     const char* slicePath = 0;
     const char* sliceDims = 0;
     const char* initialPath = 0;
+    bool paraview = false;
     for (int a = 2; a + 1 < argc; a += 2) {
         if (!strcmp(argv[a], "--inject")) injectPath = argv[a + 1];
         else if (!strcmp(argv[a], "--topology")) topoPath = argv[a + 1];
@@ -125,6 +130,7 @@ int main(int argc, char** argv)
         else if (!strcmp(argv[a], "--slices")) slicePath = argv[a + 1];
         else if (!strcmp(argv[a], "--slice-dims")) sliceDims = argv[a + 1];
         else if (!strcmp(argv[a], "--dump-initial")) initialPath = argv[a + 1];
+        else if (!strcmp(argv[a], "--paraview")) paraview = atoi(argv[a + 1]) != 0;
         else return fail("unknown option");
     }
 
@@ -208,6 +214,16 @@ int main(int argc, char** argv)
     auto tRun1 = std::chrono::steady_clock::now();
 
     if (dumpPath && !write_dump(dumpPath, byId, n, steps)) return fail("cannot open dump file");
+
+    // --paraview 1: the reference's own Paraview snapshot of the final state
+    // (CCurrentState + CParaviewFormat, CurrentState.cpp:109-244,
+    // ParaviewFormat.cpp:72-112), written as dmpccs.<runId>.con.<steps>.vtk
+    if (paraview) {
+        CParaviewFormat* pFormat = new CParaviewFormat(pBox->GetSimSpaceXLength(), pBox->GetSimSpaceYLength(),
+                                                       pBox->GetSimSpaceZLength(), false, pBox->GetBeadTypeTotal());
+        CCurrentState cs(steps, runId, pBox, pFormat, false, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0);
+        if (!cs.Serialize()) return fail("CCurrentState::Serialize failed");
+    }
 
     if (slicePath) {
         long long dims[4] = {0, 0, 0, 0};

@@ -1692,6 +1692,93 @@ int dpd_engine_write_restart(dpd_engine* e, const char* path, int32_t wall, int3
     return DPD_OK;
 }
 
+// The Paraview snapshot of CCurrentState::Serialize with CParaviewFormat
+// (CurrentState.cpp:163-244, ParaviewFormat.cpp:72-112) for n beads in file
+// order: the format's header lines (with their trailing tabs and spaces), one
+// "x y z" line per bead with the stream's default 6-significant-digit
+// formatting, the vertex list and one display id per bead.
+static bool write_paraview_file(const char* path, int64_t n, const double* x3, const int32_t* display_id)
+{
+    const int nth = (int)std::max<unsigned>(1, std::min<unsigned>(16, std::thread::hardware_concurrency()));
+    std::vector<std::string> parts(nth);
+    auto work = [&](int t) {
+        const int64_t k0 = n * t / nth, k1 = n * (t + 1) / nth;
+        std::string& out = parts[t];
+        out.reserve((size_t)(k1 - k0) * 40);
+        char line[128];
+        for (int64_t k = k0; k < k1; ++k) {
+            const int len = snprintf(line, sizeof line, "%.6g %.6g %.6g\n", x3[3 * k], x3[3 * k + 1], x3[3 * k + 2]);
+            out.append(line, (size_t)len);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return false;
+    bool ok = fprintf(fp,
+                      "# vtk DataFile Version 2.0\t\t\t    \n"
+                      "data\t\t\t\t\t\t\t\t\t\t\n"
+                      "ASCII\t\t\t\t\t\t\t\t\t\n"
+                      "DATASET POLYDATA\t\t\t\t\t\t    \n"
+                      "POINTS %lld double\t\t\n",
+                      (long long)n) > 0;
+    for (auto& pstr : parts) ok = ok && fwrite(pstr.data(), 1, pstr.size(), fp) == pstr.size();
+    ok = ok && fprintf(fp, "VERTICES  %lld %lld\n", (long long)n, (long long)(2 * n)) > 0;
+    std::string tail;
+    tail.reserve((size_t)n * 12 + 64);
+    char line[64];
+    for (int64_t k = 0; k < n; ++k) tail.append(line, (size_t)snprintf(line, sizeof line, "1 %lld\n", (long long)k));
+    tail.append("POINT_DATA ");
+    tail.append(std::to_string((long long)n));
+    tail.append("\nSCALARS ptype float 1\nLOOKUP_TABLE  default\n");
+    for (int64_t k = 0; k < n; ++k) tail.append(line, (size_t)snprintf(line, sizeof line, "%d\n", display_id[k]));
+    ok = ok && fwrite(tail.data(), 1, tail.size(), fp) == tail.size();
+    ok = (fclose(fp) == 0) && ok;
+    return ok;
+}
+
+int dpd_write_paraview(const char* path, int64_t n, const double* x3, const int32_t* display_id)
+{
+    if (!path || n < 0 || (n > 0 && (!x3 || !display_id))) return DPD_E_ARG;
+    return write_paraview_file(path, n, x3, display_id) ? DPD_OK : DPD_E_ARG;
+}
+
+int dpd_engine_write_paraview(dpd_engine* e, const char* path, const uint8_t* type_visible, const int32_t* display_id)
+{
+    if (!e) return DPD_E_ARG;
+    if (!path) return fail(e, DPD_E_ARG, "null path");
+    if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "snapshots are written for single-box engines");
+    const int64_t n = e->n;
+    std::vector<double> x(3 * (size_t)n);
+    std::vector<int32_t> cell((size_t)n);
+    int rc = run_download(e, x.data(), nullptr, nullptr, nullptr, nullptr, cell.data());
+    if (rc) return rc;
+    // CSimBox::GetAllBeadsInCNTCells (SimBox.cpp:5883-5895): cells in index
+    // order; inside a cell the reference keeps its list order, the engine the
+    // upload order.  Beads of invisible types are left out (CurrentState.cpp:
+    // 207-223).
+    std::vector<int64_t> order;
+    order.reserve((size_t)n);
+    for (int64_t b = 0; b < n; ++b)
+        if (!type_visible || type_visible[e->h_type[(size_t)b]]) order.push_back(b);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t p, int64_t q) { return cell[(size_t)p] < cell[(size_t)q]; });
+    const int64_t m = (int64_t)order.size();
+    std::vector<double> xo(3 * (size_t)m);
+    std::vector<int32_t> ids((size_t)m);
+    for (int64_t k = 0; k < m; ++k) {
+        const int64_t b = order[(size_t)k];
+        for (int d = 0; d < 3; ++d) xo[3 * (size_t)k + d] = x[3 * (size_t)b + d];
+        // the reference's default display id is the bead type (Monitor.cpp:277)
+        ids[(size_t)k] = display_id ? display_id[b] : e->h_type[(size_t)b];
+    }
+    if (!write_paraview_file(path, m, xo.data(), ids.data()))
+        return fail(e, DPD_E_ARG, std::string("write failed: ") + path);
+    return DPD_OK;
+}
+
 int dpd_engine_set_pair_params(dpd_engine* e, int32_t ntypes, const double* a, const double* gamma)
 {
     if (!e) return DPD_E_ARG;

@@ -39,6 +39,7 @@ EXPORTED = [
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
     "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
+    "dpd_write_paraview", "dpd_engine_write_paraview",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -95,6 +96,8 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_create.argtypes = [C.POINTER(DpdParams), C.POINTER(vp)]
     L.dpd_engine_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 7
     L.dpd_engine_build_random.argtypes = [vp, C.c_int64, vp, vp, C.c_uint64, C.c_int64, C.c_int64, vp, vp, vp, vp]
+    L.dpd_write_paraview.argtypes = [C.c_char_p, C.c_int64, vp, vp]
+    L.dpd_engine_write_paraview.argtypes = [vp, C.c_char_p, vp, vp]
     L.dpd_engine_upload_topology.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
     L.dpd_engine_set_pair_params.argtypes = [vp, C.c_int32, vp, vp]
     L.dpd_engine_set_dt.argtypes = [vp, C.c_double]
@@ -132,6 +135,18 @@ def load(path: Optional[str] = None) -> C.CDLL:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def write_paraview(path: str, x, display_id) -> None:
+    """A Paraview snapshot of beads in file order from host arrays
+    (dpd_write_paraview; needs no GPU)."""
+    xv = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+    dv = np.ascontiguousarray(display_id, np.int32)
+    if len(dv) != len(xv):
+        raise ValueError("one display id per bead")
+    rc = load().dpd_write_paraview(str(path).encode(), len(xv), _p(xv), _p(dv))
+    if rc != 0:
+        raise EngineError(f"dpd_write_paraview failed ({rc})")
 
 
 def restart_layout(system):
@@ -327,6 +342,13 @@ class DpdEngine:
         self._rs = (order, pid, pty, np.full(self._a.shape[0], float(radius)))
         self._check(load().dpd_engine_set_restart_layout(self.h, len(order), *[_p(a) for a in self._rs]),
                     "set_restart_layout")
+
+    def write_paraview(self, path: str, type_visible=None, display_id=None) -> None:
+        """The current state as a Paraview snapshot (dpd_engine_write_paraview):
+        beads by CNT cell, optional per-type visibility and per-bead display ids."""
+        tv = None if type_visible is None else np.ascontiguousarray(type_visible, np.uint8)
+        di = None if display_id is None else np.ascontiguousarray(display_id, np.int32)
+        self._check(load().dpd_engine_write_paraview(self.h, str(path).encode(), _p(tv), _p(di)), "write_paraview")
 
     def write_restart(self, path: str, wall: bool = False, gravity: bool = False, shear: bool = False) -> None:
         self._check(load().dpd_engine_write_restart(self.h, os.fsencode(path), int(wall), int(gravity), int(shear)),
