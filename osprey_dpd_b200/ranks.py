@@ -45,6 +45,11 @@ class Ranks:
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
             self._dist = dist
 
+    @property
+    def dist(self):
+        """The torch.distributed module when a process group is open, else None."""
+        return self._dist
+
     def barrier(self) -> None:
         if self._dist is not None:
             self._dist.barrier()

@@ -121,7 +121,7 @@ class SlabDecomposition:
         the peer's "down" records arrive as "from above" and its "up" records
         as "from below", as they must."""
         import torch
-        dist = self.g._dist
+        dist = self.g.dist
         dev = self.g.device
         below, above = (self.rank - 1) % self.world, (self.rank + 1) % self.world
         n_out = torch.tensor([len(to_below), len(to_above)], dtype=torch.int64, device=dev)
@@ -221,7 +221,7 @@ class SlabDecomposition:
             allrec = [self.owned]
         else:
             allrec = [None] * self.world
-            self.g._dist.all_gather_object(allrec, self.owned)
+            self.g.dist.all_gather_object(allrec, self.owned)
         if self.rank != 0:
             return None
         rec = np.concatenate(allrec)
