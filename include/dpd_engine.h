@@ -166,12 +166,27 @@ DPD_API int dpd_engine_set_thermostat(dpd_engine* e, int32_t on);
 /* CCNTCell::ToggleDPDBeadConservativeForces (CNTCell.cpp:235). */
 DPD_API int dpd_engine_set_conservative(dpd_engine* e, int32_t on);
 
+/* CSimBox::UpdateRenormalisedMom (SimBox.cpp:3177-3225), which the
+ * reference's Run calls before Evolve when momentum renormalisation is on and
+ * m_SimTime % period == 0 (SimBox.cpp:1314-1317): every bead's momentum is
+ * divided by sqrt(sum v^2 / (3 N kT)), the sum taken in FP64 on the device.
+ * Asynchronous (queued on the engine's stream).  Single-box engines; kT > 0. */
+DPD_API int dpd_engine_renormalise_mom(dpd_engine* e);
+
 /* Runs nsteps timesteps; first_step is the reference's m_SimTime of the first
  * (it keys the pair noise).  Asynchronous: returns once the work is queued,
  * without waiting for earlier calls.  The kernels of a call are captured once
  * as a CUDA graph per (step count, buffer parity, sample pattern, stream) and
  * replayed after that (DPD_GRAPHS=0 launches them one by one).  The
- * single-bead sums are taken at the end of the last step. */
+ * single-bead sums are taken at the end of the last step.
+ * Returns the last device status without waiting: each call's first kernel
+ * publishes the status word of all work queued before it to pinned host
+ * memory, and the next call reads that word; if it holds a bit of
+ * DPD_STATUS_FATAL_MASK the call returns DPD_E_STATUS (message in
+ * dpd_engine_last_error) and queues nothing, so a fatal condition surfaces
+ * at most two calls after the step that raised it (at once after
+ * dpd_engine_status, download, cells or observables, which wait).  A new
+ * bead upload clears the status. */
 DPD_API int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps);
 
 /* Steps at which the single-bead sums and the per-bead virial are taken:
@@ -358,11 +373,11 @@ DPD_API int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out);
 /* ---- Pair forces without any allocation ---------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that may not allocate device memory at the moment they need forces: a host
- * program whose memory pool owns the whole GPU, a capture-sensitive or
- * real-time loop where cudaMalloc would synchronise or stall the device, or a
- * plug-in whose host forbids library-side allocations.  Such a caller owns
- * its bead and force buffers but cannot give the engine the cell-list
- * scratch it would otherwise cudaMalloc (dpd_engine_create/upload).
+ * program whose memory pool owns the whole GPU, a real-time loop where
+ * cudaMalloc would stall the device, or a plug-in whose host forbids
+ * library-side allocations.  Such a caller owns its bead and force buffers
+ * but cannot give the engine the cell-list scratch it would otherwise
+ * cudaMalloc (dpd_engine_create/upload).
  *
  * It computes the DPD pair forces of CCNTCell::UpdateForce (conservative,
  * dissipative and random; FP32 arithmetic, the engine's pair kernel) for
@@ -371,19 +386,24 @@ DPD_API int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out);
  * keys the pair noise), and writes them as FP64 to f3 in the caller's bead
  * order.  x3, v3, f3 (n*3 doubles, xyz interleaved), type and id (n int32)
  * are DEVICE pointers.  params->precision is ignored; params->device selects
- * the GPU (-1: current).  The work is queued on cuda_stream (NULL: the legacy
- * default stream) and the call returns after it has finished.
+ * the GPU (-1: current; the caller's current device is restored before the
+ * call returns).  The work is queued on cuda_stream (NULL: the legacy
+ * default stream) and the call is synchronous: it waits for that stream
+ * (cudaStreamSynchronize) before it returns, to read its status word.
  *
  * Scratch: one fixed file-scope device array of about 4.5 MB, held by every
  * GPU that loads the library until the process exits.  Limits:
  * n <= DPD_NOALLOC_MAX_BEADS and nx*ny*nz <= DPD_NOALLOC_MAX_CELLS, otherwise
  * DPD_E_LIMIT with nothing launched.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the one array and each call clears the
- * parts that must start at zero, so calls that overlap on the GPU (other
- * threads or streams on the same device) race and must be serialised by the
- * caller.  Returns DPD_E_BOX if a position lies outside the box (forces are
- * then not meaningful), DPD_E_ARG for bad arguments, DPD_E_CUDA on a CUDA
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of
+ * the process; make that first call before any stream capture, and do not
+ * reset the device's context (cudaDeviceReset) between calls.  All calls
+ * share the one array and each call clears the parts that must start at
+ * zero, so calls that overlap on the GPU (other threads or streams on the
+ * same device) race and must be serialised by the caller.  Returns DPD_E_BOX
+ * if a position lies outside the box (forces are then not meaningful),
+ * DPD_E_ARG for bad arguments, including a bead type outside 0..ntypes-1
+ * (found on the device; forces then not meaningful), DPD_E_CUDA on a CUDA
  * error.  No cudaMalloc, cudaFree or other allocating routine is called. */
 #define DPD_NOALLOC_MAX_BEADS   65536
 #define DPD_NOALLOC_MAX_CELLS   32768

@@ -685,6 +685,27 @@ static void update_mom(dpdo_sim* s)
         }
 }
 
+/* CSimBox::UpdateRenormalisedMom, SimBox.cpp:3177-3225: the squared momenta
+ * of all beads in the CNT cells, summed cell by cell in list order (x, y, z
+ * of a bead in turn), give the scale sqrt(sum / (3 N kT)) that every
+ * momentum component is divided by. */
+int dpdo_renormalise_mom(dpdo_sim* s)
+{
+    if (!s || s->n <= 0 || !(s->p.kT > 0.0)) return -1;
+    double sum = 0.0;
+    for (int64_t c = 0; c < s->ncell; ++c)
+        for (int32_t b = s->head[c]; b >= 0; b = s->next[b]) {
+            sum += s->v[3 * b] * s->v[3 * b];
+            sum += s->v[3 * b + 1] * s->v[3 * b + 1];
+            sum += s->v[3 * b + 2] * s->v[3 * b + 2];
+        }
+    const double scale = sqrt(sum / (3.0 * (double)s->n * s->p.kT));
+    for (int64_t c = 0; c < s->ncell; ++c)
+        for (int32_t b = s->head[c]; b >= 0; b = s->next[b])
+            for (int d = 0; d < 3; ++d) s->v[3 * b + d] = s->v[3 * b + d] / scale;
+    return 0;
+}
+
 /* CCNTCell::CheckBeadsinCell, CNTCell.cpp:2628-2700. */
 static void check_cells(dpdo_sim* s)
 {

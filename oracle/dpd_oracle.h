@@ -101,6 +101,8 @@ int64_t dpdo_slice_errors(const dpdo_sim* s);
 int dpdo_set_dt(dpdo_sim* s, double dt);
 /* a_ij / gamma_ij update (CNTCell.cpp:434-456 sets both (i,j) and (j,i)). */
 int dpdo_set_pair(dpdo_sim* s, int32_t ti, int32_t tj, double a, double gamma);
+/* CSimBox::UpdateRenormalisedMom (SimBox.cpp:3177-3225): momenta rescaled to kT. */
+int dpdo_renormalise_mom(dpdo_sim* s);
 
 /* Random initial state of CRandomBuilder::Assemble (RandomBuilder.cpp:71-361,
  * no walls, 3-d): positions x3 and velocities v3 (3 per bead, bead order) for

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
         L.dpdo_philox_pair.restype = C.c_uint32
         L.dpdo_set_dt.argtypes = [vp, C.c_double]
         L.dpdo_set_pair.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+        L.dpdo_renormalise_mom.argtypes = [vp]
         L.dpdo_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
         L.dpdo_get_slice_stress.argtypes = [vp, vp, vp, vp]
         L.dpdo_slice_errors.argtypes = [vp]
@@ -163,6 +164,11 @@ class Oracle:
 
     def set_pair(self, ti: int, tj: int, a: float, gamma: float) -> None:
         lib().dpdo_set_pair(self.h, ti, tj, a, gamma)
+
+    def renormalise_mom(self) -> None:
+        """CSimBox::UpdateRenormalisedMom (SimBox.cpp:3177-3225)."""
+        if lib().dpdo_renormalise_mom(self.h) != 0:
+            raise RuntimeError("dpdo_renormalise_mom failed")
 
     def __del__(self):
         h = getattr(self, "h", None)

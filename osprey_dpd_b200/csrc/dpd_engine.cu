@@ -144,6 +144,7 @@ struct dpd_engine {
     int* d_block_count = nullptr;
     double* d_partials = nullptr;
     double* d_obs = nullptr;
+    double* d_renorm = nullptr;     // kinetic sums of dpd_engine_renormalise_mom (kObsTerms)
     // download staging
     double* d_out = nullptr;    // 3n x, 3n u, 3n v, 3n f, 9n stress
     int* d_out_cell = nullptr;
@@ -164,6 +165,11 @@ struct dpd_engine {
     double* d_ang_sin0 = nullptr;
     // pinned host
     unsigned* h_status = nullptr;
+    // status word as of the start of the latest call's device work, written by
+    // that call's k_set_step into mapped pinned memory (d_seen is its device
+    // address); read by dpd_engine_step without waiting
+    unsigned* h_seen = nullptr;
+    unsigned* d_seen = nullptr;
     double* h_obs = nullptr;
     bool obs_valid = false;
     bool obs_has_virial = false;
@@ -769,9 +775,16 @@ static int create_impl(const dpd_params* p, int32_t nboxes, const dpd_box* bx, d
         if ((rc = dalloc(e, &e->d_start, (size_t)ncell + 1))) break;
         if ((rc = dalloc(e, &e->d_block_count, (size_t)e->nchunk))) break;
         if ((rc = dalloc(e, &e->d_obs, kObsTerms))) break;
+        if ((rc = dalloc(e, &e->d_renorm, kObsTerms))) break;
         if (cudaMallocHost(&e->h_status, sizeof(unsigned)) != cudaSuccess ||
-            cudaMallocHost(&e->h_obs, kObsTerms * sizeof(double)) != cudaSuccess) {
+            cudaMallocHost(&e->h_obs, kObsTerms * sizeof(double)) != cudaSuccess ||
+            cudaHostAlloc(&e->h_seen, sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess) {
             rc = fail(e, DPD_E_NOMEM, "cudaMallocHost failed");
+            break;
+        }
+        *e->h_seen = 0u;
+        if (cudaHostGetDevicePointer((void**)&e->d_seen, e->h_seen, 0) != cudaSuccess || !e->d_seen) {
+            rc = fail(e, DPD_E_CUDA, "cudaHostGetDevicePointer failed");
             break;
         }
         if (cudaMemset(e->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
@@ -820,6 +833,7 @@ void dpd_engine_destroy(dpd_engine* e)
     e->allocations.clear();
     if (e->h_status) cudaFreeHost(e->h_status);
     if (e->h_obs) cudaFreeHost(e->h_obs);
+    if (e->h_seen) cudaFreeHost(e->h_seen);
     if (e->side) cudaStreamSynchronize(e->side);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->ev_join) cudaEventDestroy(e->ev_join);
@@ -1080,6 +1094,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)n, st));
     CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
     CU(cudaStreamSynchronize(st));
+    *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine is in flight after the sync
     rc = empty_topology(e, same_n);
     if (rc) return rc;
     e->uploaded = true;
@@ -1838,16 +1853,52 @@ int dpd_engine_set_conservative(dpd_engine* e, int32_t on)
     return push_constants(e);
 }
 
+int dpd_engine_renormalise_mom(dpd_engine* e)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    if (e->hboxes.size() != 1) return fail(e, DPD_E_ARG, "momentum renormalisation is for single-box engines");
+    if (!(e->params.kT > 0.0)) return fail(e, DPD_E_ARG, "momentum renormalisation needs kT > 0");
+    CU(cudaSetDevice(e->device));
+    int rc;
+    // the next step's drift, if done ahead, used the old momenta
+    if ((rc = drop_ahead(e))) return rc;
+    const int n = (int)e->n;
+    const int nb = blocks_for(n, kThreads);
+    double* v = e->d_v[e->cur];
+    k_kinetic_partials<<<nb, kThreads, 0, e->s()>>>(n, e->d_x[e->cur], v, e->d_partials);
+    if ((rc = check_launch(e, "k_kinetic_partials"))) return rc;
+    k_reduce_obs<<<1, 32 * kObsTerms, 0, e->s()>>>(nb, e->d_partials, e->d_renorm);
+    if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
+    k_renorm_scale<<<nb, kThreads, 0, e->s()>>>(n, v, e->d_renorm, 3.0 * (double)n * e->params.kT);
+    if ((rc = check_launch(e, "k_renorm_scale"))) return rc;
+    e->obs_valid = false;
+    return DPD_OK;
+}
+
 int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
 {
     if (!e) return DPD_E_ARG;
     if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
     if (nsteps < 0) return fail(e, DPD_E_ARG, "negative step count");
+    // The status word as published by the latest call whose device work has
+    // started (no wait): a fatal bit stops the run here, as the reference's
+    // CLogSimErrorTrace + ccStopNoSave would (SimBox.cpp:436-445), and no
+    // further work is queued on the invalid state.
+    const unsigned seen = *(volatile unsigned*)e->h_seen;
+    if (seen & DPD_STATUS_FATAL_MASK) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "device status 0x%x: %s%s%s", seen,
+                 (seen & DPD_STATUS_NONFINITE) ? "non-finite position, velocity or force; " : "",
+                 (seen & DPD_STATUS_IMAGE_OVERFLOW) ? "periodic image counter overflow; " : "",
+                 (seen & DPD_STATUS_INTERNAL) ? "internal capacity check" : "");
+        return fail(e, DPD_E_STATUS, msg);
+    }
     if (nsteps == 0) return DPD_OK;
     CU(cudaSetDevice(e->device));
     // the step counter keys the pair noise; it is advanced on the device
     // by the last kernel of every step
-    k_set_step<<<1, 1, 0, e->s()>>>(e->d_step, first_step);
+    k_set_step<<<1, 1, 0, e->s()>>>(e->d_step, first_step, e->d_status, e->d_seen);
     CU(cudaGetLastError());
     e->launches += 1;
     std::vector<char> samples(nsteps);
@@ -1930,6 +1981,7 @@ int dpd_engine_status(dpd_engine* e, uint32_t* bits)
     CU(cudaMemcpyAsync(e->h_status, e->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, e->s()));
     CU(cudaStreamSynchronize(e->s()));
     if (bits) *bits = *e->h_status;
+    *(volatile unsigned*)e->h_seen = *e->h_status;   // nothing in flight: the next step call sees it at once
     return DPD_OK;
 }
 

@@ -856,8 +856,15 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
 }
 
 // Sets the step counter that keys the pair noise (a launch argument, so the
-// host queues it without waiting for earlier work).
-static __global__ void k_set_step(int64_t* __restrict__ step_ptr, int64_t value) { *step_ptr = value; }
+// host queues it without waiting for earlier work) and publishes the status
+// word of all work queued before it to `seen`, a word of mapped pinned host
+// memory that the host reads without waiting (dpd_engine_step).
+static __global__ void k_set_step(int64_t* __restrict__ step_ptr, int64_t value, const unsigned* __restrict__ status,
+                                  unsigned* seen)
+{
+    *step_ptr = value;
+    *(volatile unsigned*)seen = *status;
+}
 
 // Fixed-order sum of the per-block partials (deterministic): one warp per
 // term, coalesced reads of the term-major partials into four running sums per
@@ -918,6 +925,19 @@ static __global__ void __launch_bounds__(256) k_kinetic_partials(int n, const do
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w][threadIdx.x];
         partials[threadIdx.x * gridDim.x + blockIdx.x] = a;   // term-major
     }
+}
+
+// CSimBox::UpdateRenormalisedMom (SimBox.cpp:3177-3225): every momentum
+// component divided by sqrt(sum v^2 / denom), denom = 3 N kT; sums[3..5] are
+// the per-axis squared-momentum sums of k_kinetic_partials + k_reduce_obs.
+static __global__ void __launch_bounds__(256) k_renorm_scale(int n, double* __restrict__ v,
+                                                           const double* __restrict__ sums, double denom)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double scale = sqrt((sums[3] + sums[4] + sums[5]) / denom);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d * n + s] = v[d * n + s] / scale;
 }
 
 // ---------------------------------------------------------------- download

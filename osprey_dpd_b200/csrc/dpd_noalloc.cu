@@ -4,11 +4,12 @@
 // allocator) at the point where it wants forces.  Typical cases are a host
 // application that hands the GPU to a memory pool it does not control (the
 // pool owns all device memory, so a stray cudaMalloc fails or fragments it),
-// real-time or capture-sensitive loops where an allocation would stall or
-// synchronise the device, and plug-ins embedded in a program whose
-// allocator policy forbids library-side allocations.  Such a caller already
-// owns device buffers for its beads and its forces; it only lacks the
-// cell-list scratch that the engine (dpd_engine_*) allocates for itself.
+// real-time loops where an allocation would stall the device, and plug-ins
+// embedded in a program whose allocator policy forbids library-side
+// allocations.  Such a caller already owns device buffers for its beads and
+// its forces; it only lacks the cell-list scratch that the engine
+// (dpd_engine_*) allocates for itself.  The call waits for its own work (it
+// synchronises the caller's stream before it returns).
 //
 // Here that scratch lives in one file-scope __device__ array of fixed size,
 // so the call needs nothing but the caller's input and output buffers.  The
@@ -72,6 +73,8 @@ std::mutex g_setup_mutex;
 void* g_scratch_addr[kNaMaxDevices] = {};
 
 // Once per device, with that device current: the device address of the array.
+// The address is kept for the life of the process, so a context reset
+// (cudaDeviceReset) between calls is not supported.
 int noalloc_scratch_for_current_device(unsigned char** out)
 {
     int dev = -1;
@@ -130,13 +133,14 @@ __global__ void k_na_place(int n, const int* __restrict__ cell, const int* __res
 
 // Final slot = cell start + rank of the bead index among the cell's beads;
 // writes the force kernel's shadows (position relative to the cell origin,
-// type; velocity, noise id).
+// type; velocity, noise id).  A type outside 0..ntypes-1 would index past the
+// pair tables: it sets status bit 2 and is replaced by type 0.
 __global__ void k_na_shadows(int n, const StepConst* __restrict__ K, const int* __restrict__ perm,
                              const int* __restrict__ cell, const int* __restrict__ start,
                              const double* __restrict__ x3, const double* __restrict__ v3,
                              const int32_t* __restrict__ type, const int32_t* __restrict__ id,
                              int* __restrict__ order, int* __restrict__ slot_cell, float4* __restrict__ pos4,
-                             float4* __restrict__ vel4)
+                             float4* __restrict__ vel4, unsigned* __restrict__ status)
 {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
@@ -152,7 +156,12 @@ __global__ void k_na_shadows(int n, const StepConst* __restrict__ K, const int* 
     p.x = (float)__dadd_rn(x3[3 * i], -__dmul_rn((double)ci[0], K->w[0]));
     p.y = (float)__dadd_rn(x3[3 * i + 1], -__dmul_rn((double)ci[1], K->w[1]));
     p.z = (float)__dadd_rn(x3[3 * i + 2], -__dmul_rn((double)ci[2], K->w[2]));
-    p.w = __int_as_float(type[i] & 0xFFFF);
+    int ti = type[i];
+    if (ti < 0 || ti >= K->ntypes) {
+        atomicOr(status, 2u);
+        ti = 0;
+    }
+    p.w = __int_as_float(ti);
     w.x = (float)v3[3 * i];
     w.y = (float)v3[3 * i + 1];
     w.z = (float)v3[3 * i + 2];
@@ -178,6 +187,10 @@ inline int nblk(int64_t n) { return (int)((n + kNaThreads - 1) / kNaThreads); }
 
 }  // namespace
 
+static int pair_forces_on_current_device(const dpd_params* p, int64_t step, int64_t n, int64_t ncell,
+                                         const double* x3, const double* v3, const int32_t* type,
+                                         const int32_t* id, double* f3, void* cuda_stream);
+
 extern "C" DPD_API int dpd_pair_forces_noalloc(const dpd_params* p, int64_t step, int64_t n,
                                                const double* x3, const double* v3, const int32_t* type,
                                                const int32_t* id, double* f3, void* cuda_stream)
@@ -188,7 +201,20 @@ extern "C" DPD_API int dpd_pair_forces_noalloc(const dpd_params* p, int64_t step
         return DPD_E_ARG;
     const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
     if (n > DPD_NOALLOC_MAX_BEADS || ncell > DPD_NOALLOC_MAX_CELLS) return DPD_E_LIMIT;
-    if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) return DPD_E_CUDA;
+    // the caller's current device is restored on every return below
+    int caller_dev = -1;
+    if (cudaGetDevice(&caller_dev) != cudaSuccess) return DPD_E_CUDA;
+    if (p->device >= 0 && p->device != caller_dev && cudaSetDevice(p->device) != cudaSuccess) return DPD_E_CUDA;
+    const int rc = pair_forces_on_current_device(p, step, n, ncell, x3, v3, type, id, f3, cuda_stream);
+    if (p->device >= 0 && p->device != caller_dev && cudaSetDevice(caller_dev) != cudaSuccess) return DPD_E_CUDA;
+    return rc;
+}
+
+// The work of dpd_pair_forces_noalloc with its device already current.
+static int pair_forces_on_current_device(const dpd_params* p, int64_t step, int64_t n, int64_t ncell,
+                                         const double* x3, const double* v3, const int32_t* type,
+                                         const int32_t* id, double* f3, void* cuda_stream)
+{
     unsigned char* base = nullptr;
     int rc = noalloc_scratch_for_current_device(&base);
     if (rc != DPD_OK) return rc;
@@ -240,7 +266,7 @@ extern "C" DPD_API int dpd_pair_forces_noalloc(const dpd_params* p, int64_t step
     k_scan_cells<<<nchunk, kScanThreads, 0, st>>>(nc, nn, dCount, dChunk, dStart);
     k_na_place<<<nblk(nn), kNaThreads, 0, st>>>(nn, dCell, dRank, dStart, dPerm);
     k_na_shadows<<<nblk(nn), kNaThreads, 0, st>>>(nn, dK, dPerm, dCell, dStart, x3, v3, type, id, dOrder,
-                                                  dSlotCell, dPos, dVel);
+                                                  dSlotCell, dPos, dVel, dStatus);
     k_pair_forces_ref<float, false><<<(nn + 127) / 128, 128, 0, st>>>(nn, dK, dStep, dTab, dSlotCell, dStart,
                                                                       dPos, dVel, dF, nullptr);
     k_na_scatter<<<nblk(nn), kNaThreads, 0, st>>>(nn, dOrder, dF, f3);
@@ -249,5 +275,6 @@ extern "C" DPD_API int dpd_pair_forces_noalloc(const dpd_params* p, int64_t step
     if (cudaMemcpyAsync(&status, dStatus, sizeof status, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return DPD_E_CUDA;
-    return status ? DPD_E_BOX : DPD_OK;
+    if (status & 2u) return DPD_E_ARG;   // a bead type outside 0..ntypes-1
+    return (status & 1u) ? DPD_E_BOX : DPD_OK;
 }

@@ -39,7 +39,7 @@ EXPORTED = [
     "dpd_batch_observables", "dpd_engine_set_launch_shape", "dpd_engine_set_pair_scheme",
     "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
-    "dpd_write_paraview", "dpd_engine_write_paraview",
+    "dpd_write_paraview", "dpd_engine_write_paraview", "dpd_engine_renormalise_mom",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -103,6 +103,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_dt.argtypes = [vp, C.c_double]
     L.dpd_engine_set_thermostat.argtypes = [vp, C.c_int32]
     L.dpd_engine_set_conservative.argtypes = [vp, C.c_int32]
+    L.dpd_engine_renormalise_mom.argtypes = [vp]
     L.dpd_engine_step.argtypes = [vp, C.c_int64, C.c_int32]
     L.dpd_engine_status.argtypes = [vp, C.POINTER(C.c_uint32)]
     L.dpd_engine_download.argtypes = [vp] + [vp] * 5
@@ -266,6 +267,9 @@ class DpdEngine:
 
     def set_conservative(self, on: bool) -> None:
         self._check(load().dpd_engine_set_conservative(self.h, int(bool(on))), "set_conservative")
+
+    def renormalise_mom(self) -> None:
+        self._check(load().dpd_engine_renormalise_mom(self.h), "renormalise_mom")
 
     def step(self, first_step: int, nsteps: int) -> None:
         self._check(load().dpd_engine_step(self.h, int(first_step), int(nsteps)), "step")

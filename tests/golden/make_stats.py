@@ -8,7 +8,8 @@ distribution function, and for the polymer melt the bond-length and
 end-to-end-distance distributions.  Standard errors come from block
 averages.  Written to stats_*.npz here:
 
-    python tests/golden/make_stats.py
+    python tests/golden/make_stats.py            # 3,000-bead water, 10^3 polymer melt
+    python tests/golden/make_stats.py --large    # 12,288-bead water (RDF) and H3T6 bilayer
 """
 import os
 import sys
@@ -33,6 +34,21 @@ def water_system():
 
 def polymer_system():
     return W.polymer_solution(cells=(10, 10, 10), seed=W.BASE_SEED + 40)
+
+
+def water16_system():
+    """12,288-bead water box: the RDF reference at the 1e-3 bound."""
+    return W.water(16, seed=W.BASE_SEED + 160)
+
+
+def bilayer16_system():
+    """H3T6 bilayer in water, 16^3 cells (12,288 beads, 376 lipids: the area
+    per lipid of the 393,216-bead workload), bonds and tail bond pairs."""
+    return W.bilayer(cells=(16, 16, 16), nlipids=376, seed=W.BASE_SEED + 161)
+
+
+# Bonds of the bilayer: head-tail bead pairs of the linear H3T6 chains.
+BILAYER_CHAIN = 9
 
 
 def rdf_counts(x, L):
@@ -61,6 +77,12 @@ def chain_stats(u, chain_len, nchains):
     return np.histogram(b, BOND_BINS)[0].astype(np.float64), np.histogram(e, E2E_BINS)[0].astype(np.float64)
 
 
+def bond_lengths(u, head, tail):
+    """Histogram of the lengths of the given bonds (unPBC positions, 0-based bead indices)."""
+    d = u[head] - u[tail]
+    return np.histogram(np.sqrt((d * d).sum(axis=1)), BOND_BINS)[0].astype(np.float64)
+
+
 def block_se(samples, nblocks=10):
     a = np.asarray(samples, dtype=np.float64)
     m = len(a) // nblocks
@@ -81,30 +103,35 @@ class Sampler:
         self.nsnap = 0
         self.polymer = polymer
 
-    def add(self, x, u, v, virial_trace):
+    def add(self, x, u, v, virial_trace, rdf=True):
         n = self.s.n
         v2 = float((v * v).sum())
         V = float(np.prod(self.L))
         self.kT.append(v2 / (3.0 * n))
         self.P.append(0.3333333333 * (1.0 / V) * (v2 + virial_trace))
-        self.rdf += rdf_counts(x, self.L)
-        if self.polymer:
+        if rdf:
+            self.rdf += rdf_counts(x, self.L)
+            self.nsnap += 1
+        if self.polymer == "bonds":
+            self.bond += bond_lengths(u, self.s.bond_head - 1, self.s.bond_tail - 1)
+        elif self.polymer:
             b, e = chain_stats(u, *self.polymer)
             self.bond += b
             self.e2e += e
-        self.nsnap += 1
 
     def result(self):
         out = {"kT_mean": np.mean(self.kT), "kT_se": block_se(self.kT), "P_mean": np.mean(self.P),
                "P_se": block_se(self.P), "nsnap": self.nsnap,
                "rdf": rdf_normalise(self.rdf, self.nsnap, self.s.n, self.L), "rdf_bins": RDF_BINS}
-        if self.polymer:
+        if self.polymer == "bonds":
+            out.update(bond=self.bond / self.bond.sum(), bond_bins=BOND_BINS)
+        elif self.polymer:
             out.update(bond=self.bond / self.bond.sum(), bond_bins=BOND_BINS, e2e=self.e2e / self.e2e.sum(),
                        e2e_bins=E2E_BINS)
         return out
 
 
-def run_oracle(system, equil, steps, every, polymer=None):
+def run_oracle(system, equil, steps, every, polymer=None, rdf=True):
     import dpd_oracle
     o = dpd_oracle.Oracle(system, noise=dpd_oracle.NOISE_LCG)
     o.step(1, equil)
@@ -115,8 +142,18 @@ def run_oracle(system, equil, steps, every, polymer=None):
         t += every
         st = o.state()
         tr = st["stress"].sum(axis=0)
-        smp.add(st["x"], st["unpbc"], st["v"], tr[0] + tr[4] + tr[8])
+        smp.add(st["x"], st["unpbc"], st["v"], tr[0] + tr[4] + tr[8], rdf=rdf)
     return smp.result()
+
+
+def large():
+    """The 12,288-bead water and bilayer references (several minutes each)."""
+    res = run_oracle(water16_system(), 1000, 40000, 10)
+    np.savez_compressed(os.path.join(HERE, "stats_water_16.npz"), equil=1000, steps=40000, every=10, **res)
+    print("water16", res["kT_mean"], res["kT_se"], res["P_mean"], res["P_se"])
+    res = run_oracle(bilayer16_system(), 2000, 20000, 10, polymer="bonds", rdf=False)
+    np.savez_compressed(os.path.join(HERE, "stats_bilayer_16.npz"), equil=2000, steps=20000, every=10, **res)
+    print("bilayer16", res["kT_mean"], res["kT_se"], res["P_mean"], res["P_se"])
 
 
 def main():
@@ -132,4 +169,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "--large" in sys.argv:
+        large()
+    else:
+        main()

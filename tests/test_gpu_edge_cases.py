@@ -190,3 +190,85 @@ def test_parameter_mutators_follow_the_reference(engine_mod, oracle_mod):
     eng.set_thermostat(True)
     eng.step(6, 1)
     assert eng.status() == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_conservative_toggle_follows_the_reference(engine_mod, oracle_mod, precision):
+    """ToggleDPDBeadConservativeForces (CNTCell.cpp:235-310): off zeroes every
+    a_ij, on restores the tables it saved."""
+    s = W.binary_mixture(cells=(6, 7, 8))
+    eng, orc = _both(engine_mod, oracle_mod, s, precision)
+    tol = 1e-4 if precision == 0 else 1e-10
+    eng.step(1, 2)
+    orc.step(1, 2)
+    eng.set_conservative(False)
+    for i in range(2):
+        for j in range(i, 2):
+            orc.set_pair(i, j, 0.0, s.gamma[i, j])
+    eng.step(3, 2)
+    orc.step(3, 2)
+    assert rel_err(eng.download()["f"], orc.state()["f"]) < tol
+    eng.set_conservative(True)
+    for i in range(2):
+        for j in range(i, 2):
+            orc.set_pair(i, j, s.a[i, j], s.gamma[i, j])
+    eng.step(5, 2)
+    orc.step(5, 2)
+    g, o = eng.download(), orc.state()
+    assert rel_err(g["f"], o["f"]) < tol
+    assert np.array_equal(eng.cells(), orc.cells())
+    assert eng.status() == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_renormalised_momenta_follow_the_reference(engine_mod, oracle_mod, precision):
+    """CSimBox::UpdateRenormalisedMom (SimBox.cpp:3177-3225) between steps, as
+    the reference's Run calls it before Evolve (SimBox.cpp:1314-1317)."""
+    s = W.bilayer(cells=(12, 12, 12), nlipids=60)
+    s.v *= 1.7          # far from kT = 1, so the rescale is large
+    eng, orc = _both(engine_mod, oracle_mod, s, precision)
+    eng.step(1, 3)
+    orc.step(1, 3)
+    eng.renormalise_mom()
+    orc.renormalise_mom()
+    g, o = eng.download(), orc.state()
+    vtol = 1e-5 if precision == 0 else 1e-12
+    assert rel_err(g["v"], o["v"], scale=1.0) < vtol
+    kT = float((g["v"] ** 2).sum() / (3 * s.n))
+    assert abs(kT - s.kT) < 1e-12
+    # the renormalised momenta drive the next drift
+    eng.step(4, 2)
+    orc.step(4, 2)
+    g, o = eng.download(), orc.state()
+    ftol = 1e-4 if precision == 0 else 1e-10
+    assert rel_err(g["f"], o["f"]) < ftol
+    assert float(np.max(np.abs(g["unpbc"] - o["unpbc"]))) < (1e-6 if precision == 0 else 1e-12)
+    assert eng.status() == 0
+
+
+def test_step_returns_the_fatal_status_without_waiting(engine_mod):
+    """A non-finite state raised on the device is returned by a later
+    dpd_engine_step (DPD_E_STATUS, no further work queued) without a
+    synchronous status call: at most two calls after the step that raised it."""
+    s = W.water(6)
+    eng = engine_mod.DpdEngine.from_system(s, precision=engine_mod.MIXED)
+    f = np.zeros_like(s.x)
+    f[10] = [1e308, 0.0, 0.0]
+    eng.upload_beads(s.ids, s.types, s.movable, s.x, s.unpbc, s.v, f)
+    import torch
+    eng.step(1, 1)                       # raises the non-finite bit on the device
+    torch.cuda.synchronize()             # the device work has finished; no engine call waited for it
+    eng.step(2, 1)                       # its first kernel publishes the status of call 1
+    torch.cuda.synchronize()
+    with pytest.raises(engine_mod.EngineError, match=r"\(-5\).*non-finite"):
+        eng.step(3, 1)
+    l0 = eng.launch_count()
+    with pytest.raises(engine_mod.EngineError):
+        eng.step(3, 1)
+    assert eng.launch_count() == l0      # nothing is queued on the invalid state
+    # a fresh upload clears the status and the engine steps again
+    eng.upload_beads(s.ids, s.types, s.movable, s.x, s.unpbc, s.v)
+    eng.step(10, 2)
+    eng.step(12, 2)
+    assert eng.status() == 0
+    eng.close()
