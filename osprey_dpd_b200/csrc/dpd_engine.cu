@@ -22,6 +22,7 @@
 #include "dpd_kernels.cuh"
 #include "pair_forces.cuh"
 #include "pair_staged.cuh"
+#include "pair_cells.cuh"
 #include "slice_stress.cuh"
 #include "monitor.cuh"
 #include "upload.cuh"
@@ -411,6 +412,10 @@ struct Timed {
 template <typename real>
 auto pair_kernel(bool multi, bool sample, int scheme)
 {
+    if constexpr (sizeof(real) == 4) {
+        if (scheme == DPD_PAIR_CELLS && !multi) return sample ? k_pair_forces_cells<true> : k_pair_forces_cells<false>;
+    }
+    if (scheme == DPD_PAIR_CELLS) scheme = DPD_PAIR_HALF_SHELL;   // FP64 and batches: the half-shell kernels
     if (scheme == DPD_PAIR_STAGED)
         return multi ? (sample ? k_pair_forces_staged<real, true, true> : k_pair_forces_staged<real, false, true>)
                      : (sample ? k_pair_forces_staged<real, true, false> : k_pair_forces_staged<real, false, false>);
@@ -426,7 +431,9 @@ template <typename real>
 size_t pair_dyn_bytes(const dpd_engine* e, bool multi)
 {
     if (e->pair_scheme == DPD_PAIR_STAGED) return StgLayout<real>(e->ntypes, e->pair_hitcap, multi).total;
-    if (e->pair_scheme == DPD_PAIR_HALF_SHELL) return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+    if (e->pair_scheme == DPD_PAIR_CELLS && sizeof(real) == 4 && !multi) return cells_smem_bytes(e->ntypes, kPairWarps);
+    if (e->pair_scheme == DPD_PAIR_HALF_SHELL || e->pair_scheme == DPD_PAIR_CELLS)
+        return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
     return pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
 }
 
@@ -581,11 +588,13 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
-        const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
+        const bool cells = e->pair_scheme == DPD_PAIR_CELLS && sizeof(real) == 4 && !multi;   // one tile per block
+        const int tpb = (e->pair_bps > 0 && !cells) ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
         CU(launch_step(e, kern, blocks_for(tiles, tpb), kPairBlock, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
-                       (real*)e->d_F, (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status));
+                       (real*)e->d_F, (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status,
+                       (const double*)e->d_x[b]));
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
     if (slices) {
@@ -646,7 +655,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "bps") e->pair_bps = std::max(val, 0);
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
-            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
+            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_CELLS) e->pair_scheme = val;
             else if (key == "ahead") e->ahead_enabled = val != 0;
             else if (key == "pdl") e->pdl = val != 0;
         }
@@ -864,7 +873,8 @@ int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persisten
 int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
 {
     if (!e) return DPD_E_ARG;
-    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED)
+    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED &&
+        scheme != DPD_PAIR_CELLS)
         return fail(e, DPD_E_ARG, "unknown pair scheme");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));

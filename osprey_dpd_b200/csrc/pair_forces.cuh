@@ -38,13 +38,49 @@ constexpr float kPruneR2 = 1.0f + 1e-5f;
 
 template <typename real> struct RealOps;
 template <> struct RealOps<float> {
-    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+    // The hardware reciprocal square root, refined by one Newton-Raphson step
+    // for 1/sqrt(x), y' = y (3 - x y^2) / 2: the approximation's error (about
+    // 2^-22 relative) otherwise reaches 1e-5 of the force RMS in the largest
+    // boxes through w = 1 - r at the cut-off.  x = 0 gives NaN, which the
+    // callers mask (coincident beads, r^2 <= 1e-18).
+    static __device__ __forceinline__ float rsqrt(float x)
+    {
+        const float y = rsqrtf(x);
+        return y * (1.5f - (0.5f * x) * (y * y));
+    }
     static __device__ __forceinline__ float rnd(float x) { return rintf(x); }
 };
 template <> struct RealOps<double> {
     static __device__ __forceinline__ double rsqrt(double x) { return 1.0 / sqrt(x); }
     static __device__ __forceinline__ double rnd(double x) { return rint(x); }
 };
+
+// Pairs closer than 0.1 take their separation from the FP64 positions
+// (slot order, three planes of n; minimum image in a box of lengths L): the
+// FP32 cell-relative shadows carry ~6e-8 absolute error, which for beads a
+// few 1e-3 apart (random initial states of millions of beads) turns the pair
+// direction by ~1e-5.  Rare, so the branch costs little.  FP64 shadows are
+// exact already.
+constexpr float kCloseR2 = 0.01f;
+__device__ __forceinline__ void refine_close(double&, double&, double&, double&, const double*, int, int, int,
+                                             const double*)
+{
+}
+__device__ __forceinline__ void refine_close(float& dx, float& dy, float& dz, float& r2, const double* __restrict__ xs,
+                                             int n, int i, int j, const double* L)
+{
+    if (r2 < kCloseR2 && xs) {
+        float d[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            double e = xs[(size_t)q * n + i] - xs[(size_t)q * n + j];
+            e = e > 0.5 * L[q] ? e - L[q] : (e < -0.5 * L[q] ? e + L[q] : e);
+            d[q] = (float)e;
+        }
+        dx = d[0]; dy = d[1]; dz = d[2];
+        r2 = dx * dx + dy * dy + dz * dz;
+    }
+}
 
 // Dynamic shared memory of one block: pair tables, then the hit lists
 // (entry k of thread t at lists[k * kPairBlock + t], so a warp's stores and
@@ -75,7 +111,8 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
                                                 const typename Vec4<real>::type& vi, const real* __restrict__ T,
                                                 int nt, real wx, real wy, real wz, const uint32_t* keys,
                                                 const typename Vec4<real>::type* __restrict__ pos4,
-                                                const typename Vec4<real>::type* __restrict__ vel4, real* acc)
+                                                const typename Vec4<real>::type* __restrict__ vel4, real* acc,
+                                                const double* __restrict__ xs, int n, int i, const double* L)
 {
     typedef typename Vec4<real>::type V4;
     const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -88,10 +125,11 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
             const int j = (int)(e & 0x03FFFFFFu);
             const V4 pj = pos4[j];
             const V4 vj = vel4[j];
-            const real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
-            const real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
-            const real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-            const real r2 = dx * dx + dy * dy + dz * dz;
+            real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
+            real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
+            real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
+            real r2 = dx * dx + dy * dy + dz * dz;
+            refine_close(dx, dy, dz, r2, xs, n, i, j, L);
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -154,7 +192,7 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
-    unsigned* __restrict__ status)
+    unsigned* __restrict__ status, const double* __restrict__ xs)
 {
     pdl_wait();
     pdl_launch();
@@ -221,7 +259,8 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
             for (int base = 0; base < trip; base += hitcap) {
                 const int clen = min(max(len - base, 0), hitcap);
                 if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
-                    pair_force_pass<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc);
+                    pair_force_pass<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, xs, n,
+                                                  i, B.L);
                     cnt = 0;
                 }
                 const int tend = base + min(trip - base, hitcap);
@@ -259,7 +298,7 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
             }
         }
     }
-    pair_force_pass<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc);
+    pair_force_pass<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, xs, n, i, B.L);
     if (live) {
         F[i] = acc[0];
         F[n + i] = acc[1];
@@ -314,7 +353,7 @@ __device__ __forceinline__ void balanced_force_pass(
     const typename Vec4<real>::type* stg, int tile_base, const Box* __restrict__ boxes, const real* Tsh,
     const real* __restrict__ tab, int nt, const uint32_t* keys0, const real* w0, int64_t step,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
-    real* __restrict__ F, real* __restrict__ stress, int n)
+    real* __restrict__ F, real* __restrict__ stress, int n, const double* __restrict__ xs)
 {
     typedef typename Vec4<real>::type V4;
     const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
@@ -353,6 +392,7 @@ __device__ __forceinline__ void balanced_force_pass(
             for (int q = 0; q < 10; ++q) keys[q] = keys0[q];
         }
         int cur_box = -1;
+        const double* Lb = boxes[0].L;   // the owner's box lengths (MULTI: reloaded with the box)
         auto load_owner = [&](int oo) {
             const int to = wbase + oo;
             pi = sh.hpos[to];
@@ -367,6 +407,7 @@ __device__ __forceinline__ void balanced_force_pass(
                 cur_box = flag_box(real_bits(pi.w));
                 const Box& B = boxes[cur_box];
                 wx = (real)B.w[0]; wy = (real)B.w[1]; wz = (real)B.w[2];
+                Lb = B.L;
                 if (STAGED) iw = real(1) / wx;
                 T = tab + B.tab;
                 uint32_t k = philox_step_key(B.seed, step);
@@ -419,7 +460,8 @@ __device__ __forceinline__ void balanced_force_pass(
                 dz = (pi.z - pj.z) - (real)((int)(ent >> 30) - 1) * wz;
             }
             const V4 vj = vel4[j];
-            const real r2 = dx * dx + dy * dy + dz * dz;
+            real r2 = dx * dx + dy * dy + dz * dz;
+            refine_close(dx, dy, dz, r2, xs, n, islot, j, Lb);
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -434,10 +476,10 @@ __device__ __forceinline__ void balanced_force_pass(
             }
             const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
                              T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-            // the staged test decides pairs at the cut-off from rounded
-            // window coordinates: re-apply the exact cut-off here; the
-            // unstaged test leaves coincident beads (r2 <= 1e-18) to this pass
-            const real m = ((STAGED ? r2 < real(1) : true) && r2 > real(1e-18)) ? mag * inv : real(0);
+            // the staged tests decide pairs at the cut-off from rounded
+            // window coordinates: the exact cut-off is applied here, and
+            // coincident beads (r2 <= 1e-18) are left to this pass
+            const real m = (r2 < real(1) && r2 > real(1e-18)) ? mag * inv : real(0);
             const real gx = m * dx, gy = m * dy, gz = m * dz;
             acc[0] += gx; acc[1] += gy; acc[2] += gz;
             atomicAdd(F + j, -gx);
@@ -469,7 +511,8 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
                                                      int nt, real wx, real wy, real wz, const uint32_t* keys,
                                                      const typename Vec4<real>::type* __restrict__ pos4,
                                                      const typename Vec4<real>::type* __restrict__ vel4, real* acc,
-                                                     real* __restrict__ F, int n)
+                                                     real* __restrict__ F, int n, const double* __restrict__ xs,
+                                                     int i, const double* L)
 {
     typedef typename Vec4<real>::type V4;
     const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
@@ -482,10 +525,11 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
             const int j = (int)(e & 0x03FFFFFFu);
             const V4 pj = pos4[j];
             const V4 vj = vel4[j];
-            const real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
-            const real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
-            const real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-            const real r2 = dx * dx + dy * dy + dz * dz;
+            real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
+            real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
+            real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
+            real r2 = dx * dx + dy * dy + dz * dz;
+            refine_close(dx, dy, dz, r2, xs, n, i, j, L);
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -525,7 +569,7 @@ __device__ __forceinline__ void half_shell_tile_lanes(
     int tile, int n, int nt, const Box* __restrict__ boxes, int64_t step, const real* __restrict__ tab,
     const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
-    real* __restrict__ F, real* __restrict__ stress, int hitcap, uint32_t* lists)
+    real* __restrict__ F, real* __restrict__ stress, int hitcap, uint32_t* lists, const double* __restrict__ xs)
 {
     typedef typename Vec4<real>::type V4;
     uint32_t* list = lists + threadIdx.x;
@@ -608,7 +652,7 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                     const int clen = min(max(len - base, 0), hitcap);
                     if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
                         pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4,
-                                                           acc, F, n);
+                                                           acc, F, n, xs, i, B.L);
                         cnt = 0;
                     }
                     const int tend = base + min(trip - base, hitcap);
@@ -648,7 +692,8 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                 }
             }
         }
-        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n);
+        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n, xs, i,
+                                           B.L);
         if (live) {
             atomicAdd(F + i, acc[0]);
             atomicAdd(F + n + i, acc[1]);
@@ -706,7 +751,7 @@ __device__ __forceinline__ void half_shell_tile(
     const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, uint32_t* lists, const HalfShared<real>& sh,
-    const uint32_t* keys0)
+    const uint32_t* keys0, const double* __restrict__ xs)
 {
     typedef typename Vec4<real>::type V4;
     uint32_t* list = lists + threadIdx.x;
@@ -789,7 +834,7 @@ __device__ __forceinline__ void half_shell_tile(
                 if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
                     balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh,
                                                                     tab, nt, keys0, w0, step, pos4, vel4, F, stress,
-                                                                    n);
+                                                                    n, xs);
                     cnt = 0;
                 }
                 const int tend = base + min(trip - base, hitcap);
@@ -837,7 +882,7 @@ __device__ __forceinline__ void half_shell_tile(
         }
     }
     balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh, tab, nt, keys0,
-                                                    w0, step, pos4, vel4, F, stress, n);
+                                                    w0, step, pos4, vel4, F, stress, n, xs);
 }
 
 // Which force pass a k_pair_forces_half instantiation uses: the balanced pass
@@ -853,7 +898,7 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
-    unsigned* __restrict__ status)
+    unsigned* __restrict__ status, const double* __restrict__ xs)
 {
     pdl_wait();
     pdl_launch();
@@ -878,10 +923,10 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
         if (tile * kPairBlock >= n) break;
         if (kHalfBalanced<real, MULTI>)
             half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
-                                                 stress, hitcap, lists, sh, keys0);
+                                                 stress, hitcap, lists, sh, keys0, xs);
         else
             half_shell_tile_lanes<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
-                                                       F, stress, hitcap, lists);
+                                                       F, stress, hitcap, lists, xs);
     }
 }
 

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
     real* __restrict__ F, real* __restrict__ stress, int hitcap, int tiles_per_block,
-    unsigned* __restrict__ status)
+    unsigned* __restrict__ status, const double* __restrict__ xs)
 {
     pdl_wait();
     pdl_launch();
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
         }
         if (H > kStgRows) {   // block-uniform
             half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
-                                                 stress, hitcap, lists, sh, keys0);
+                                                 stress, hitcap, lists, sh, keys0, xs);
             continue;
         }
         const int h = before + __popc(fb & ((2u << lane) - 1u)) - 1;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
         const int S = (int)(all >> 32), NT = (int)(all & 0xFFFFFFFFll);
         if (S > cap || NT > kStgCells) {   // block-uniform
             half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
-                                                 stress, hitcap, lists, sh, keys0);
+                                                 stress, hitcap, lists, sh, keys0, xs);
             continue;
         }
         if (t < 5 * H) {
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
                 if (__any_sync(0xffffffffu, cnt > hitcap - 2)) {
                     balanced_force_pass<real, VIRIAL, MULTI, true>(cnt, lists, sh, stg, tile * kPairBlock, boxes,
                                                                    Tsh, tab, nt, keys0, w0, step, pos4, vel4, F,
-                                                                   stress, n);
+                                                                   stress, n, xs);
                     cnt = 0;
                 }
                 const bool v0 = u < len, v1 = u + 1 < len;
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
             }
         }
         balanced_force_pass<real, VIRIAL, MULTI, true>(cnt, lists, sh, stg, tile * kPairBlock, boxes, Tsh, tab, nt,
-                                                       keys0, w0, step, pos4, vel4, F, stress, n);
+                                                       keys0, w0, step, pos4, vel4, F, stress, n, xs);
     }
 }
 
