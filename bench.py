@@ -219,13 +219,13 @@ def tune_candidates(reproducible: bool):
     if reproducible:
         return autotune.DEFAULT_CANDIDATES
     return (autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES + autotune.STAGED_CANDIDATES +
-            autotune.CELLS_CANDIDATES)
+            autotune.FRAME_CANDIDATES)
 
 
-FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1), "staged": (16, 0, 100, 2), "cells": (32, 0, -1, 3)}
-SCHEME_NAMES = {0: "full", 1: "half", 2: "staged", 3: "cells"}
+FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1), "staged": (16, 0, 100, 2), "frame": (32, 0, -1, 3)}
+SCHEME_NAMES = {0: "full", 1: "half", 2: "staged", 3: "frame"}
 PAIR_KERNELS = {"full": "k_pair_forces", "half": "k_pair_forces_half", "staged": "k_pair_forces_staged",
-                "cells": "k_pair_forces_cells"}
+                "frame": "k_pair_forces_frame"}
 
 
 def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False,
@@ -250,11 +250,11 @@ def scheme_of(shape) -> str:
 def pair_scheme_name(shape) -> str:
     return {"full": "full shell (reproducible)", "half": "half shell (atomics)",
             "staged": "half shell staged in shared memory (atomics)",
-            "cells": "half shell, lanes over one home cell's candidates (atomics)"}[scheme_of(shape)]
+            "frame": "half shell, candidates tested on an absolute-x frame shadow (atomics)"}[scheme_of(shape)]
 
 
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
-                shape=None, profile_steps: int = 20):
+                shape=None, profile_steps: int = 20, flush: bool = True):
     """Per-step device time (ms) of single-step calls with L2 flushed before
     each step; then, when asked, a separate pass with CUDA events around every
     kernel (launched one by one) for the per-kernel durations."""
@@ -265,13 +265,15 @@ def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev
     eng.set_sample_period(SAMPLE_PERIOD)
     stream = torch.cuda.Stream(device=dev)
     eng.set_stream(stream.cuda_stream)
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    clean = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    flush_buf = torch.empty(L2_FLUSH_BYTES if flush else 1, dtype=torch.uint8, device=dev)
+    clean = torch.ones(L2_FLUSH_BYTES // 4 if flush else 1, dtype=torch.float32, device=dev)
 
     def flush_l2():
         # evict the state by writing a buffer larger than L2, then read a second
         # one so the dirty lines of the first are written back before the step
-        flush.zero_()
+        if not flush:
+            return None
+        flush_buf.zero_()
         return clean.sum()
 
     t = 1
@@ -430,6 +432,36 @@ def run_replica_sweep(args, dev, torch, E):
     }
 
 
+def time_melt(engine_mod, dev, torch, warmup: int, steps: int = 20):
+    """The 6,291,456-bead polymer solution (north_star's >= 1.5e9 bead-steps/s
+    target), mixed precision, the half-shell scheme: per-step CUDA-event times
+    of single-step calls; its state (~1.3 GB) exceeds L2, so no flush."""
+    system, desc = workload("polymer")
+    ms, prof, launches, status = time_engine(engine_mod, system, engine_mod.MIXED, steps, warmup, dev, torch, False,
+                                             list(FIXED_SHAPES["half"]), flush=False)
+    total = sum(ms)
+    return {"workload": desc, "n_beads": system.n, "value": system.n * steps / (total / 1000.0),
+            "unit": UNIT, "ms_per_step": total / steps, "steps": steps, "warmup": warmup, "target": 1.5e9,
+            "precision": "mixed", "pair_scheme": pair_scheme_name(FIXED_SHAPES["half"]),
+            "l2": "state (~1.3 GB) larger than L2", "gpu_launches": launches, "status_bits": status}
+
+
+def time_sweep(engine_mod, dev, torch, nrep: int = 512, graph_steps: int = 100):
+    """The 512-replica A/B sweep (north_star's >= 3x over replicas one at a
+    time): one batch of all replicas as captured 100-step graphs against the
+    same replicas stepped engine by engine, one 100-step call each."""
+    ns = argparse.Namespace(replicas=nrep, graph_steps=graph_steps, steps=1, warmup=1, pair_scheme="half",
+                            no_autotune=True, reproducible=False)
+    r = run_replica_sweep(ns, dev, torch, engine_mod)
+    return {"workload": r["config"]["workload"], "value": r["value"], "unit": UNIT,
+            "ms_per_step": r["ms_per_step"], "one_at_a_time": r["one_at_a_time"],
+            "batch_over_one_at_a_time": r["batch_over_one_at_a_time"], "target_ratio": 3.0,
+            "launch": "one packed box table (all replicas) per kernel launch, each 100-step call a captured CUDA "
+                      "graph; not a persistent kernel: persistent grids of 2-8 blocks per SM measured slower "
+                      "(+10 % to +190 %) than one tile per block on this engine",
+            "gpu_launches": r["gpu_launches"], "status_bits": r["status_bits"]}
+
+
 def time_slice_profile(engine_mod, system, nslices: int, shape, dev, torch, steps: int = 20):
     """Cost of the slice stress profile (CMonitor::AddBeadStress & co.) on a
     sample step: per-kernel CUDA events over ``steps`` steps that all sample,
@@ -514,11 +546,13 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
     ap.add_argument("--reproducible", action="store_true",
                     help="tune over the full-shell (bitwise reproducible) pair scheme only")
-    ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged", "cells"], default="auto",
+    ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged", "frame"], default="auto",
                     help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     ap.add_argument("--monitor", action="store_true",
                     help="also time dpd_engine_monitor against the state download it replaces")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the 6.3M-bead melt and the 512-replica sweep keys of the default line")
     ap.add_argument("--slices", type=int, default=0,
                     help="also time the slice stress profile over this many z slices on sample steps")
     args = ap.parse_args()
@@ -642,6 +676,9 @@ def main():
     if sm_seen:
         line["roofline"]["frac_at_observed_clock"] = achieved / (sms * 128 * float(sm_seen) * 1e6)
         line["roofline"]["observed_sm_mhz"] = float(sm_seen)
+    if not args.no_extra and args.workload == "bilayer" and ws == 1:
+        line["melt"] = time_melt(E, dev, torch, args.warmup)
+        line["replica_sweep"] = time_sweep(E, dev, torch)
     if args.slices > 0:
         line["slice_profile"] = time_slice_profile(E, system, args.slices, mixed["shape"], dev, torch)
     if args.monitor:

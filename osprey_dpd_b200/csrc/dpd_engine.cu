@@ -22,7 +22,7 @@
 #include "dpd_kernels.cuh"
 #include "pair_forces.cuh"
 #include "pair_staged.cuh"
-#include "pair_cells.cuh"
+#include "pair_frame.cuh"
 #include "slice_stress.cuh"
 #include "monitor.cuh"
 #include "upload.cuh"
@@ -104,6 +104,7 @@ struct dpd_engine {
     void* d_stress = nullptr;   // per-bead virial of the last sample step (real, 9 planes)
     void* d_pos4 = nullptr;
     void* d_vel4 = nullptr;
+    float4* d_tst4 = nullptr;   // frame shadow (single-box FP32 engines), n + kFramePad entries
     int* d_rank = nullptr;
     int* d_perm = nullptr;
     int* d_pid[2] = {nullptr, nullptr};   // noise id (reference bead id) in slot order
@@ -304,6 +305,7 @@ int push_constants(dpd_engine* e)
     }
     K.ntypes = e->ntypes;
     K.seed = b0.seed;
+    K.tst4 = e->pair_scheme == DPD_PAIR_FRAME ? e->d_tst4 : nullptr;
     const int m = e->ntypes * e->ntypes;
     const size_t nb = e->hboxes.size();
     std::vector<double> tab(3 * (size_t)m * nb);
@@ -413,9 +415,9 @@ template <typename real>
 auto pair_kernel(bool multi, bool sample, int scheme)
 {
     if constexpr (sizeof(real) == 4) {
-        if (scheme == DPD_PAIR_CELLS && !multi) return sample ? k_pair_forces_cells<true> : k_pair_forces_cells<false>;
+        if (scheme == DPD_PAIR_FRAME && !multi) return sample ? k_pair_forces_frame<true> : k_pair_forces_frame<false>;
     }
-    if (scheme == DPD_PAIR_CELLS) scheme = DPD_PAIR_HALF_SHELL;   // FP64 and batches: the half-shell kernels
+    if (scheme == DPD_PAIR_FRAME) scheme = DPD_PAIR_HALF_SHELL;   // FP64 and batches: the half-shell kernels
     if (scheme == DPD_PAIR_STAGED)
         return multi ? (sample ? k_pair_forces_staged<real, true, true> : k_pair_forces_staged<real, false, true>)
                      : (sample ? k_pair_forces_staged<real, true, false> : k_pair_forces_staged<real, false, false>);
@@ -431,8 +433,7 @@ template <typename real>
 size_t pair_dyn_bytes(const dpd_engine* e, bool multi)
 {
     if (e->pair_scheme == DPD_PAIR_STAGED) return StgLayout<real>(e->ntypes, e->pair_hitcap, multi).total;
-    if (e->pair_scheme == DPD_PAIR_CELLS && sizeof(real) == 4 && !multi) return cells_smem_bytes(e->ntypes, kPairWarps);
-    if (e->pair_scheme == DPD_PAIR_HALF_SHELL || e->pair_scheme == DPD_PAIR_CELLS)
+    if (e->pair_scheme == DPD_PAIR_HALF_SHELL || e->pair_scheme == DPD_PAIR_FRAME)
         return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
     return pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
 }
@@ -588,8 +589,8 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
-        const bool cells = e->pair_scheme == DPD_PAIR_CELLS && sizeof(real) == 4 && !multi;   // one tile per block
-        const int tpb = (e->pair_bps > 0 && !cells) ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
+        const bool frame = e->pair_scheme == DPD_PAIR_FRAME && sizeof(real) == 4 && !multi;   // one tile per block
+        const int tpb = (e->pair_bps > 0 && !frame) ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
         CU(launch_step(e, kern, blocks_for(tiles, tpb), kPairBlock, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
@@ -655,7 +656,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "bps") e->pair_bps = std::max(val, 0);
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
-            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_CELLS) e->pair_scheme = val;
+            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_FRAME) e->pair_scheme = val;
             else if (key == "ahead") e->ahead_enabled = val != 0;
             else if (key == "pdl") e->pdl = val != 0;
         }
@@ -874,14 +875,14 @@ int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
 {
     if (!e) return DPD_E_ARG;
     if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED &&
-        scheme != DPD_PAIR_CELLS)
+        scheme != DPD_PAIR_FRAME)
         return fail(e, DPD_E_ARG, "unknown pair scheme");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
     e->pair_scheme = scheme;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
-    return DPD_OK;
+    return push_constants(e);   // the frame shadow is written only under DPD_PAIR_FRAME
 }
 
 int dpd_engine_set_sample_period(dpd_engine* e, int64_t period)
@@ -1045,7 +1046,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
                          (void**)&e->d_perm, (void**)&e->d_pid[0], (void**)&e->d_pid[1], (void**)&e->d_pid_of,
                          (void**)&e->d_partials,
                          (void**)&e->d_out, (void**)&e->d_out_cell, (void**)&e->d_xa, (void**)&e->d_imga,
-                         (void**)&e->d_cella};
+                         (void**)&e->d_cella, (void**)&e->d_tst4};
         for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
         const size_t rs = real_size(e);
         int rc;
@@ -1072,7 +1073,15 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(n, kThreads) * kObsTerms))) return rc;
         if ((rc = dalloc(e, &e->d_out, 21 * (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
+        if (e->precision == DPD_PRECISION_MIXED && e->hboxes.size() == 1) {
+            // frame shadow with far-away padding past the last bead (its test
+            // loop reads there without a per-candidate clamp)
+            if ((rc = dalloc(e, &e->d_tst4, (size_t)n + kFramePad))) return rc;
+            std::vector<float4> pad(kFramePad, make_float4(1e30f, 1e30f, 1e30f, 0.f));
+            CU(cudaMemcpy(e->d_tst4 + n, pad.data(), sizeof(float4) * kFramePad, cudaMemcpyHostToDevice));
+        }
         e->n = n;
+        if ((rc = push_constants(e))) return rc;   // the frame shadow's address
     }
     // cell starts, then the slot order: by cell, inside a cell by upload index
     k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start);

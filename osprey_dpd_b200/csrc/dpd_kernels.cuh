@@ -64,6 +64,10 @@ struct StepConst {
     int nc[3];
     int ntypes;
     uint64_t seed;
+    // frame shadow of the DPD_PAIR_FRAME scheme (FP32 absolute x, cell-relative
+    // y and z per slot, padded past the last bead), written by k_gather; NULL
+    // when that scheme is not in use
+    float4* tst4;
 };
 
 // One simulation box (CCNTCell::SetSimBoxLengths, CNTCell.cpp:143-158).  An
@@ -368,6 +372,7 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid, real(0));
     pos4[o] = p;
     vel4[o] = w;
+    if (K->tst4) K->tst4[o] = make_float4((float)xs[0], (float)rel[1], (float)rel[2], 0.f);
     if (flag_bonded(tfl)) {
         // unPBC position (x + image*L + upload offset) for the bonded terms,
         // stored by upload index: chain partners sit in the same lines

@@ -52,7 +52,7 @@ def run(program, name, env=None, timeout=1800):
 
 
 def main():
-    for name in RUNS:
+    for name in (sys.argv[1:] or RUNS):
         hist, log, dt = run(REF_MAIN, name)
         np.savez_compressed(os.path.join(HERE, f"glue_{name}.npz"), history=hist, seconds=dt)
         print(name, hist.shape, f"{dt:.1f} s")

@@ -72,7 +72,7 @@ def test_binding_runs_the_water_control_file():
 
 @pytest.mark.gpu
 def test_binding_runs_the_bilayer_control_file_with_a_time_step_change():
-    _compare("bilayer", 2000)
+    _compare("bilayer", 10000)
 
 
 @pytest.mark.gpu

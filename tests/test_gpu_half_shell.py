@@ -1,6 +1,6 @@
 """The half-shell pair schemes (each pair evaluated once, the partner's share
-added with atomics; unstaged, staged per tile in shared memory, and with the
-lanes over one home cell's candidates) against the CPU
+added with atomics; unstaged, staged per tile in shared memory, and tested
+on the absolute-x frame shadow) against the CPU
 oracle.  Its force sums are rounded in
 a run-dependent order, so the bounds are the tolerances of the full-shell
 tests rather than bit equality:
@@ -26,7 +26,7 @@ SYSTEMS = {
 }
 
 
-SCHEMES = pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "cells"])
+SCHEMES = pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "frame"])
 
 
 def _half(engine_mod, oracle_mod, s, precision, scheme=1, **kw):
@@ -150,7 +150,7 @@ def test_switching_schemes_between_calls(engine_mod):
         b.set_pair_scheme(7)
 
 
-@pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "cells"])
+@pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "frame"])
 @pytest.mark.parametrize("workload", ["bilayer", "polymer"])
 def test_half_shell_matches_full_shell_at_full_size(engine_mod, workload, scheme):
     """The half-shell schemes against the full-shell kernel on the full-size
