@@ -599,10 +599,11 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
     }
     if ((rc = check_launch(e, "k_pair_forces"))) return rc;
     if (slices) {
-        const size_t smem = (size_t)e->slice_S * e->ntypes * e->ntypes * 9 * sizeof(double);
-        const int sb = smem <= kSliceSmemMax;
+        const int KT = e->ntypes * e->ntypes;
+        const int sb = slice_smem_bytes<real>(e->slice_S, KT, true) <= kSliceSmemMax;
+        const size_t smem = slice_smem_bytes<real>(e->slice_S, KT, sb != 0);
         Timed t(e, DPD_KERNEL_SLICES);
-        CU(launch_step(e, k_slice_pairs<real>, e->sms * 2, 256, sb ? smem : 0, st, n, e->d_K, e->d_boxes, e->d_step,
+        CU(launch_step(e, k_slice_pairs<real>, e->sms * 4, kSliceBlock, smem, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
                        (const double*)e->d_x[b], sp, sb));
         if ((rc = check_launch(e, "k_slice_pairs"))) return rc;
@@ -1449,11 +1450,12 @@ int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t nbondtyp
         CU(cudaMemcpy(e->d_slice_bpt, bondpair_type, sizeof(int) * e->topo_na, cudaMemcpyHostToDevice));
     }
     CU(cudaMemset(e->d_slice, 0, slice_bins(e) * sizeof(double)));
-    const size_t smem = (size_t)nslices * e->ntypes * e->ntypes * 9 * sizeof(double);
-    if (smem <= kSliceSmemMax) {
-        CU(cudaFuncSetAttribute(k_slice_pairs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CU(cudaFuncSetAttribute(k_slice_pairs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
+    // dynamic shared memory of the pair part: bins (when they fit) and hit lists
+    const int KT = e->ntypes * e->ntypes;
+    const size_t sf = slice_smem_bytes<float>(nslices, KT, slice_smem_bytes<float>(nslices, KT, true) <= kSliceSmemMax);
+    const size_t sd = slice_smem_bytes<double>(nslices, KT, slice_smem_bytes<double>(nslices, KT, true) <= kSliceSmemMax);
+    CU(cudaFuncSetAttribute(k_slice_pairs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf));
+    CU(cudaFuncSetAttribute(k_slice_pairs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sd));
     return DPD_OK;
 }
 

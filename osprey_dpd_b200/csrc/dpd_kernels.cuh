@@ -525,19 +525,24 @@ __device__ __forceinline__ void outer9(const double f[3], const double d[3], dou
     o[6] = f[2] * d[0]; o[7] = f[2] * d[1]; o[8] = f[2] * d[2];
 }
 
-__device__ __forceinline__ void slice_put(double* arr, int K, int idx, int sl, const double fdx[9], double fac,
+// Bins in FP64 (global, or block-private in an FP64 engine) or FP32
+// (block-private partial sums of a mixed-precision engine, added to the FP64
+// bins once per block).
+template <typename bin_t>
+__device__ __forceinline__ void slice_put(bin_t* arr, int K, int idx, int sl, const double fdx[9], double fac,
                                           bool scale)
 {
-    double* q = arr + ((size_t)sl * K + idx) * 9;
+    bin_t* q = arr + ((size_t)sl * K + idx) * 9;
 #pragma unroll
-    for (int c = 0; c < 9; ++c) atomicAdd(q + c, scale ? fdx[c] * fac : fdx[c]);
+    for (int c = 0; c < 9; ++c) atomicAdd(q + c, (bin_t)(scale ? fdx[c] * fac : fdx[c]));
 }
 
 // One contribution over the slices between two beads: za is the z of the
 // bead the separation points to (bead 1, bond head, bead j+1), zb the
 // other's, zDiff the separation's z component.  Same branch structure and
 // arithmetic as the reference's three functions.
-__device__ __forceinline__ void slice_add(const SliceParams& sp, double* arr, int K, int idx, const double fdx[9],
+template <typename bin_t>
+__device__ __forceinline__ void slice_add(const SliceParams& sp, bin_t* arr, int K, int idx, const double fdx[9],
                                           double zDiff, double za, double zb)
 {
     double up, lo;

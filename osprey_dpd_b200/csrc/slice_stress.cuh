@@ -23,13 +23,84 @@
 
 namespace dpd {
 
-// Pair part on a sample step: one thread per bead i over its own cell (beads
-// after i) and the 13 cells of the reference's half shell, the DPD pair force
-// of the force kernels (same Philox draw), accumulated into block-private
-// bins in shared memory when they fit (sbins), else straight into global.
-// Grid-stride loop; the bins are flushed once per block.
+// Pair part on a sample step, in two phases per 128-bead tile (one lane per
+// bead i).  Test: the lane walks its own cell (beads after i) and the 13 cells
+// of the reference's half shell, one cell at a time (a constant cell shift),
+// and lists the candidates inside the cut-off in its column of shared memory.
+// Evaluate: the lane takes its listed pairs, computes the DPD pair force of the
+// force kernels (same Philox draw) and splits force x separation over the
+// slices (slice_add).  Only listed pairs pay for the force and the split, so
+// no lane idles through another's force work on the ~85 % of candidates that
+// miss.  Bins are block-private in shared memory when they fit (sbins) --
+// FP32 partial sums in a mixed-precision engine, FP64 in an FP64 engine --
+// and added once per block to the FP64 profile; else they go straight to
+// global memory.  Grid-stride loop over the tiles.
+constexpr int kSliceBlock = 128;
+constexpr int kSliceHits = 32;   // list entries per lane before an evaluation pass
+
 template <typename real>
-__global__ void __launch_bounds__(256) k_slice_pairs(
+__host__ __device__ constexpr size_t slice_bin_bytes(int S, int KT)
+{
+    return ((sizeof(real) * (size_t)S * KT * 9 + 15) / 16) * 16;
+}
+template <typename real>
+__host__ __device__ constexpr size_t slice_smem_bytes(int S, int KT, bool sbins)
+{
+    return (sbins ? slice_bin_bytes<real>(S, KT) : 0) + sizeof(uint32_t) * (kSliceHits + 1) * kSliceBlock;
+}
+
+// The listed pairs of one lane: force, then its slices.  bins: the block's
+// shared bins (real) or the global FP64 profile.
+template <typename real, typename bin_t>
+__device__ __forceinline__ void slice_eval(int cnt, const uint32_t* __restrict__ list, int i, int n,
+                                           const typename Vec4<real>::type& pi, const typename Vec4<real>::type& vi,
+                                           double zi, const real* __restrict__ tab, int nt, const uint32_t* keys,
+                                           real wx, real wy, real wz, const typename Vec4<real>::type* __restrict__ pos4,
+                                           const typename Vec4<real>::type* __restrict__ vel4,
+                                           const double* __restrict__ x, const SliceParams& sp, bin_t* bins,
+                                           const double* L)
+{
+    typedef typename Vec4<real>::type V4;
+    const int m2 = nt * nt, KT = nt * nt;
+    const int ti = real_bits(pi.w) & 0xFF;
+    const uint32_t idi = (uint32_t)real_bits(vi.w);
+    for (int k = 0; k < cnt; ++k) {
+        const uint32_t e = list[k * kSliceBlock];
+        const int j = (int)(e & 0x03FFFFFFu);
+        const V4 pj = pos4[j];
+        const V4 vj = vel4[j];
+        real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
+        real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
+        real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
+        real r2 = dx * dx + dy * dy + dz * dz;
+        refine_close(dx, dy, dz, r2, x, n, i, j, L);
+        if (!(r2 < real(1) && r2 > real(1e-18))) continue;   // the test's rounding differs at the cut-off
+        const real inv = RealOps<real>::rsqrt(r2);
+        const real wr = real(1) - r2 * inv;
+        const int tj = real_bits(pj.w) & 0xFF;
+        const int tt = ti * nt + tj;
+        const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
+        const uint32_t idj = (uint32_t)real_bits(vj.w);
+        uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) {
+            const uint64_t prod = (uint64_t)0xD256D193u * c0;
+            c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
+            c1 = (uint32_t)prod;
+        }
+        const real mag = tab[tt] * wr - tab[m2 + tt] * wr * wr * rdotv +
+                         tab[2 * m2 + tt] * wr * noise_centered(c0, real(0));
+        const real m = mag * inv;
+        const double f[3] = {(double)(m * dx), (double)(m * dy), (double)(m * dz)};
+        const double d[3] = {(double)dx, (double)dy, (double)dz};
+        double fdx[9];
+        outer9(f, d, fdx);
+        slice_add(sp, bins, KT, tt, fdx, d[2], zi, x[2 * (size_t)n + j]);
+    }
+}
+
+template <typename real>
+__global__ void __launch_bounds__(kSliceBlock) k_slice_pairs(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
@@ -38,12 +109,14 @@ __global__ void __launch_bounds__(256) k_slice_pairs(
     pdl_wait();
     pdl_launch();
     typedef typename Vec4<real>::type V4;
-    extern __shared__ double sbin[];
+    extern __shared__ __align__(16) unsigned char slice_dyn[];
     const int nt = K->ntypes, KT = nt * nt;
     const int nbins = sp.S * KT * 9;
-    double* bins = sbins ? sbin : sp.pair;
+    real* sbin = reinterpret_cast<real*>(slice_dyn);
+    uint32_t* lists = reinterpret_cast<uint32_t*>(slice_dyn + (sbins ? slice_bin_bytes<real>(sp.S, KT) : 0));
+    uint32_t* list = lists + threadIdx.x;
     if (sbins) {
-        for (int k = threadIdx.x; k < nbins; k += blockDim.x) sbin[k] = 0.0;
+        for (int k = threadIdx.x; k < nbins; k += blockDim.x) sbin[k] = real(0);
         __syncthreads();
     }
     const Box& B = boxes[0];
@@ -55,15 +128,27 @@ __global__ void __launch_bounds__(256) k_slice_pairs(
 #pragma unroll
         for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
     }
-    const int m2 = nt * nt;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const V4 pi = pos4[i], vi = vel4[i];
-        const int c = cell[i] - B.cell_base;
-        const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-        const int ti = real_bits(pi.w) & 0xFF;
-        const uint32_t idi = (uint32_t)real_bits(vi.w);
-        const double zi = x[2 * (size_t)n + i];
-        // o = 0: own cell after i; o = 1..13: (dx, dy, dz) of the reference's half shell
+    const int ntiles = (n + kSliceBlock - 1) / kSliceBlock;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int i = tile * kSliceBlock + threadIdx.x;
+        const bool live = i < n;
+        V4 pi, vi;
+        int cx = 0, cy = 0, cz = 0;
+        double zi = 0.0;
+        if (live) {
+            pi = pos4[i];
+            vi = vel4[i];
+            const int c = cell[i] - B.cell_base;
+            cx = c % nx;
+            cy = (c / nx) % ny;
+            cz = c / (nx * ny);
+            zi = x[2 * (size_t)n + i];
+        } else {
+            pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
+        }
+        int cnt = 0;
+        // o = 0: own cell after i; o = 1..13: (dx, dy, dz) of the reference's half
+        // shell (CSimBox::MakeCNTCells, SimBox.cpp:845-856)
         for (int o = 0; o < 14; ++o) {
             int ox = 0, oy = 0, oz = 0;
             if (o >= 1 && o <= 9) { ox = (o - 1) % 3 - 1; oy = (o - 1) / 3 - 1; oz = 1; }
@@ -74,43 +159,48 @@ __global__ void __launch_bounds__(256) k_slice_pairs(
             y2 += y2 < 0 ? ny : (y2 >= ny ? -ny : 0);
             z2 += z2 >= nz ? -nz : 0;
             const int c2 = B.cell_base + x2 + nx * (y2 + ny * z2);
-            const int jb = o == 0 ? i + 1 : start[c2], je = start[c2 + 1];
-            for (int j = jb; j < je; ++j) {
-                const V4 pj = pos4[j];
-                const real dx = (pi.x - pj.x) - (real)ox * wx;
-                const real dy = (pi.y - pj.y) - (real)oy * wy;
-                const real dz = (pi.z - pj.z) - (real)oz * wz;
-                const real r2 = dx * dx + dy * dy + dz * dz;
-                if (!(r2 < real(1) && r2 > real(1e-18))) continue;
-                const V4 vj = vel4[j];
-                const real inv = RealOps<real>::rsqrt(r2);
-                const real wr = real(1) - r2 * inv;
-                const int tj = real_bits(pj.w) & 0xFF;
-                const int tt = ti * nt + tj;
-                const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
-                const uint32_t idj = (uint32_t)real_bits(vj.w);
-                uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
-#pragma unroll
-                for (int q = 0; q < 10; ++q) {
-                    const uint64_t prod = (uint64_t)0xD256D193u * c0;
-                    c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
-                    c1 = (uint32_t)prod;
+            int jb = 0, je = 0;
+            if (live) {
+                jb = o == 0 ? i + 1 : start[c2];
+                je = start[c2 + 1];
+            }
+            const int len = max(je - jb, 0);
+            const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+            const real pxs = pi.x - (real)ox * wx, pys = pi.y - (real)oy * wy, pzs = pi.z - (real)oz * wz;
+            const uint32_t code = ((uint32_t)(ox + 1) << 26) | ((uint32_t)(oy + 1) << 28) | ((uint32_t)(oz + 1) << 30);
+            for (int base = 0; base < trip; base += kSliceHits) {
+                const int clen = min(max(len - base, 0), kSliceHits);
+                if (__any_sync(0xffffffffu, cnt + clen > kSliceHits)) {
+                    if (sbins)
+                        slice_eval<real>(cnt, list, i, n, pi, vi, zi, tab, nt, keys, wx, wy, wz, pos4, vel4, x, sp,
+                                         sbin, B.L);
+                    else
+                        slice_eval<real>(cnt, list, i, n, pi, vi, zi, tab, nt, keys, wx, wy, wz, pos4, vel4, x, sp,
+                                         sp.pair, B.L);
+                    cnt = 0;
                 }
-                const real mag = tab[tt] * wr - tab[m2 + tt] * wr * wr * rdotv +
-                                 tab[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-                const real m = mag * inv;
-                const double f[3] = {(double)(m * dx), (double)(m * dy), (double)(m * dz)};
-                const double d[3] = {(double)dx, (double)dy, (double)dz};
-                double fdx[9];
-                outer9(f, d, fdx);
-                slice_add(sp, bins, KT, tt, fdx, d[2], zi, x[2 * (size_t)n + j]);
+                const int tend = base + min(trip - base, kSliceHits);
+                for (int t = base; t < tend; ++t) {
+                    // the entry is stored always and kept by advancing cnt
+                    // (cnt + clen <= kSliceHits: at most the spare row)
+                    const int j = min(jb + t, n - 1);
+                    const V4 pj = pos4[j];
+                    const real dx = pxs - pj.x, dy = pys - pj.y, dz = pzs - pj.z;
+                    const real r2 = dx * dx + dy * dy + dz * dz;
+                    list[cnt * kSliceBlock] = (uint32_t)j | code;
+                    cnt += (t < len && r2 < real(1) && r2 > real(1e-18)) ? 1 : 0;
+                }
             }
         }
+        if (sbins)
+            slice_eval<real>(cnt, list, i, n, pi, vi, zi, tab, nt, keys, wx, wy, wz, pos4, vel4, x, sp, sbin, B.L);
+        else
+            slice_eval<real>(cnt, list, i, n, pi, vi, zi, tab, nt, keys, wx, wy, wz, pos4, vel4, x, sp, sp.pair, B.L);
     }
     if (sbins) {
         __syncthreads();
         for (int k = threadIdx.x; k < nbins; k += blockDim.x)
-            if (sbin[k] != 0.0) atomicAdd(sp.pair + k, sbin[k]);
+            if (sbin[k] != real(0)) atomicAdd(sp.pair + k, (double)sbin[k]);
     }
 }
 
