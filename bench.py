@@ -218,14 +218,12 @@ def tune_candidates(reproducible: bool):
     from osprey_dpd_b200 import autotune
     if reproducible:
         return autotune.DEFAULT_CANDIDATES
-    return (autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES + autotune.STAGED_CANDIDATES +
-            autotune.FRAME_CANDIDATES)
+    return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES + autotune.STAGED_CANDIDATES
 
 
-FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1), "staged": (16, 0, 100, 2), "frame": (32, 0, -1, 3)}
-SCHEME_NAMES = {0: "full", 1: "half", 2: "staged", 3: "frame"}
-PAIR_KERNELS = {"full": "k_pair_forces", "half": "k_pair_forces_half", "staged": "k_pair_forces_staged",
-                "frame": "k_pair_forces_frame"}
+FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1), "staged": (16, 0, 100, 2)}
+SCHEME_NAMES = {0: "full", 1: "half", 2: "staged"}
+PAIR_KERNELS = {"full": "k_pair_forces", "half": "k_pair_forces_half", "staged": "k_pair_forces_staged"}
 
 
 def tuned_shape(engine_mod, system, precision: int, dev, torch, enabled: bool, reproducible: bool = False,
@@ -249,8 +247,7 @@ def scheme_of(shape) -> str:
 
 def pair_scheme_name(shape) -> str:
     return {"full": "full shell (reproducible)", "half": "half shell (atomics)",
-            "staged": "half shell staged in shared memory (atomics)",
-            "frame": "half shell, candidates tested on an absolute-x frame shadow (atomics)"}[scheme_of(shape)]
+            "staged": "half shell staged in shared memory (atomics)"}[scheme_of(shape)]
 
 
 def time_engine(engine_mod, system, precision: int, steps: int, warmup: int, dev, torch, profile: bool,
@@ -546,7 +543,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default pair-kernel launch shape")
     ap.add_argument("--reproducible", action="store_true",
                     help="tune over the full-shell (bitwise reproducible) pair scheme only")
-    ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged", "frame"], default="auto",
+    ap.add_argument("--pair-scheme", choices=["auto", "full", "half", "staged"], default="auto",
                     help="fixed pair scheme with its default shape instead of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both")
     ap.add_argument("--monitor", action="store_true",

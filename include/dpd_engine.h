@@ -216,13 +216,6 @@ DPD_API int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t p
  * neighbour rows staged in shared memory; same accuracy and run-to-run
  * variation as DPD_PAIR_HALF_SHELL (slower on a B200: kept for comparison). */
 #define DPD_PAIR_STAGED     2
-/* DPD_PAIR_FRAME: the half-shell pair set with the candidate test reading a
- * shadow of FP32 absolute x (cell-relative y, z), so a row segment has one
- * constant x shift instead of a per-candidate choice; the force pass takes
- * the x separation from the FP64 positions.  Same accuracy and run-to-run
- * variation as DPD_PAIR_HALF_SHELL.  Single-box FP32 forces; FP64 engines and
- * replica batches run the DPD_PAIR_HALF_SHELL kernels under this setting. */
-#define DPD_PAIR_FRAME      3
 DPD_API int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme);
 
 /* Waits for queued work; returns the device status bits seen so far. */

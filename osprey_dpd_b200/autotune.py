@@ -28,9 +28,6 @@ HALF_SHELL_CANDIDATES: Tuple[Shape, ...] = (
 )
 # staged half-shell shape (pair scheme 2): smaller hit lists leave room for the staged rows
 STAGED_CANDIDATES: Tuple[Shape, ...] = ((16, 0, 100, 2),)
-# half shell tested on the absolute-x frame shadow (pair scheme 3, single box, FP32;
-# FP64 engines and batches fall back to scheme 1 under it)
-FRAME_CANDIDATES: Tuple[Shape, ...] = ((32, 0, -1, 3), (24, 0, -1, 3), (32, 0, 100, 3), (24, 0, 100, 3))
 CACHE = os.environ.get("DPD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "osprey_dpd_b200",
                                                        "launch_shapes.json"))
 

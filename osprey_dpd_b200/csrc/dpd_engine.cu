@@ -22,7 +22,6 @@
 #include "dpd_kernels.cuh"
 #include "pair_forces.cuh"
 #include "pair_staged.cuh"
-#include "pair_frame.cuh"
 #include "slice_stress.cuh"
 #include "monitor.cuh"
 #include "upload.cuh"
@@ -104,7 +103,6 @@ struct dpd_engine {
     void* d_stress = nullptr;   // per-bead virial of the last sample step (real, 9 planes)
     void* d_pos4 = nullptr;
     void* d_vel4 = nullptr;
-    float4* d_tst4 = nullptr;   // frame shadow (single-box FP32 engines), n + kFramePad entries
     int* d_rank = nullptr;
     int* d_perm = nullptr;
     int* d_pid[2] = {nullptr, nullptr};   // noise id (reference bead id) in slot order
@@ -305,7 +303,6 @@ int push_constants(dpd_engine* e)
     }
     K.ntypes = e->ntypes;
     K.seed = b0.seed;
-    K.tst4 = e->pair_scheme == DPD_PAIR_FRAME ? e->d_tst4 : nullptr;
     const int m = e->ntypes * e->ntypes;
     const size_t nb = e->hboxes.size();
     std::vector<double> tab(3 * (size_t)m * nb);
@@ -414,10 +411,6 @@ struct Timed {
 template <typename real>
 auto pair_kernel(bool multi, bool sample, int scheme)
 {
-    if constexpr (sizeof(real) == 4) {
-        if (scheme == DPD_PAIR_FRAME && !multi) return sample ? k_pair_forces_frame<true> : k_pair_forces_frame<false>;
-    }
-    if (scheme == DPD_PAIR_FRAME) scheme = DPD_PAIR_HALF_SHELL;   // FP64 and batches: the half-shell kernels
     if (scheme == DPD_PAIR_STAGED)
         return multi ? (sample ? k_pair_forces_staged<real, true, true> : k_pair_forces_staged<real, false, true>)
                      : (sample ? k_pair_forces_staged<real, true, false> : k_pair_forces_staged<real, false, false>);
@@ -433,7 +426,7 @@ template <typename real>
 size_t pair_dyn_bytes(const dpd_engine* e, bool multi)
 {
     if (e->pair_scheme == DPD_PAIR_STAGED) return StgLayout<real>(e->ntypes, e->pair_hitcap, multi).total;
-    if (e->pair_scheme == DPD_PAIR_HALF_SHELL || e->pair_scheme == DPD_PAIR_FRAME)
+    if (e->pair_scheme == DPD_PAIR_HALF_SHELL)
         return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
     return pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
 }
@@ -536,21 +529,29 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
                        e->d_block_count, e->d_start));
     }
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
-    {
-        Timed t(e, DPD_KERNEL_PERMUTE);
-        CU(launch_step(e, k_permute, blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st, n,
-                       e->nchunk, cell_in, e->d_rank, e->d_start, e->d_perm, e->d_block_count));
+    // The full shell keeps every cell's beads in the order of their previous
+    // slots (bitwise reproducible forces): arrival permutation, then a gather.
+    // The half-shell schemes add forces with atomics in no fixed order anyway:
+    // their beads are scattered to cell start + arrival rank, one kernel less.
+    const bool stable = e->pair_scheme == DPD_PAIR_FULL_SHELL;
+    if (stable) {
+        {
+            Timed t(e, DPD_KERNEL_PERMUTE);
+            CU(launch_step(e, k_permute, blocks_for(std::max<int64_t>(n, e->nchunk), kThreads), kThreads, 0, st, n,
+                           e->nchunk, cell_in, e->d_rank, e->d_start, e->d_perm, e->d_block_count));
+        }
+        if ((rc = check_launch(e, "k_permute"))) return rc;
     }
-    if ((rc = check_launch(e, "k_permute"))) return rc;
     {
         Timed t(e, DPD_KERNEL_GATHER);
         // the half-shell schemes accumulate into F with atomics: k_gather clears it
-        const int zero_F = e->pair_scheme != DPD_PAIR_FULL_SHELL ? 1 : 0;
-        CU(launch_step(e, k_gather<real>, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_perm, e->d_start, x_in,
-                       e->d_v[a], (real*)e->d_F, e->d_bid[a], e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b],
-                       (real*)e->d_Fold, e->d_bid[b], e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b],
-                       (V4*)e->d_pos4, (V4*)e->d_vel4, e->d_ubuf, (const double*)(e->off_active ? e->d_off : nullptr),
-                       zero_F));
+        const int zero_F = stable ? 0 : 1;
+        CU(launch_step(e, k_gather<real>, blocks_for(std::max<int64_t>(n, stable ? 0 : e->nchunk), kThreads), kThreads,
+                       0, st, n, e->d_K, e->d_boxes, e->d_perm, e->d_start, x_in, e->d_v[a], (real*)e->d_F,
+                       e->d_bid[a], e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b], (real*)e->d_Fold,
+                       e->d_bid[b], e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b], (V4*)e->d_pos4,
+                       (V4*)e->d_vel4, e->d_ubuf, (const double*)(e->off_active ? e->d_off : nullptr), zero_F,
+                       (const int*)(stable ? nullptr : e->d_rank), (int)e->nchunk, e->d_block_count));
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
     // bond and bond-pair forces: a branch beside the pair kernel (on the
@@ -589,8 +590,7 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
         const int tiles = blocks_for(n, kPairBlock);
-        const bool frame = e->pair_scheme == DPD_PAIR_FRAME && sizeof(real) == 4 && !multi;   // one tile per block
-        const int tpb = (e->pair_bps > 0 && !frame) ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
+        const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
         CU(launch_step(e, kern, blocks_for(tiles, tpb), kPairBlock, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
@@ -657,7 +657,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "bps") e->pair_bps = std::max(val, 0);
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
-            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_FRAME) e->pair_scheme = val;
+            else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
             else if (key == "ahead") e->ahead_enabled = val != 0;
             else if (key == "pdl") e->pdl = val != 0;
         }
@@ -875,15 +875,14 @@ int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persisten
 int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
 {
     if (!e) return DPD_E_ARG;
-    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED &&
-        scheme != DPD_PAIR_FRAME)
+    if (scheme != DPD_PAIR_FULL_SHELL && scheme != DPD_PAIR_HALF_SHELL && scheme != DPD_PAIR_STAGED)
         return fail(e, DPD_E_ARG, "unknown pair scheme");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
     e->pair_scheme = scheme;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
-    return push_constants(e);   // the frame shadow is written only under DPD_PAIR_FRAME
+    return DPD_OK;
 }
 
 int dpd_engine_set_sample_period(dpd_engine* e, int64_t period)
@@ -1047,7 +1046,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
                          (void**)&e->d_perm, (void**)&e->d_pid[0], (void**)&e->d_pid[1], (void**)&e->d_pid_of,
                          (void**)&e->d_partials,
                          (void**)&e->d_out, (void**)&e->d_out_cell, (void**)&e->d_xa, (void**)&e->d_imga,
-                         (void**)&e->d_cella, (void**)&e->d_tst4};
+                         (void**)&e->d_cella};
         for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
         const size_t rs = real_size(e);
         int rc;
@@ -1074,15 +1073,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(n, kThreads) * kObsTerms))) return rc;
         if ((rc = dalloc(e, &e->d_out, 21 * (size_t)n))) return rc;
         if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
-        if (e->precision == DPD_PRECISION_MIXED && e->hboxes.size() == 1) {
-            // frame shadow with far-away padding past the last bead (its test
-            // loop reads there without a per-candidate clamp)
-            if ((rc = dalloc(e, &e->d_tst4, (size_t)n + kFramePad))) return rc;
-            std::vector<float4> pad(kFramePad, make_float4(1e30f, 1e30f, 1e30f, 0.f));
-            CU(cudaMemcpy(e->d_tst4 + n, pad.data(), sizeof(float4) * kFramePad, cudaMemcpyHostToDevice));
-        }
         e->n = n;
-        if ((rc = push_constants(e))) return rc;   // the frame shadow's address
     }
     // cell starts, then the slot order: by cell, inside a cell by upload index
     k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start);

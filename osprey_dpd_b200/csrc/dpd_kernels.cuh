@@ -64,10 +64,6 @@ struct StepConst {
     int nc[3];
     int ntypes;
     uint64_t seed;
-    // frame shadow of the DPD_PAIR_FRAME scheme (FP32 absolute x, cell-relative
-    // y and z per slot, padded past the last bead), written by k_gather; NULL
-    // when that scheme is not in use
-    float4* tst4;
 };
 
 // One simulation box (CCNTCell::SetSimBoxLengths, CNTCell.cpp:143-158).  An
@@ -318,13 +314,19 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     uint32_t* __restrict__ img_out, int* __restrict__ cell_out, const int* __restrict__ pid_in,
     int* __restrict__ pid_out, typename Vec4<real>::type* __restrict__ pos4,
     typename Vec4<real>::type* __restrict__ vel4, double4* __restrict__ ubuf, const double* __restrict__ off,
-    int zero_F)
+    int zero_F, const int* __restrict__ rank, int nchunk, int* __restrict__ block_count)
 {
     pdl_wait();
     pdl_launch();
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= n) return;
-    const int s = perm[d];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    // Scatter mode (rank != NULL): thread t moves source slot t to its cell
+    // start plus its arrival rank, in no fixed order inside the cell, and the
+    // arrival permutation (k_permute) is not needed; it also clears the
+    // per-chunk totals for the next step.  Gather mode: thread t fills slot t
+    // from perm, in the order of the beads' previous slots.
+    if (rank && t < nchunk) block_count[t] = 0;
+    if (t >= n) return;
+    const int s = rank ? t : perm[t];
     // the bead's state is independent of its final slot: load it before the
     // rank scan so both memory round trips overlap
     const int c = cell_in[s];
@@ -340,10 +342,15 @@ __global__ void __launch_bounds__(256, 6) k_gather(
         vs[q] = v_in[q * n + s];
         fs[q] = F_in[q * n + s];
     }
-    const int beg = start[c], end = start[c + 1];
-    int k = 0;
-    for (int e = beg; e < end; ++e) k += (perm[e] < s);
-    const int o = beg + k;
+    int o;
+    if (rank) {
+        o = start[c] + rank[s];
+    } else {
+        const int beg = start[c], end = start[c + 1];
+        int k = 0;
+        for (int e = beg; e < end; ++e) k += (perm[e] < s);
+        o = beg + k;
+    }
     const Box& B = boxes[flag_box(tfl)];
     const int nx = B.nc[0], ny = B.nc[1];
     const int cl = c - B.cell_base;
@@ -372,7 +379,6 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     w.x = vt[0]; w.y = vt[1]; w.z = vt[2]; w.w = as_real_bits(pid, real(0));
     pos4[o] = p;
     vel4[o] = w;
-    if (K->tst4) K->tst4[o] = make_float4((float)xs[0], (float)rel[1], (float)rel[2], 0.f);
     if (flag_bonded(tfl)) {
         // unPBC position (x + image*L + upload offset) for the bonded terms,
         // stored by upload index: chain partners sit in the same lines

@@ -28,7 +28,6 @@ STATUS_IMAGE_OVERFLOW = 0x4
 PAIR_FULL_SHELL = 0      # default: bitwise reproducible forces
 PAIR_HALF_SHELL = 1      # each pair once, partner force by atomics
 PAIR_STAGED = 2          # half shell with the neighbour rows staged in shared memory
-PAIR_FRAME = 3           # half shell, candidate test on an absolute-x shadow (one x shift per row segment)
 
 EXPORTED = [
     "dpd_engine_create", "dpd_engine_upload_beads", "dpd_engine_upload_topology",

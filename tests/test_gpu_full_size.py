@@ -34,7 +34,7 @@ WORKLOADS = {
     "polymer": lambda: W.polymer_solution(),
 }
 # the pair schemes the benchmark's autotuner chooses from for a single box
-SCHEMES = {"half": 1, "frame": 3}
+SCHEMES = {"half": 1}
 
 
 def _face_distance(x, widths):

@@ -1,6 +1,5 @@
 """The half-shell pair schemes (each pair evaluated once, the partner's share
-added with atomics; unstaged, staged per tile in shared memory, and tested
-on the absolute-x frame shadow) against the CPU
+added with atomics; unstaged and staged in shared memory) against the CPU
 oracle.  Its force sums are rounded in
 a run-dependent order, so the bounds are the tolerances of the full-shell
 tests rather than bit equality:
@@ -26,7 +25,7 @@ SYSTEMS = {
 }
 
 
-SCHEMES = pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "frame"])
+SCHEMES = pytest.mark.parametrize("scheme", [1, 2], ids=["half", "staged"])
 
 
 def _half(engine_mod, oracle_mod, s, precision, scheme=1, **kw):
@@ -94,8 +93,7 @@ def _dense_cluster_system():
 
 
 @pytest.mark.parametrize("tune", ["half=1", "half=1,hitcap=8", "half=1,hitcap=64,bps=1", "scheme=2",
-                                  "scheme=2,hitcap=8", "scheme=2,hitcap=64,bps=1", "scheme=3", "scheme=3,hitcap=8",
-                                  "scheme=3,hitcap=64"])
+                                  "scheme=2,hitcap=8", "scheme=2,hitcap=64,bps=1"])
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
 def test_half_shell_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precision, tune, monkeypatch):
     """Selected through DPD_TUNE, with a 60-bead cell and extreme hit-list sizes."""
@@ -150,7 +148,7 @@ def test_switching_schemes_between_calls(engine_mod):
         b.set_pair_scheme(7)
 
 
-@pytest.mark.parametrize("scheme", [1, 2, 3], ids=["half", "staged", "frame"])
+@pytest.mark.parametrize("scheme", [1, 2], ids=["half", "staged"])
 @pytest.mark.parametrize("workload", ["bilayer", "polymer"])
 def test_half_shell_matches_full_shell_at_full_size(engine_mod, workload, scheme):
     """The half-shell schemes against the full-shell kernel on the full-size
