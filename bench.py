@@ -515,14 +515,18 @@ def time_monitor(engine_mod, system, dev, reps: int = 10):
             "timing": "host wall clock around synchronous calls"}
 
 
-def read_traffic(n_beads: int, scheme: str = "full"):
+def read_traffic(n_beads: int, scheme: str = "full", workload: str = None):
     """Per-launch DRAM bytes of the pair kernel (full, half or staged) from the
-    committed ncu summary, scaled to the bead count."""
+    committed ncu summaries: the capture of this scheme on this workload when
+    there is one, else the scheme's melt capture scaled to the bead count."""
     p = os.path.join(ROOT, "profiles", "pair_forces_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
-        d = json.load(fh).get(scheme) or {}
+        table = json.load(fh)
+    d = table.get(f"{scheme}_{workload}") or table.get(scheme) or {}
+    if d.get("n_beads") == n_beads:
+        return d["dram_bytes_read"] + d["dram_bytes_write"]
     per_bead = d.get("dram_bytes_per_bead")
     return None if per_bead is None else per_bead * n_beads
 
@@ -653,7 +657,7 @@ def main():
                      "avg_launch_ms": t_pair * 1000.0,
                      "timing": "CUDA events around every kernel on the engine's stream, in a 20-step pass "
                                "after the timed region (same engine and workload, kernels launched one by one)",
-                     "traffic": read_traffic(system.n, scheme)},
+                     "traffic": read_traffic(system.n, scheme, args.workload)},
         "roofline_step_hbm": {"bound": "hbm", "achieved": hbm_ach / 1e9, "peak": float(peaks["hbm_gbs"]),
                               "unit": "GB/s", "frac": hbm_ach / 1e9 / float(peaks["hbm_gbs"]),
                               "bytes_per_bead_step": ALG_BYTES_PER_BEAD_STEP["mixed"], "basis": peak_kind},
