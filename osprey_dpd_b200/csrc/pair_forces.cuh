@@ -38,16 +38,7 @@ constexpr float kPruneR2 = 1.0f + 1e-5f;
 
 template <typename real> struct RealOps;
 template <> struct RealOps<float> {
-    // The hardware reciprocal square root, refined by one Newton-Raphson step
-    // for 1/sqrt(x), y' = y (3 - x y^2) / 2: the approximation's error (about
-    // 2^-22 relative) otherwise reaches 1e-5 of the force RMS in the largest
-    // boxes through w = 1 - r at the cut-off.  x = 0 gives NaN, which the
-    // callers mask (coincident beads, r^2 <= 1e-18).
-    static __device__ __forceinline__ float rsqrt(float x)
-    {
-        const float y = rsqrtf(x);
-        return y * (1.5f - (0.5f * x) * (y * y));
-    }
+    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
     static __device__ __forceinline__ float rnd(float x) { return rintf(x); }
 };
 template <> struct RealOps<double> {
@@ -59,15 +50,23 @@ template <> struct RealOps<double> {
 // (slot order, three planes of n; minimum image in a box of lengths L): the
 // FP32 cell-relative shadows carry ~6e-8 absolute error, which for beads a
 // few 1e-3 apart (random initial states of millions of beads) turns the pair
-// direction by ~1e-5.  Rare, so the branch costs little.  FP64 shadows are
-// exact already.
+// direction by ~1e-5.  Rare, so the branch costs little.  The pair is first
+// evaluated as every other pair; close_pair_fix then replaces its separation
+// and force scalar m (a, g, s: a_ij, gamma_ij, sigma_ij; noise: 0.5 - U), and
+// the callers accumulate m * separation with explicit round-to-nearest
+// operations, so the arithmetic of ordinary pairs does not depend on the
+// presence of this branch (a replica batch and a single box round alike).
+// FP64 shadows are exact already.
 constexpr float kCloseR2 = 0.01f;
-__device__ __forceinline__ void refine_close(double&, double&, double&, double&, const double*, int, int, int,
-                                             const double*)
+template <typename V4>
+__device__ __forceinline__ void close_pair_fix(double&, double&, double&, double&, double, const double*, int, int, int,
+                                               const double*, const V4&, const V4&, double, double, double, double)
 {
 }
-__device__ __forceinline__ void refine_close(float& dx, float& dy, float& dz, float& r2, const double* __restrict__ xs,
-                                             int n, int i, int j, const double* L)
+template <typename V4>
+__device__ __forceinline__ void close_pair_fix(float& dx, float& dy, float& dz, float& m, float r2,
+                                               const double* __restrict__ xs, int n, int i, int j, const double* L,
+                                               const V4& vi, const V4& vj, float a, float g, float s, float noise)
 {
     if (r2 < kCloseR2 && xs) {
         float d[3];
@@ -78,7 +77,44 @@ __device__ __forceinline__ void refine_close(float& dx, float& dy, float& dz, fl
             d[q] = (float)e;
         }
         dx = d[0]; dy = d[1]; dz = d[2];
-        r2 = dx * dx + dy * dy + dz * dz;
+        const float rr = dx * dx + dy * dy + dz * dz;
+        const float inv = rsqrtf(rr);
+        const float wr = 1.f - rr * inv;
+        const float rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
+        m = rr > 1e-18f ? (a * wr - g * wr * wr * rdotv + s * wr * noise) * inv : 0.f;
+    }
+}
+
+// The pair's force m * (dx, dy, dz) added to acc (and the virial terms), with
+// explicit roundings (see close_pair_fix); returns the force in g.
+template <typename real, bool VIRIAL>
+__device__ __forceinline__ void pair_accumulate(real m, real dx, real dy, real dz, real* acc, real g[3])
+{
+    g[0] = m * dx;
+    g[1] = m * dy;
+    g[2] = m * dz;
+    if (sizeof(real) == 4) {
+        g[0] = __fmul_rn((float)m, (float)dx);
+        g[1] = __fmul_rn((float)m, (float)dy);
+        g[2] = __fmul_rn((float)m, (float)dz);
+        acc[0] = __fadd_rn((float)acc[0], (float)g[0]);
+        acc[1] = __fadd_rn((float)acc[1], (float)g[1]);
+        acc[2] = __fadd_rn((float)acc[2], (float)g[2]);
+        if (VIRIAL) {
+            const float d[3] = {(float)dx, (float)dy, (float)dz};
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    acc[3 + 3 * r + c] = __fadd_rn((float)acc[3 + 3 * r + c], __fmul_rn(d[c], (float)g[r]));
+        }
+    } else {
+        acc[0] += g[0]; acc[1] += g[1]; acc[2] += g[2];
+        if (VIRIAL) {
+            acc[3] += dx * g[0]; acc[4] += dy * g[0]; acc[5] += dz * g[0];
+            acc[6] += dx * g[1]; acc[7] += dy * g[1]; acc[8] += dz * g[1];
+            acc[9] += dx * g[2]; acc[10] += dy * g[2]; acc[11] += dz * g[2];
+        }
     }
 }
 
@@ -128,8 +164,7 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
             real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
             real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
             real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-            real r2 = dx * dx + dy * dy + dz * dz;
-            refine_close(dx, dy, dz, r2, xs, n, i, j, L);
+            const real r2 = dx * dx + dy * dy + dz * dz;
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -142,16 +177,11 @@ __device__ __forceinline__ void pair_force_pass(int cnt, const uint32_t* __restr
                 c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
                 c1 = (uint32_t)prod;
             }
-            const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
-                             T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-            const real m = mag * inv;
-            const real gx = m * dx, gy = m * dy, gz = m * dz;
-            acc[0] += gx; acc[1] += gy; acc[2] += gz;
-            if (VIRIAL) {
-                acc[3] += dx * gx; acc[4] += dy * gx; acc[5] += dz * gx;
-                acc[6] += dx * gy; acc[7] += dy * gy; acc[8] += dz * gy;
-                acc[9] += dx * gz; acc[10] += dy * gz; acc[11] += dz * gz;
-            }
+            const real ta = T[tt], tg = T[m2 + tt], ts = T[2 * m2 + tt], noise = noise_centered(c0, real(0));
+            real m = (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv;
+            close_pair_fix(dx, dy, dz, m, r2, xs, n, i, j, L, vi, vj, ta, tg, ts, noise);
+            real g[3];
+            pair_accumulate<real, VIRIAL>(m, dx, dy, dz, acc, g);
         }
     }
 }
@@ -460,8 +490,7 @@ __device__ __forceinline__ void balanced_force_pass(
                 dz = (pi.z - pj.z) - (real)((int)(ent >> 30) - 1) * wz;
             }
             const V4 vj = vel4[j];
-            real r2 = dx * dx + dy * dy + dz * dz;
-            refine_close(dx, dy, dz, r2, xs, n, islot, j, Lb);
+            const real r2 = dx * dx + dy * dy + dz * dz;
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -474,22 +503,18 @@ __device__ __forceinline__ void balanced_force_pass(
                 c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
                 c1 = (uint32_t)prod;
             }
-            const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
-                             T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-            // the staged tests decide pairs at the cut-off from rounded
-            // window coordinates: the exact cut-off is applied here, and
-            // coincident beads (r2 <= 1e-18) are left to this pass
-            const real m = (r2 < real(1) && r2 > real(1e-18)) ? mag * inv : real(0);
-            const real gx = m * dx, gy = m * dy, gz = m * dz;
-            acc[0] += gx; acc[1] += gy; acc[2] += gz;
-            atomicAdd(F + j, -gx);
-            atomicAdd(F + n + j, -gy);
-            atomicAdd(F + 2 * n + j, -gz);
-            if (VIRIAL) {
-                acc[3] += dx * gx; acc[4] += dy * gx; acc[5] += dz * gx;
-                acc[6] += dx * gy; acc[7] += dy * gy; acc[8] += dz * gy;
-                acc[9] += dx * gz; acc[10] += dy * gz; acc[11] += dz * gz;
-            }
+            const real ta = T[tt], tg = T[m2 + tt], ts = T[2 * m2 + tt], noise = noise_centered(c0, real(0));
+            // the staged test decides pairs at the cut-off from rounded window
+            // coordinates: the exact cut-off is applied here, and coincident
+            // beads (r2 <= 1e-18) are left to this pass
+            real m = (r2 < real(1) && r2 > real(1e-18)) ? (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv
+                                                          : real(0);
+            close_pair_fix(dx, dy, dz, m, r2, xs, n, islot, j, Lb, vi, vj, ta, tg, ts, noise);
+            real g[3];
+            pair_accumulate<real, VIRIAL>(m, dx, dy, dz, acc, g);
+            atomicAdd(F + j, -g[0]);
+            atomicAdd(F + n + j, -g[1]);
+            atomicAdd(F + 2 * n + j, -g[2]);
         }
         atomicAdd(F + islot, acc[0]);
         atomicAdd(F + n + islot, acc[1]);
@@ -528,8 +553,7 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
             real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
             real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
             real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-            real r2 = dx * dx + dy * dy + dz * dz;
-            refine_close(dx, dy, dz, r2, xs, n, i, j, L);
+            const real r2 = dx * dx + dy * dy + dz * dz;
             const real inv = RealOps<real>::rsqrt(r2);
             const real wr = real(1) - r2 * inv;
             const int tt = ti + (real_bits(pj.w) & 0xFF);
@@ -542,19 +566,14 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
                 c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
                 c1 = (uint32_t)prod;
             }
-            const real mag = T[tt] * wr - T[m2 + tt] * wr * wr * rdotv +
-                             T[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-            const real m = mag * inv;
-            const real gx = m * dx, gy = m * dy, gz = m * dz;
-            acc[0] += gx; acc[1] += gy; acc[2] += gz;
-            atomicAdd(F + j, -gx);
-            atomicAdd(F + n + j, -gy);
-            atomicAdd(F + 2 * n + j, -gz);
-            if (VIRIAL) {
-                acc[3] += dx * gx; acc[4] += dy * gx; acc[5] += dz * gx;
-                acc[6] += dx * gy; acc[7] += dy * gy; acc[8] += dz * gy;
-                acc[9] += dx * gz; acc[10] += dy * gz; acc[11] += dz * gz;
-            }
+            const real ta = T[tt], tg = T[m2 + tt], ts = T[2 * m2 + tt], noise = noise_centered(c0, real(0));
+            real m = (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv;
+            close_pair_fix(dx, dy, dz, m, r2, xs, n, i, j, L, vi, vj, ta, tg, ts, noise);
+            real g[3];
+            pair_accumulate<real, VIRIAL>(m, dx, dy, dz, acc, g);
+            atomicAdd(F + j, -g[0]);
+            atomicAdd(F + n + j, -g[1]);
+            atomicAdd(F + 2 * n + j, -g[2]);
         }
     }
 }

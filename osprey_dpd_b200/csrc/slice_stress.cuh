@@ -72,8 +72,7 @@ __device__ __forceinline__ void slice_eval(int cnt, const uint32_t* __restrict__
         real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
         real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
         real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-        real r2 = dx * dx + dy * dy + dz * dz;
-        refine_close(dx, dy, dz, r2, x, n, i, j, L);
+        const real r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 < real(1) && r2 > real(1e-18))) continue;   // the test's rounding differs at the cut-off
         const real inv = RealOps<real>::rsqrt(r2);
         const real wr = real(1) - r2 * inv;
@@ -88,9 +87,9 @@ __device__ __forceinline__ void slice_eval(int cnt, const uint32_t* __restrict__
             c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
             c1 = (uint32_t)prod;
         }
-        const real mag = tab[tt] * wr - tab[m2 + tt] * wr * wr * rdotv +
-                         tab[2 * m2 + tt] * wr * noise_centered(c0, real(0));
-        const real m = mag * inv;
+        const real ta = tab[tt], tg = tab[m2 + tt], ts = tab[2 * m2 + tt], noise = noise_centered(c0, real(0));
+        real m = (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv;
+        close_pair_fix(dx, dy, dz, m, r2, x, n, i, j, L, vi, vj, ta, tg, ts, noise);
         const double f[3] = {(double)(m * dx), (double)(m * dy), (double)(m * dz)};
         const double d[3] = {(double)dx, (double)dy, (double)dz};
         double fdx[9];
