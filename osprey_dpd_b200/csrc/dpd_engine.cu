@@ -166,10 +166,13 @@ struct dpd_engine {
     // pinned host
     unsigned* h_status = nullptr;
     // status word as of the start of the latest call's device work, written by
-    // that call's k_set_step into mapped pinned memory (d_seen is its device
+    // that call's first kernel into mapped pinned memory (d_seen is its device
     // address); read by dpd_engine_step without waiting
     unsigned* h_seen = nullptr;
     unsigned* d_seen = nullptr;
+    // the value the device step counter holds once every queued step has run
+    // (each step's k_update_mom advances it); INT64_MIN: unknown
+    int64_t dev_step = INT64_MIN;
     double* h_obs = nullptr;
     bool obs_valid = false;
     bool obs_has_virial = false;
@@ -519,14 +522,16 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
             Timed t(e, DPD_KERNEL_UPDATE_POS);
             CU(launch_step(e, k_update_pos<real>, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
                            (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
-                           e->d_block_count, e->d_status));
+                           e->d_block_count, e->d_status, first ? e->d_seen : (unsigned*)nullptr));
         }
         if ((rc = check_launch(e, "k_update_pos"))) return rc;
     }
     {
         Timed t(e, DPD_KERNEL_SCAN_CELLS);
+        // the call's first kernel publishes the status word (k_update_pos when it runs)
         CU(launch_step(e, k_scan_cells, e->nchunk, kScanThreads, 0, st, (int)e->ncell, n, e->d_count,
-                       e->d_block_count, e->d_start));
+                       e->d_block_count, e->d_start, (const unsigned*)e->d_status,
+                       (first && from_ahead) ? e->d_seen : (unsigned*)nullptr));
     }
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
     // The full shell keeps every cell's beads in the order of their previous
@@ -576,6 +581,14 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
             kern<<<blocks_for(e->nbb, kThreads), kThreads, 0, bst>>>((int)e->nbb, n, e->d_bb, topo, e->d_Fb, e->d_Sb);
         }
         if ((rc = check_launch(e, "k_bonds"))) return rc;
+        if (slices && e->topo_nb + e->topo_na > 0) {
+            // the profile's bond and bond-pair part, bonds and bond pairs in whole warps each
+            Timed t(e, DPD_KERNEL_BONDED);
+            const int64_t threads = ((e->topo_nb + 31) & ~(int64_t)31) + ((e->topo_na + 31) & ~(int64_t)31);
+            k_bonded_slices<<<blocks_for(threads, kThreads), kThreads, 0, bst>>>((int)e->topo_nb, (int)e->topo_na,
+                                                                                 topo);
+            if ((rc = check_launch(e, "k_bonded_slices"))) return rc;
+        }
         if (fork) CU(cudaEventRecord(e->ev_join, e->side));
     }
     {
@@ -1076,7 +1089,8 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         e->n = n;
     }
     // cell starts, then the slot order: by cell, inside a cell by upload index
-    k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start);
+    k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start,
+                                                     (const unsigned*)e->d_status, (unsigned*)nullptr);
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
     CU(cudaMemsetAsync(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk, st));
     k_up_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, e->d_up_cell, e->d_start, e->d_count,
@@ -1908,11 +1922,16 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     }
     if (nsteps == 0) return DPD_OK;
     CU(cudaSetDevice(e->device));
-    // the step counter keys the pair noise; it is advanced on the device
-    // by the last kernel of every step
-    k_set_step<<<1, 1, 0, e->s()>>>(e->d_step, first_step, e->d_status, e->d_seen);
-    CU(cudaGetLastError());
-    e->launches += 1;
+    // the step counter keys the pair noise; it is advanced on the device by
+    // every step's k_update_mom, so it is set only when this call does not
+    // continue where the queued work ends
+    const bool continues = first_step == e->dev_step;
+    e->dev_step = INT64_MIN;   // until this call's steps are all queued
+    if (!continues) {
+        k_set_step<<<1, 1, 0, e->s()>>>(e->d_step, first_step, e->d_status, e->d_seen);
+        CU(cudaGetLastError());
+        e->launches += 1;
+    }
     std::vector<char> samples(nsteps);
     const bool from_ahead = e->ahead_valid, to_ahead = e->ahead_enabled;
     for (int32_t k = 0; k < nsteps; ++k) {
@@ -1978,6 +1997,7 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
             break;
         }
     e->ahead_valid = to_ahead;
+    e->dev_step = first_step + nsteps;
     e->stepped = true;
     e->obs_valid = false;
     e->box_obs_valid = false;

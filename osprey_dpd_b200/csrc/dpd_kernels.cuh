@@ -100,6 +100,15 @@ __device__ __forceinline__ double as_real_bits(int v, double) { return __longlon
 __device__ __forceinline__ int real_bits(float v) { return __float_as_int(v); }
 __device__ __forceinline__ int real_bits(double v) { return (int)__double_as_longlong(v); }
 
+// The first kernel of a call copies the status word of all work queued
+// before it (its predecessors have completed: a call's first kernel waits
+// for them in full) to `seen`, a word of mapped pinned host memory that the
+// host reads without waiting; seen = NULL in every other launch.
+__device__ __forceinline__ void publish_status(const unsigned* status, unsigned* seen)
+{
+    if (seen && blockIdx.x == 0 && threadIdx.x == 0) *(volatile unsigned*)seen = *(const volatile unsigned*)status;
+}
+
 // ------------------------------------------------------------- UpdatePos
 
 // One bead's drift and cell move; returns its new cell and writes x, img and
@@ -199,10 +208,11 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
     const double* __restrict__ v,
     const real* __restrict__ F, const int* __restrict__ tf, uint32_t* __restrict__ img,
     int* __restrict__ cell, int* __restrict__ rank, int* __restrict__ count,
-    int* __restrict__ block_count, unsigned* __restrict__ status)
+    int* __restrict__ block_count, unsigned* __restrict__ status, unsigned* seen)
 {
     pdl_wait();
     pdl_launch();
+    publish_status(status, seen);
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = s < n;
     int cnew = 0;
@@ -232,10 +242,11 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
 // Counts are cleared for the next step.
 static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     int ncell, int n, int* __restrict__ count, const int* __restrict__ block_count,
-    int* __restrict__ start)
+    int* __restrict__ start, const unsigned* status, unsigned* seen)
 {
     pdl_wait();
     pdl_launch();
+    publish_status(status, seen);
     __shared__ int warp_sum[kScanThreads / 32];
     __shared__ int base_s;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, wid = t >> 5;
@@ -617,6 +628,63 @@ __device__ __forceinline__ void unwrapped(const double4* __restrict__ ubuf, int 
     u[2] = q.z;
 }
 
+// CBond::AddForce (Bond.cpp:123-160, the serial build's unPBC coordinates):
+// the bond vector b = head - tail and the force g on the head bead.
+__device__ __forceinline__ void bond_force(const Topology& topo, int idx, double b[3], double g[3])
+{
+    double uh[3], ut[3];
+    unwrapped(topo.ubuf, topo.bond_h[idx], uh);
+    unwrapped(topo.ubuf, topo.bond_t[idx], ut);
+    const double bx = uh[0] - ut[0], by = uh[1] - ut[1], bz = uh[2] - ut[2];
+    const double len = sqrt(bx * bx + by * by + bz * bz);
+    const double k2 = topo.bond_k2[idx], l0 = topo.bond_l0[idx];
+    b[0] = bx; b[1] = by; b[2] = bz;
+    g[0] = k2 * (l0 - len) * bx / len;
+    g[1] = k2 * (l0 - len) * by / len;
+    g[2] = k2 * (l0 - len) * bz / len;
+}
+
+// CBondPair::AddForce (BondPair.cpp:140-285): the unPBC positions of the
+// first bond's tail and head and the second bond's head, and the forces on
+// the first bond's tail (G0) and the second bond's head (G2); the middle bead
+// takes -G0 - G2.  Zero forces for a degenerate pair (|b1||b2| <= 1e-4).
+__device__ __forceinline__ void bondpair_force(const Topology& topo, int idx, double u1t[3], double u1h[3],
+                                               double u2h[3], double G0[3], double G2[3])
+{
+    double u2t[3];
+    unwrapped(topo.ubuf, topo.ang_b1h[idx], u1h);
+    unwrapped(topo.ubuf, topo.ang_b1t[idx], u1t);
+    unwrapped(topo.ubuf, topo.ang_b2h[idx], u2h);
+    unwrapped(topo.ubuf, topo.ang_b2t[idx], u2t);
+    double b1[3], b2[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        b1[d] = u1h[d] - u1t[d];
+        b2[d] = u2h[d] - u2t[d];
+        G0[d] = 0.0;
+        G2[d] = 0.0;
+    }
+    const double l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
+    const double l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
+    const double mag = l1 * l2;
+    if (mag > 0.0001) {
+        const double dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
+        const double o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
+        const double k3 = topo.ang_k3[idx];
+        double fm = k3 / mag;
+        const double s0 = topo.ang_sin0[idx];
+        if (s0 != 0.0 && fabs(dot) > 0.000001) {
+            const double pre = sqrt(1.0 / (o1 * o2) - 1.0);
+            fm = k3 * (topo.ang_cos0[idx] - s0 / pre) / mag;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            G0[d] = fm * (o1 * b1[d] - b2[d]);
+            G2[d] = fm * (b1[d] - o2 * b2[d]);
+        }
+    }
+}
+
 // Bond and bond-pair forces of one bonded bead each, in upload order (chains
 // are contiguous there, so the partners' positions and the term tables are
 // read as whole lines), FP64 in both precision modes: the bond-pair force
@@ -624,6 +692,7 @@ __device__ __forceinline__ void unwrapped(const double4* __restrict__ ubuf, int 
 // nearly straight chains.  Each bond is evaluated by both of its beads and
 // each bond pair by its three beads, so no atomics.  Writes the bonded force
 // (and on sample steps the bond virial of the head bead) by upload index.
+// The slice stress profile's bonded part is k_bonded_slices.
 template <bool SAMPLE>
 __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __restrict__ bb, Topology topo,
                                                double4* __restrict__ Fb, double* __restrict__ Sb)
@@ -640,101 +709,26 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
             const int term = topo.csr_term[t];
             const int code = term & 7, idx = term >> 3;
             if (code <= kBondTail) {
-                // CBond::AddForce, Bond.cpp:123-160 (serial build: unPBC coordinates)
-                const int h = topo.bond_h[idx], tl = topo.bond_t[idx];
-                double uh[3], ut[3];
-                unwrapped(topo.ubuf, h, uh);
-                unwrapped(topo.ubuf, tl, ut);
-                const double bx = uh[0] - ut[0], by = uh[1] - ut[1], bz = uh[2] - ut[2];
-                const double len = sqrt(bx * bx + by * by + bz * bz);
-                const double k2 = topo.bond_k2[idx], l0 = topo.bond_l0[idx];
-                const double gx = k2 * (l0 - len) * bx / len;
-                const double gy = k2 * (l0 - len) * by / len;
-                const double gz = k2 * (l0 - len) * bz / len;
+                double bv[3], g[3];
+                bond_force(topo, idx, bv, g);
                 if (code == kBondHead) {
-                    bf[0] += gx; bf[1] += gy; bf[2] += gz;
+                    bf[0] += g[0]; bf[1] += g[1]; bf[2] += g[2];
                     if (SAMPLE) {
-                        bs[0] += bx * gx; bs[1] += by * gx; bs[2] += bz * gx;
-                        bs[3] += bx * gy; bs[4] += by * gy; bs[5] += bz * gy;
-                        bs[6] += bx * gz; bs[7] += by * gz; bs[8] += bz * gz;
-                        if (topo.sp.S) {   // CMonitor::AddBondStress, once per bond (its head bead)
-                            const double g[3] = {gx, gy, gz}, bv[3] = {bx, by, bz};
-                            double fdx[9];
-                            outer9(g, bv, fdx);
-                            slice_add(topo.sp, topo.sp.bond, topo.sp.nbt, topo.sp.bond_type[idx], fdx, bz,
-                                      topo.ubuf[h].w, topo.ubuf[tl].w);
-                        }
+                        bs[0] += bv[0] * g[0]; bs[1] += bv[1] * g[0]; bs[2] += bv[2] * g[0];
+                        bs[3] += bv[0] * g[1]; bs[4] += bv[1] * g[1]; bs[5] += bv[2] * g[1];
+                        bs[6] += bv[0] * g[2]; bs[7] += bv[1] * g[2]; bs[8] += bv[2] * g[2];
                     }
                 } else {
-                    bf[0] -= gx; bf[1] -= gy; bf[2] -= gz;
+                    bf[0] -= g[0]; bf[1] -= g[1]; bf[2] -= g[2];
                 }
             } else {
-                // CBondPair::AddForce, BondPair.cpp:140-285
-                double u1h[3], u1t[3], u2h[3], u2t[3];
-                const int a1h = topo.ang_b1h[idx], a1t = topo.ang_b1t[idx];
-                const int a2h = topo.ang_b2h[idx], a2t = topo.ang_b2t[idx];
-                unwrapped(topo.ubuf, a1h, u1h);
-                unwrapped(topo.ubuf, a1t, u1t);
-                unwrapped(topo.ubuf, a2h, u2h);
-                unwrapped(topo.ubuf, a2t, u2t);
-                double b1[3], b2[3];
+                double u1t[3], u1h[3], u2h[3], G0[3], G2[3];
+                bondpair_force(topo, idx, u1t, u1h, u2h, G0, G2);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    b1[d] = u1h[d] - u1t[d];
-                    b2[d] = u2h[d] - u2t[d];
-                }
-                const double l1 = sqrt(b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2]);
-                const double l2 = sqrt(b2[0] * b2[0] + b2[1] * b2[1] + b2[2] * b2[2]);
-                const double mag = l1 * l2;
-                double G0[3] = {0.0, 0.0, 0.0}, G2[3] = {0.0, 0.0, 0.0};
-                if (mag > 0.0001) {
-                    const double dot = b1[0] * b2[0] + b1[1] * b2[1] + b1[2] * b2[2];
-                    const double o1 = dot / (l1 * l1), o2 = dot / (l2 * l2);
-                    const double k3 = topo.ang_k3[idx];
-                    double fm = k3 / mag;
-                    const double s0 = topo.ang_sin0[idx];
-                    if (s0 != 0.0 && fabs(dot) > 0.000001) {
-                        const double pre = sqrt(1.0 / (o1 * o2) - 1.0);
-                        fm = k3 * (topo.ang_cos0[idx] - s0 / pre) / mag;
-                    }
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const double g0 = fm * (o1 * b1[d] - b2[d]);
-                        const double g2 = fm * (b1[d] - o2 * b2[d]);
-                        G0[d] = g0;
-                        G2[d] = g2;
-                        if (code == kAngle0) bf[d] += g0;
-                        else if (code == kAngle2) bf[d] += g2;
-                        else bf[d] += -g0 - g2;
-                    }
-                }
-                if (SAMPLE && topo.sp.S && code == kAngle0) {
-                    // CMonitor::AddBondPairStress, once per bond pair (its first tail bead): segments
-                    // first.tail -> first.head -> second.head -> first.tail, force 0.33333333 *
-                    // (F[j+1] - F[j]).  A degenerate pair (|b1||b2| <= 1e-4) adds zero here; the
-                    // reference would reuse the forces of its last non-degenerate step.
-                    const double* U[4] = {u1t, u1h, u2h, u1t};
-                    const double Z[4] = {topo.ubuf[a1t].w, topo.ubuf[a1h].w, topo.ubuf[a2h].w, topo.ubuf[a1t].w};
-                    double FF[4][3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        FF[0][d] = G0[d];
-                        FF[1][d] = -G0[d] - G2[d];
-                        FF[2][d] = G2[d];
-                        FF[3][d] = G0[d];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        double dv[3], fo[3], fdx[9];
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            dv[d] = U[j + 1][d] - U[j][d];
-                            fo[d] = 0.33333333 * (FF[j + 1][d] - FF[j][d]);
-                        }
-                        outer9(fo, dv, fdx);
-                        slice_add(topo.sp, topo.sp.bondpair, topo.sp.nbpt, topo.sp.bondpair_type[idx], fdx, dv[2],
-                                  Z[j + 1], Z[j]);
-                    }
+                    if (code == kAngle0) bf[d] += G0[d];
+                    else if (code == kAngle2) bf[d] += G2[d];
+                    else bf[d] += -G0[d] - G2[d];
                 }
             }
         }
@@ -742,6 +736,192 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
         if (SAMPLE) {
 #pragma unroll
             for (int q = 0; q < 9; ++q) Sb[(size_t)q * n + b] = bs[q];
+        }
+    }
+}
+
+// The slices one contribution spreads over, as slice_add visits them: kind 0
+// none (a z rounded up to L_z, or a type out of range), 1 one slice whole, 2
+// two halves (both beads on one slice face), 3 a span: `inner` slices
+// crossed whole (weight width/|dz|), then the lower end slice and, when
+// covered, the upper one.
+struct SliceSpan {
+    int kind, ui, li, n_inner;
+    double ur, lr, inner;
+};
+
+__device__ __forceinline__ SliceSpan slice_span(const SliceParams& sp, int K, int idx, double zDiff, double za,
+                                                double zb)
+{
+    SliceSpan s{0, 0, 0, 0, 0.0, 0.0, 0.0};
+    double up, lo;
+    if (zDiff > 0.00001) {
+        up = za * sp.inv;
+        lo = zb * sp.inv;
+    } else if (zDiff < -0.00001) {
+        zDiff = -zDiff;
+        up = zb * sp.inv;
+        lo = za * sp.inv;
+    } else {
+        up = za * sp.inv;
+        lo = up;
+    }
+    const int S = sp.S;
+    s.ui = (int)up;
+    s.ur = up - (double)s.ui;
+    s.li = (int)lo;
+    s.lr = lo - (double)s.li;
+    if (s.ui < 0 || s.ui >= S || s.li < 0 || s.li >= S || idx < 0 || idx >= K) return s;
+    if (s.ui == s.li) {
+        s.kind = (up != lo || s.ur > 0.00001) ? 1 : 2;
+    } else {
+        s.kind = 3;
+        s.inner = sp.width / zDiff;
+        s.n_inner = s.ui > s.li ? s.ui - s.li - 1 : S + s.ui - s.li - 1;
+    }
+    return s;
+}
+
+__device__ __forceinline__ int span_count(const SliceSpan& s)
+{
+    return s.kind == 0 ? 0 : (s.kind == 1 ? 1 : (s.kind == 2 ? 2 : s.n_inner + 1 + (s.ur > 0.000001 ? 1 : 0)));
+}
+
+// Entry t of the span: slice and weight (1.0 for a slice taken whole).
+__device__ __forceinline__ void span_entry(const SliceSpan& s, int S, int t, int& sl, double& fac)
+{
+    if (s.kind == 1) {
+        sl = s.li;
+        fac = 1.0;
+    } else if (s.kind == 2) {
+        sl = t == 0 ? s.ui : (s.li == 0 ? S - 1 : s.li - 1);
+        fac = 0.5;
+    } else if (t < s.n_inner) {
+        const int k = s.li + 1 + t;
+        sl = k >= S ? k - S : k;
+        fac = s.inner;
+    } else if (t == s.n_inner) {
+        sl = s.li;
+        fac = s.lr > 0.000001 ? (1.0 - s.lr) * s.inner : s.inner;
+    } else {
+        sl = s.ui;
+        fac = s.ur * s.inner;
+    }
+}
+
+// Adds v (9 components) to the FP64 bins arr[key * 9 ...] for every lane of
+// the warp with key >= 0: the lanes sharing a key are summed by shuffles and
+// one of them adds the sum, so lanes that meet on one bin (the bonds of a
+// membrane leaflet share a few slices) take one atomic instead of queueing
+// on it.  Called by all 32 lanes.
+__device__ __forceinline__ void warp_bin_add(double* __restrict__ arr, int key, const double v[9])
+{
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(0xffffffffu, key >= 0);
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const int kl = __shfl_sync(0xffffffffu, key, leader);
+        const unsigned grp = __ballot_sync(0xffffffffu, key == kl);
+        const bool mine = (grp >> lane) & 1u;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            double a = mine ? v[c] : 0.0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == leader) atomicAdd(arr + (size_t)kl * 9 + c, a);
+        }
+        pending &= ~grp;
+    }
+}
+
+// One contribution of every lane (fdx over the span of slices between its
+// beads) into bins arr[S][K][9]; lanes with cnt = 0 add nothing.
+__device__ __forceinline__ void warp_span_add(const SliceParams& sp, double* __restrict__ arr, int K, int idx,
+                                              const SliceSpan& s, const double fdx[9])
+{
+    const int cnt = span_count(s);
+    const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int t = 0; t < trip; ++t) {
+        int key = -1;
+        double v[9];
+        if (t < cnt) {
+            int sl;
+            double fac;
+            span_entry(s, sp.S, t, sl, fac);
+            key = sl * K + idx;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) v[c] = fdx[c] * fac;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) v[c] = 0.0;
+        }
+        warp_bin_add(arr, key, v);
+    }
+}
+
+// The bonded part of the slice stress profile on a sample step: one thread
+// per bond (CMonitor::AddBondStress, the bond's force on its head x the bond
+// vector, Monitor.cpp:2220-2470) and per bond pair (AddBondPairStress: the
+// segments first tail -> first head -> second head -> first tail with force
+// 0.33333333 (F[j+1] - F[j]), Monitor.cpp:2480-2755), the forces recomputed
+// as k_bonds computes them.  Threads [0, nbp) are bonds and [nbp, nbp + na)
+// bond pairs, nbp = nb rounded up to whole warps, so every warp runs one
+// kind of term and the span loops are warp-uniform.  A degenerate bond pair
+// adds zero, where the reference would reuse its last forces.
+static __global__ void __launch_bounds__(256) k_bonded_slices(int nb, int na, Topology topo)
+{
+    const SliceParams& sp = topo.sp;
+    const int nbp = (nb + 31) & ~31;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nbp) {
+        const bool live = k < nb;
+        double fdx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        SliceSpan s{0, 0, 0, 0, 0.0, 0.0, 0.0};
+        int type = 0;
+        if (live) {
+            double bv[3], g[3];
+            bond_force(topo, k, bv, g);
+            outer9(g, bv, fdx);
+            type = sp.bond_type[k];
+            s = slice_span(sp, sp.nbt, type, bv[2], topo.ubuf[topo.bond_h[k]].w, topo.ubuf[topo.bond_t[k]].w);
+        }
+        warp_span_add(sp, sp.bond, sp.nbt, type, s, fdx);
+    } else if (k < nbp + ((na + 31) & ~31)) {
+        const int a = k - nbp;
+        const bool live = a < na;
+        double U[4][3], FF[4][3], Z[4] = {0.0, 0.0, 0.0, 0.0};
+        int type = 0;
+        if (live) {
+            double G0[3], G2[3];
+            bondpair_force(topo, a, U[0], U[1], U[2], G0, G2);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                U[3][d] = U[0][d];
+                FF[0][d] = G0[d];
+                FF[1][d] = -G0[d] - G2[d];
+                FF[2][d] = G2[d];
+                FF[3][d] = G0[d];
+            }
+            Z[0] = topo.ubuf[topo.ang_b1t[a]].w;
+            Z[1] = topo.ubuf[topo.ang_b1h[a]].w;
+            Z[2] = topo.ubuf[topo.ang_b2h[a]].w;
+            Z[3] = Z[0];
+            type = sp.bondpair_type[a];
+        }
+        for (int j = 0; j < 3; ++j) {
+            double fdx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            SliceSpan s{0, 0, 0, 0, 0.0, 0.0, 0.0};
+            if (live) {
+                double dv[3], fo[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    dv[d] = U[j + 1][d] - U[j][d];
+                    fo[d] = 0.33333333 * (FF[j + 1][d] - FF[j][d]);
+                }
+                outer9(fo, dv, fdx);
+                s = slice_span(sp, sp.nbpt, type, dv[2], Z[j + 1], Z[j]);
+            }
+            warp_span_add(sp, sp.bondpair, sp.nbpt, type, s, fdx);
         }
     }
 }
@@ -872,9 +1052,9 @@ __global__ void __launch_bounds__(256, 4) k_update_mom(
 }
 
 // Sets the step counter that keys the pair noise (a launch argument, so the
-// host queues it without waiting for earlier work) and publishes the status
-// word of all work queued before it to `seen`, a word of mapped pinned host
-// memory that the host reads without waiting (dpd_engine_step).
+// host queues it without waiting for earlier work) when a call does not
+// continue where the previous one ended, and publishes the status word of
+// all work queued before it to `seen` (see publish_status).
 static __global__ void k_set_step(int64_t* __restrict__ step_ptr, int64_t value, const unsigned* __restrict__ status,
                                   unsigned* seen)
 {

@@ -34,7 +34,8 @@ namespace dpd {
 // miss.  Bins are block-private in shared memory when they fit (sbins) --
 // FP32 partial sums in a mixed-precision engine, FP64 in an FP64 engine --
 // and added once per block to the FP64 profile; else they go straight to
-// global memory.  Grid-stride loop over the tiles.
+// global memory.  Grid-stride loop over warps; each lane's beads lie in its
+// own 32nd of the box (see below).
 constexpr int kSliceBlock = 128;
 constexpr int kSliceHits = 32;   // list entries per lane before an evaluation pass
 
@@ -127,9 +128,16 @@ __global__ void __launch_bounds__(kSliceBlock) k_slice_pairs(
 #pragma unroll
         for (int q = 0; q < 10; ++q) { keys[q] = k; k += 0x9E3779B9u; }
     }
-    const int ntiles = (n + kSliceBlock - 1) / kSliceBlock;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int i = tile * kSliceBlock + threadIdx.x;
+    // Lane l of a warp takes its beads from the l-th 32nd of the slot range
+    // (slots are cell-sorted, z-major): the 32 lanes sit at 32 different
+    // heights and rarely add into the same slice bins at the same time, where
+    // the beads of one cell row would all meet on a few (shared-memory float
+    // atomics retry on every collision).
+    const int lane = threadIdx.x & 31;
+    const int P = (n + 31) / 32;
+    const int nwarps = gridDim.x * (kSliceBlock / 32);
+    for (int v = blockIdx.x * (kSliceBlock / 32) + (threadIdx.x >> 5); v < P; v += nwarps) {
+        const int i = lane * P + v;
         const bool live = i < n;
         V4 pi, vi;
         int cx = 0, cy = 0, cz = 0;

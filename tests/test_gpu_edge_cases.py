@@ -246,6 +246,21 @@ def test_renormalised_momenta_follow_the_reference(engine_mod, oracle_mod, preci
     assert eng.status() == 0
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_step_counter_follows_the_calls(engine_mod, oracle_mod, precision):
+    """The pair noise is keyed on the step: calls that continue where the
+    previous one ended and calls that name another step both draw the noise
+    of the steps they name (the device counter is set only on a jump)."""
+    s = W.binary_mixture(8)
+    eng, orc = _both(engine_mod, oracle_mod, s, precision)
+    for t0, k in ((1, 3), (4, 2), (50, 2), (52, 1), (7, 2)):
+        eng.step(t0, k)
+        orc.step(t0, k)
+    ftol = 1e-4 if precision == 0 else 1e-10
+    assert rel_err(eng.download()["f"], orc.state()["f"]) < ftol
+    assert eng.status() == 0
+
+
 def test_step_returns_the_fatal_status_without_waiting(engine_mod):
     """A non-finite state raised on the device is returned by a later
     dpd_engine_step (DPD_E_STATUS, no further work queued) without a
