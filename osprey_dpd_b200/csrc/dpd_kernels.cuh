@@ -542,64 +542,6 @@ __device__ __forceinline__ void outer9(const double f[3], const double d[3], dou
     o[6] = f[2] * d[0]; o[7] = f[2] * d[1]; o[8] = f[2] * d[2];
 }
 
-// Bins in FP64 (global, or block-private in an FP64 engine) or FP32
-// (block-private partial sums of a mixed-precision engine, added to the FP64
-// bins once per block).
-template <typename bin_t>
-__device__ __forceinline__ void slice_put(bin_t* arr, int K, int idx, int sl, const double fdx[9], double fac,
-                                          bool scale)
-{
-    bin_t* q = arr + ((size_t)sl * K + idx) * 9;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) atomicAdd(q + c, (bin_t)(scale ? fdx[c] * fac : fdx[c]));
-}
-
-// One contribution over the slices between two beads: za is the z of the
-// bead the separation points to (bead 1, bond head, bead j+1), zb the
-// other's, zDiff the separation's z component.  Same branch structure and
-// arithmetic as the reference's three functions.
-template <typename bin_t>
-__device__ __forceinline__ void slice_add(const SliceParams& sp, bin_t* arr, int K, int idx, const double fdx[9],
-                                          double zDiff, double za, double zb)
-{
-    double up, lo;
-    if (zDiff > 0.00001) {
-        up = za * sp.inv;
-        lo = zb * sp.inv;
-    } else if (zDiff < -0.00001) {
-        zDiff = -zDiff;
-        up = zb * sp.inv;
-        lo = za * sp.inv;
-    } else {
-        up = za * sp.inv;
-        lo = up;
-    }
-    const int S = sp.S;
-    int ui = (int)up;
-    const double ur = up - (double)ui;
-    int li = (int)lo;
-    const double lr = lo - (double)li;
-    if (ui < 0 || ui >= S || li < 0 || li >= S || idx < 0 || idx >= K) return;   // a z rounded up to L_z
-    if (ui == li) {
-        if (up != lo || ur > 0.00001) {
-            slice_put(arr, K, idx, li, fdx, 1.0, false);
-        } else {
-            slice_put(arr, K, idx, ui, fdx, 0.5, true);
-            if (--li < 0) li += S;
-            slice_put(arr, K, idx, li, fdx, 0.5, true);
-        }
-    } else {
-        const double inner = sp.width / zDiff;
-        if (ui > li) {
-            for (int k = li + 1; k <= ui - 1; ++k) slice_put(arr, K, idx, k, fdx, inner, true);
-        } else {
-            for (int kp = li + 1; kp <= S + ui - 1; ++kp) slice_put(arr, K, idx, kp >= S ? kp - S : kp, fdx, inner, true);
-        }
-        slice_put(arr, K, idx, li, fdx, lr > 0.000001 ? (1.0 - lr) * inner : inner, true);
-        if (ur > 0.000001) slice_put(arr, K, idx, ui, fdx, ur * inner, true);
-    }
-}
-
 struct Topology {
     const int* csr_ptr;     // per bead (upload index): first term
     const int* csr_term;    // term = index * 8 + code
@@ -740,11 +682,14 @@ __global__ void __launch_bounds__(256) k_bonds(int nbb, int n, const int* __rest
     }
 }
 
-// The slices one contribution spreads over, as slice_add visits them: kind 0
-// none (a z rounded up to L_z, or a type out of range), 1 one slice whole, 2
-// two halves (both beads on one slice face), 3 a span: `inner` slices
-// crossed whole (weight width/|dz|), then the lower end slice and, when
-// covered, the upper one.
+// The slices one contribution spreads over (CMonitor::AddBeadStress /
+// AddBondStress / AddBondPairStress, Monitor.cpp:2180-2755, with the same
+// branch structure and arithmetic): za is the z of the bead the separation
+// points to (bead 1, bond head, bead j+1), zb the other's, zDiff the
+// separation's z component.  kind 0: none (a z rounded up to L_z, or a type
+// out of range); 1: one slice whole; 2: two halves (both beads on one slice
+// face); 3: a span of `n_inner` slices crossed whole (weight width/|dz|),
+// then the lower end slice and, when covered, the upper one.
 struct SliceSpan {
     int kind, ui, li, n_inner;
     double ur, lr, inner;

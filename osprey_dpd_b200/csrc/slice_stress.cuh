@@ -16,7 +16,7 @@
 // used when |dz| <= 1e-5) is reproduced for every pair in different cells;
 // for a pair inside one cell the reference's order is its linked-list order,
 // and the engine takes the lower slot as bead 1.
-// SliceParams and the contour split itself (slice_add) live in
+// SliceParams and the contour split itself (slice_span, span_entry) live in
 // dpd_kernels.cuh, shared with the bonded kernel.
 #pragma once
 #include "pair_forces.cuh"
@@ -29,7 +29,7 @@ namespace dpd {
 // and lists the candidates inside the cut-off in its column of shared memory.
 // Evaluate: the lane takes its listed pairs, computes the DPD pair force of the
 // force kernels (same Philox draw) and splits force x separation over the
-// slices (slice_add).  Only listed pairs pay for the force and the split, so
+// slices (slice_span).  Only listed pairs pay for the force and the split, so
 // no lane idles through another's force work on the ~85 % of candidates that
 // miss.  Bins are block-private in shared memory when they fit (sbins) --
 // FP32 partial sums in a mixed-precision engine, FP64 in an FP64 engine --
@@ -50,8 +50,10 @@ __host__ __device__ constexpr size_t slice_smem_bytes(int S, int KT, bool sbins)
     return (sbins ? slice_bin_bytes<real>(S, KT) : 0) + sizeof(uint32_t) * (kSliceHits + 1) * kSliceBlock;
 }
 
-// The listed pairs of one lane: force, then its slices.  bins: the block's
-// shared bins (real) or the global FP64 profile.
+// The listed pairs of the warp's lanes, one pair per lane per iteration (the
+// loop runs to the longest list, so it is warp-uniform): the force, then the
+// slices it spreads over, every lane's adds to one slice issued together
+// (slice_span / span_entry).  Called by all 32 lanes.  bins: the block's shared bins (real) or the global FP64 profile.
 template <typename real, typename bin_t>
 __device__ __forceinline__ void slice_eval(int cnt, const uint32_t* __restrict__ list, int i, int n,
                                            const typename Vec4<real>::type& pi, const typename Vec4<real>::type& vi,
@@ -65,42 +67,61 @@ __device__ __forceinline__ void slice_eval(int cnt, const uint32_t* __restrict__
     const int m2 = nt * nt, KT = nt * nt;
     const int ti = real_bits(pi.w) & 0xFF;
     const uint32_t idi = (uint32_t)real_bits(vi.w);
-    for (int k = 0; k < cnt; ++k) {
-        const uint32_t e = list[k * kSliceBlock];
-        const int j = (int)(e & 0x03FFFFFFu);
-        const V4 pj = pos4[j];
-        const V4 vj = vel4[j];
-        real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
-        real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
-        real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
-        const real r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 < real(1) && r2 > real(1e-18))) continue;   // the test's rounding differs at the cut-off
-        const real inv = RealOps<real>::rsqrt(r2);
-        const real wr = real(1) - r2 * inv;
-        const int tj = real_bits(pj.w) & 0xFF;
-        const int tt = ti * nt + tj;
-        const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
-        const uint32_t idj = (uint32_t)real_bits(vj.w);
-        uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
-#pragma unroll
-        for (int q = 0; q < 10; ++q) {
-            const uint64_t prod = (uint64_t)0xD256D193u * c0;
-            c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
-            c1 = (uint32_t)prod;
-        }
-        const real ta = tab[tt], tg = tab[m2 + tt], ts = tab[2 * m2 + tt], noise = noise_centered(c0, real(0));
-        real m = (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv;
-        close_pair_fix(dx, dy, dz, m, r2, x, n, i, j, L, vi, vj, ta, tg, ts, noise);
-        const double f[3] = {(double)(m * dx), (double)(m * dy), (double)(m * dz)};
-        const double d[3] = {(double)dx, (double)dy, (double)dz};
+    const int trip = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    for (int k = 0; k < trip; ++k) {
         double fdx[9];
-        outer9(f, d, fdx);
-        slice_add(sp, bins, KT, tt, fdx, d[2], zi, x[2 * (size_t)n + j]);
+        SliceSpan s{0, 0, 0, 0, 0.0, 0.0, 0.0};
+        int tt = 0;
+        if (k < cnt) {
+            const uint32_t e = list[k * kSliceBlock];
+            const int j = (int)(e & 0x03FFFFFFu);
+            const V4 pj = pos4[j];
+            const V4 vj = vel4[j];
+            real dx = (pi.x - pj.x) - (real)((int)((e >> 26) & 3u) - 1) * wx;
+            real dy = (pi.y - pj.y) - (real)((int)((e >> 28) & 3u) - 1) * wy;
+            real dz = (pi.z - pj.z) - (real)((int)(e >> 30) - 1) * wz;
+            const real r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < real(1) && r2 > real(1e-18)) {   // the test's rounding differs at the cut-off
+                const real inv = RealOps<real>::rsqrt(r2);
+                const real wr = real(1) - r2 * inv;
+                const int tj = real_bits(pj.w) & 0xFF;
+                tt = ti * nt + tj;
+                const real rdotv = (dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z)) * inv;
+                const uint32_t idj = (uint32_t)real_bits(vj.w);
+                uint32_t c0 = min(idi, idj), c1 = max(idi, idj);
+#pragma unroll
+                for (int q = 0; q < 10; ++q) {
+                    const uint64_t prod = (uint64_t)0xD256D193u * c0;
+                    c0 = (uint32_t)(prod >> 32) ^ keys[q] ^ c1;
+                    c1 = (uint32_t)prod;
+                }
+                const real ta = tab[tt], tg = tab[m2 + tt], ts = tab[2 * m2 + tt],
+                           noise = noise_centered(c0, real(0));
+                real m = (ta * wr - tg * wr * wr * rdotv + ts * wr * noise) * inv;
+                close_pair_fix(dx, dy, dz, m, r2, x, n, i, j, L, vi, vj, ta, tg, ts, noise);
+                const double f[3] = {(double)(m * dx), (double)(m * dy), (double)(m * dz)};
+                const double d[3] = {(double)dx, (double)dy, (double)dz};
+                outer9(f, d, fdx);
+                s = slice_span(sp, KT, tt, d[2], zi, x[2 * (size_t)n + j]);
+            }
+        }
+        const int ms = span_count(s);
+        const int mt = (int)__reduce_max_sync(0xffffffffu, (unsigned)ms);
+        for (int t = 0; t < mt; ++t) {
+            if (t < ms) {
+                int sl;
+                double fac;
+                span_entry(s, sp.S, t, sl, fac);
+                bin_t* q = bins + ((size_t)sl * KT + tt) * 9;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) atomicAdd(q + c, (bin_t)(fdx[c] * fac));
+            }
+        }
     }
 }
 
 template <typename real>
-__global__ void __launch_bounds__(kSliceBlock) k_slice_pairs(
+__global__ void __launch_bounds__(kSliceBlock, 4) k_slice_pairs(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
