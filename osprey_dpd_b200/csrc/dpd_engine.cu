@@ -759,6 +759,7 @@ static int create_impl(const dpd_params* p, int32_t nboxes, const dpd_box* bx, d
         for (int d = 0; d < 3; ++d) b.L[d] = (double)b.nc[d] * b.w[d];
         b.cell_base = (int)base;
         b.seed = bx[k].seed;
+        set_cell_division(b);
         base += (int64_t)b.nc[0] * b.nc[1] * b.nc[2];
         e->hboxes.push_back(b);
         e->box_a.insert(e->box_a.end(), bx[k].a, bx[k].a + m);

@@ -77,7 +77,39 @@ struct Box {
     uint64_t seed;     // pair-noise seed of this box
     int tab;           // offset of this box's pair tables (3 * ntypes^2 reals)
     int pad;
+    double iw[3];      // 1 / w
+    // division of a box-local cell index c < 2^31 by nx and by nx*ny as a
+    // multiply and shift (set_cell_division)
+    unsigned long long mx, mxy;
+    int kx, kxy;
 };
+
+// Division by an invariant integer d (1 <= d < 2^31) for numerators below
+// 2^31 as floor(c * m / 2^k), k = 31 + ceil(log2 d), m = ceil(2^k / d)
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, with N = 31 numerator bits): exact, since
+// c * (m d - 2^k) / (d 2^k) < 1/d.
+__host__ __device__ inline void division_magic(unsigned d, unsigned long long& m, int& k)
+{
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    k = 31 + l;
+    m = ((1ull << k) + d - 1) / d;
+}
+inline void set_cell_division(Box& b)
+{
+    division_magic((unsigned)b.nc[0], b.mx, b.kx);
+    division_magic((unsigned)b.nc[0] * (unsigned)b.nc[1], b.mxy, b.kxy);
+    for (int d = 0; d < 3; ++d) b.iw[d] = 1.0 / b.w[d];
+}
+// Cell coordinates (ix, iy, iz) of box-local cell index cl = nx*(ny*iz+iy)+ix.
+__device__ __forceinline__ void cell_coords(const Box& B, int cl, int ci[3])
+{
+    const int q = (int)(((unsigned long long)(unsigned)cl * B.mx) >> B.kx);     // cl / nx
+    ci[2] = (int)(((unsigned long long)(unsigned)cl * B.mxy) >> B.kxy);         // cl / (nx ny)
+    ci[0] = cl - q * B.nc[0];
+    ci[1] = q - ci[2] * B.nc[1];
+}
 
 // Bead flags word: type in bits 0..7, box in bits 8..23, frozen (never
 // moves) in bit 24, has bond or bond-pair terms in bit 25.  The force
@@ -124,7 +156,8 @@ __device__ __forceinline__ int drift_and_move(const StepConst* __restrict__ K, c
     const Box& B = boxes[flag_box(tfl)];
     const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
     const int cl = c - B.cell_base;
-    int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
+    int ci[3];
+    cell_coords(B, cl, ci);
     const bool ext = ci[0] == 0 || ci[0] == nx - 1 || ci[1] == 0 || ci[1] == ny - 1 ||
                      ci[2] == 0 || ci[2] == nz - 1;
     double xn[3];
@@ -159,11 +192,18 @@ __device__ __forceinline__ int drift_and_move(const StepConst* __restrict__ K, c
         }
         cnew = B.cell_base + nci[0] + nx * (nci[1] + ny * nci[2]);
     }
-    // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650)
-    const long long ax = (long long)(xn[0] / B.w[0]);
-    const long long ay = (long long)(xn[1] / B.w[1]);
-    const long long az = (long long)(xn[2] / B.w[2]);
-    if (B.cell_base + (long long)nx * ((long long)ny * az + ay) + ax != cnew) bad |= 0x1u;
+    // CCNTCell::CheckBeadsinCell audit (CNTCell.cpp:2636-2650), run by the
+    // reference after every step (SimBox.cpp:1322): (long)(x / w) per axis,
+    // from x * (1/w) (within 2 ulp of x / w) except within 1e-9 of a cell
+    // face, where the truncation could differ and the division is done
+    long long a[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double q = xn[d] * B.iw[d];
+        a[d] = (long long)q;
+        if (fabs(q - rint(q)) < 1e-9) a[d] = (long long)(xn[d] / B.w[d]);
+    }
+    if (B.cell_base + (long long)nx * ((long long)ny * a[2] + a[1]) + a[0] != cnew) bad |= 0x1u;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (!isfinite(xn[d])) bad |= 0x2u;
@@ -363,9 +403,8 @@ __global__ void __launch_bounds__(256, 6) k_gather(
         o = beg + k;
     }
     const Box& B = boxes[flag_box(tfl)];
-    const int nx = B.nc[0], ny = B.nc[1];
-    const int cl = c - B.cell_base;
-    const int ci[3] = {cl % nx, (cl / nx) % ny, cl / (nx * ny)};
+    int ci[3];
+    cell_coords(B, c - B.cell_base, ci);
     const bool frozen = flag_frozen(tfl);
     real rel[3], vt[3];
 #pragma unroll

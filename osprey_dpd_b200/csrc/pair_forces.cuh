@@ -252,9 +252,11 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
     if (live) {
         const int c = cell[i] - B.cell_base;
-        cx = c % nx;
-        cy = (c / nx) % ny;
-        cz = c / (nx * ny);
+        int cc[3];
+        cell_coords(B, c, cc);
+        cx = cc[0];
+        cy = cc[1];
+        cz = cc[2];
     }
     const real* T = MULTI ? tab + B.tab : Tsh;
     uint32_t keys[10];
@@ -607,9 +609,11 @@ __device__ __forceinline__ void half_shell_tile_lanes(
         const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
         if (live) {
             const int c = cell[i] - B.cell_base;
-            cx = c % nx;
-            cy = (c / nx) % ny;
-            cz = c / (nx * ny);
+            int cc[3];
+            cell_coords(B, c, cc);
+            cx = cc[0];
+            cy = cc[1];
+            cz = cc[2];
         }
         const real* T = MULTI ? tab + B.tab : Tsh;
         uint32_t keys[10];
@@ -788,9 +792,11 @@ __device__ __forceinline__ void half_shell_tile(
     const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
     if (live) {
         const int c = cell[i] - B.cell_base;
-        cx = c % nx;
-        cy = (c / nx) % ny;
-        cz = c / (nx * ny);
+        int cc[3];
+        cell_coords(B, c, cc);
+        cx = cc[0];
+        cy = cc[1];
+        cz = cc[2];
     }
     sh.hpos[threadIdx.x] = pi;
     sh.hvel[threadIdx.x] = vi;

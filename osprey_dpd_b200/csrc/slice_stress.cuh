@@ -167,9 +167,11 @@ __global__ void __launch_bounds__(kSliceBlock, 4) k_slice_pairs(
             pi = pos4[i];
             vi = vel4[i];
             const int c = cell[i] - B.cell_base;
-            cx = c % nx;
-            cy = (c / nx) % ny;
-            cz = c / (nx * ny);
+            int cc[3];
+            cell_coords(B, c, cc);
+            cx = cc[0];
+            cy = cc[1];
+            cz = cc[2];
             zi = x[2 * (size_t)n + i];
         } else {
             pi.x = pi.y = pi.z = pi.w = vi.x = vi.y = vi.z = vi.w = real(0);
