@@ -174,6 +174,9 @@ struct dpd_engine {
     // (each step's k_update_mom advances it); INT64_MIN: unknown
     int64_t dev_step = INT64_MIN;
     double* h_obs = nullptr;
+    // pinned staging for the host-built topology arrays (grown as needed)
+    unsigned char* h_stage = nullptr;
+    size_t cap_h_stage = 0;
     bool obs_valid = false;
     bool obs_has_virial = false;
     int64_t sample_period = 0;      // 0: sample at the last step of every call
@@ -858,6 +861,7 @@ void dpd_engine_destroy(dpd_engine* e)
     e->allocations.clear();
     if (e->h_status) cudaFreeHost(e->h_status);
     if (e->h_obs) cudaFreeHost(e->h_obs);
+    if (e->h_stage) cudaFreeHost(e->h_stage);
     if (e->h_seen) cudaFreeHost(e->h_seen);
     if (e->side) cudaStreamSynchronize(e->side);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -1300,6 +1304,37 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
     const int64_t n = e->n;
+    // The device arrays are built on the host in one pinned staging buffer
+    // and copied asynchronously; the call waits once, at the end.
+    const size_t nterm = (size_t)(2 * nb + 3 * na);
+    if (nb * 2 + na * 3 > ((int64_t)1 << 28)) return fail(e, DPD_E_ARG, "topology too large");
+    auto words = [](size_t k, size_t w) { return (k * w + 15) / 16 * 16; };   // 16-byte aligned pieces
+    const size_t stage = words(2 * (size_t)nb, 4) + words(2 * (size_t)nb, 8) + words(4 * (size_t)na, 4) +
+                         words(3 * (size_t)na, 8) + words((size_t)n + 1, 4) + words(nterm, 4) + words((size_t)n, 4);
+    if (stage > e->cap_h_stage) {
+        if (e->h_stage) cudaFreeHost(e->h_stage);
+        e->h_stage = nullptr;
+        e->cap_h_stage = 0;
+        if (cudaHostAlloc((void**)&e->h_stage, stage, cudaHostAllocDefault) != cudaSuccess) {
+            e->h_stage = nullptr;
+            return fail(e, DPD_E_CUDA, "pinned staging allocation failed");
+        }
+        e->cap_h_stage = stage;
+    }
+    unsigned char* arena = e->h_stage;
+    auto carve = [&](size_t k, size_t w) {
+        unsigned char* q = arena;
+        arena += words(k, w);
+        return q;
+    };
+    int* bh = reinterpret_cast<int*>(carve(2 * (size_t)nb, 4));
+    int* bt = bh + nb;
+    double* bk = reinterpret_cast<double*>(carve(2 * (size_t)nb, 8));   // k2, then l0
+    int* a4 = reinterpret_cast<int*>(carve(4 * (size_t)na, 4));          // four planes of na
+    double* ak = reinterpret_cast<double*>(carve(3 * (size_t)na, 8));    // k3, cos(phi0), sin(phi0)
+    int* cnt = reinterpret_cast<int*>(carve((size_t)n + 1, 4));
+    int* terms = reinterpret_cast<int*>(carve(nterm, 4));
+    int* bbl = reinterpret_cast<int*>(carve((size_t)n, 4));
     // bead id -> upload index (the ids kept from the bead upload)
     const std::vector<int64_t>& hpid = e->h_id;
     bool identity = true;
@@ -1314,69 +1349,67 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         const auto it = by_id.find(idv);
         return it == by_id.end() ? -1 : it->second;
     };
-    std::vector<int> bh(nb), bt(nb);
     for (int64_t i = 0; i < nb; ++i) {
         bh[i] = index_of(bond_head_id[i]);
         bt[i] = index_of(bond_tail_id[i]);
         if (bh[i] < 0 || bt[i] < 0) return fail(e, DPD_E_ARG, "bond refers to an unknown bead id");
         if (bh[i] == bt[i]) return fail(e, DPD_E_ARG, "bond joins a bead to itself");
+        bk[i] = k2[i];
+        bk[nb + i] = l0[i];
     }
-    std::vector<int> a4[4];
-    for (auto& v : a4) v.resize(na);
-    std::vector<double> acos0(na), asin0(na);
     for (int64_t i = 0; i < na; ++i) {
         if (first_bond[i] < 0 || first_bond[i] >= nb || second_bond[i] < 0 || second_bond[i] >= nb)
             return fail(e, DPD_E_ARG, "bond pair refers to an unknown bond");
-        a4[0][i] = bh[first_bond[i]];
-        a4[1][i] = bt[first_bond[i]];
-        a4[2][i] = bh[second_bond[i]];
-        a4[3][i] = bt[second_bond[i]];
+        a4[i] = bh[first_bond[i]];
+        a4[na + i] = bt[first_bond[i]];
+        a4[2 * na + i] = bh[second_bond[i]];
+        a4[3 * na + i] = bt[second_bond[i]];
         // CBondPair ctor caches cos/sin of phi0; the phi0 > 0 branch of
         // BondPair.cpp:178-188 is selected by sin0 != 0
-        acos0[i] = phi0[i] > 0.0 ? std::cos(phi0[i]) : 1.0;
-        asin0[i] = phi0[i] > 0.0 ? std::sin(phi0[i]) : 0.0;
+        ak[i] = k3[i];
+        ak[na + i] = phi0[i] > 0.0 ? std::cos(phi0[i]) : 1.0;
+        ak[2 * na + i] = phi0[i] > 0.0 ? std::sin(phi0[i]) : 0.0;
     }
     // per-bead term lists (CSR by upload index); terms in bond order then pair order
-    std::vector<int> cnt(n + 1, 0);
+    std::fill(cnt, cnt + n + 1, 0);
     for (int64_t i = 0; i < nb; ++i) { cnt[bh[i] + 1]++; cnt[bt[i] + 1]++; }
-    for (int64_t i = 0; i < na; ++i) { cnt[a4[1][i] + 1]++; cnt[a4[0][i] + 1]++; cnt[a4[2][i] + 1]++; }
+    for (int64_t i = 0; i < na; ++i) { cnt[a4[na + i] + 1]++; cnt[a4[i] + 1]++; cnt[a4[2 * na + i] + 1]++; }
     for (int64_t b = 0; b < n; ++b) cnt[b + 1] += cnt[b];
-    std::vector<int> fillp(cnt.begin(), cnt.end() - 1), terms(cnt[n]);
-    if (nb * 2 + na * 3 > ((int64_t)1 << 28)) return fail(e, DPD_E_ARG, "topology too large");
+    std::vector<int> fillp(cnt, cnt + n);
     for (int64_t i = 0; i < nb; ++i) {
         terms[fillp[bh[i]]++] = (int)(i * 8 + kBondHead);
         terms[fillp[bt[i]]++] = (int)(i * 8 + kBondTail);
     }
     for (int64_t i = 0; i < na; ++i) {
-        terms[fillp[a4[1][i]]++] = (int)(i * 8 + kAngle0);   // first bond's tail: force [0]
-        terms[fillp[a4[0][i]]++] = (int)(i * 8 + kAngle1);   // middle bead:       force [1]
-        terms[fillp[a4[2][i]]++] = (int)(i * 8 + kAngle2);   // second bond's head: force [2]
+        terms[fillp[a4[na + i]]++] = (int)(i * 8 + kAngle0);    // first bond's tail: force [0]
+        terms[fillp[a4[i]]++] = (int)(i * 8 + kAngle1);         // middle bead:       force [1]
+        terms[fillp[a4[2 * na + i]]++] = (int)(i * 8 + kAngle2);  // second bond's head: force [2]
     }
+    int64_t nbl = 0;
+    for (int64_t b = 0; b < n; ++b)
+        if (cnt[b + 1] > cnt[b]) bbl[nbl++] = (int)b;
     bool moved = false;
     int rc;
-    std::vector<int> bbl;
-    for (int64_t b = 0; b < n; ++b)
-        if (cnt[b + 1] > cnt[b]) bbl.push_back((int)b);
-    if (!bbl.empty()) {
+    cudaStream_t st = e->s();
+    if (nbl) {
         if ((rc = ensure(e, &e->d_ubuf, e->cap_ubuf, (size_t)n, &moved))) return rc;
         if ((rc = ensure(e, &e->d_Fb, e->cap_Fb, (size_t)n, &moved))) return rc;
         if ((rc = ensure(e, &e->d_Sb, e->cap_Sb, 9 * (size_t)n, &moved))) return rc;
-        if ((rc = ensure(e, &e->d_bb, e->cap_bb, bbl.size(), &moved))) return rc;
-        CU(cudaMemcpy(e->d_bb, bbl.data(), bbl.size() * sizeof(int), cudaMemcpyHostToDevice));
+        if ((rc = ensure(e, &e->d_bb, e->cap_bb, (size_t)nbl, &moved))) return rc;
+        CU(cudaMemcpyAsync(e->d_bb, bbl, (size_t)nbl * sizeof(int), cudaMemcpyHostToDevice, st));
     }
-    if ((int64_t)bbl.size() != e->nbb) drop_graphs(e);   // the bonded branch appears or changes size
-    e->nbb = (int64_t)bbl.size();
+    if (nbl != e->nbb) drop_graphs(e);   // the bonded branch appears or changes size
+    e->nbb = nbl;
     if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)n + 1, &moved))) return rc;
-    if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, terms.size(), &moved))) return rc;
-    CU(cudaMemcpy(e->d_csr_ptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice));
-    if (!terms.empty()) CU(cudaMemcpy(e->d_csr_term, terms.data(), terms.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, nterm, &moved))) return rc;
+    CU(cudaMemcpyAsync(e->d_csr_ptr, cnt, ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (nterm) CU(cudaMemcpyAsync(e->d_csr_term, terms, nterm * sizeof(int), cudaMemcpyHostToDevice, st));
     // mark the beads that have terms (kFlagBonded) so k_update_mom skips the
     // topology lookup for all others, and k_gather writes their unPBC
     // position into the FP64 buffer the bonded terms read
-    k_mark_bonded<<<blocks_for(n, kThreads), kThreads, 0, e->s()>>>((int)n, e->d_bid[e->cur], e->d_csr_ptr,
-                                                                    e->d_tf[e->cur]);
+    k_mark_bonded<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, e->d_bid[e->cur], e->d_csr_ptr,
+                                                                e->d_tf[e->cur]);
     if ((rc = check_launch(e, "k_mark_bonded"))) return rc;
-    CU(cudaStreamSynchronize(e->s()));
     if (nb) {
         size_t c = e->cap_bond;
         if ((rc = ensure(e, &e->d_bond_h, c, nb, &moved))) return rc;
@@ -1387,17 +1420,17 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         c = e->cap_bond;
         if ((rc = ensure(e, &e->d_bond_l0, c, nb, &moved))) return rc;
         e->cap_bond = std::max(e->cap_bond, (size_t)nb);
-        CU(cudaMemcpy(e->d_bond_h, bh.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->d_bond_t, bt.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->d_bond_k2, k2, nb * sizeof(double), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->d_bond_l0, l0, nb * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(e->d_bond_h, bh, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(e->d_bond_t, bt, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(e->d_bond_k2, bk, nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(e->d_bond_l0, bk + nb, nb * sizeof(double), cudaMemcpyHostToDevice, st));
     }
     if (na) {
         const size_t c0 = e->cap_ang;
         for (int k = 0; k < 4; ++k) {
             size_t c = c0;
             if ((rc = ensure(e, &e->d_ang[k], c, na, &moved))) return rc;
-            CU(cudaMemcpy(e->d_ang[k], a4[k].data(), na * sizeof(int), cudaMemcpyHostToDevice));
+            CU(cudaMemcpyAsync(e->d_ang[k], a4 + k * na, na * sizeof(int), cudaMemcpyHostToDevice, st));
         }
         size_t c = c0;
         if ((rc = ensure(e, &e->d_ang_k3, c, na, &moved))) return rc;
@@ -1406,11 +1439,12 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         c = c0;
         if ((rc = ensure(e, &e->d_ang_sin0, c, na, &moved))) return rc;
         e->cap_ang = std::max(c0, (size_t)na);
-        CU(cudaMemcpy(e->d_ang_k3, k3, na * sizeof(double), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->d_ang_cos0, acos0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->d_ang_sin0, asin0.data(), na * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(e->d_ang_k3, ak, na * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(e->d_ang_cos0, ak + na, na * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(e->d_ang_sin0, ak + 2 * na, na * sizeof(double), cudaMemcpyHostToDevice, st));
         e->h_ang_phi0.assign(phi0, phi0 + na);
     }
+    CU(cudaStreamSynchronize(st));   // the staging buffer is reused by the next call
     e->topo_nb = nb;
     e->topo_na = na;
     e->mon_set = false;   // the monitor's bond types refer to the previous topology
