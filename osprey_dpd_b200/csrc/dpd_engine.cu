@@ -115,6 +115,11 @@ struct dpd_engine {
     // slice stress profile (CMonitor::AddBeadStress & co.), built on sample steps
     int slice_S = 0, slice_nbt = 0, slice_nbpt = 0;
     double* d_slice = nullptr;            // pair | bond | bondpair bins, one allocation
+    // the profile's pair list (kSliceListPerBead entries a bead) and its counters
+    uint2* d_slice_list = nullptr;
+    unsigned* d_slice_cnt = nullptr;
+    double* d_slice_part = nullptr;      // k_slice_eval's per-block partial sums
+    size_t cap_slice_list = 0, cap_slice_cnt = 0, cap_slice_part = 0;
     size_t cap_slice = 0;
     int* d_slice_bt = nullptr;            // bond type per bond
     int* d_slice_bpt = nullptr;           // bond-pair type per bond pair
@@ -619,9 +624,31 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         const int sb = slice_smem_bytes<real>(e->slice_S, KT, true) <= kSliceSmemMax;
         const size_t smem = slice_smem_bytes<real>(e->slice_S, KT, sb != 0);
         Timed t(e, DPD_KERNEL_SLICES);
+        // pairs listed by the test, then evaluated from the list; the
+        // one-kernel form runs instead when the list cannot hold them
+        const SliceList L{e->d_slice_list, e->d_slice_cnt, (int)std::min<size_t>(e->cap_slice_list, INT_MAX)};
+        const bool listed = e->d_slice_list && e->cap_slice_list >= (size_t)kSliceListPerBead * (size_t)n;
+        if (listed) {
+            CU(cudaMemsetAsync(e->d_slice_cnt, 0, 2 * sizeof(unsigned), st));
+            CU(launch_step(e, k_slice_pairs<real>, e->sms * 4, kSliceBlock, slice_smem_bytes<real>(e->slice_S, KT, false),
+                           st, n, e->d_K, e->d_boxes, e->d_step, (const real*)e->d_tab, e->d_cell[b], e->d_start,
+                           (const V4*)e->d_pos4, (const V4*)e->d_vel4, (const double*)e->d_x[b], sp, 0, L,
+                           (int)kSliceList));
+            if ((rc = check_launch(e, "k_slice_pairs"))) return rc;
+            const int nbins = e->slice_S * KT * 9;
+            const int eblocks = e->sms * kSliceEvalBlocksPerSM;
+            CU(launch_step(e, k_slice_eval<real>, eblocks, kSliceEvalBlock,
+                           slice_eval_smem_bytes<real>(e->slice_S, KT, sb != 0), st, n, e->d_K, e->d_boxes, e->d_step,
+                           (const real*)e->d_tab, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
+                           (const double*)e->d_x[b], sp, sb, L, (real*)e->d_slice_part));
+            if ((rc = check_launch(e, "k_slice_eval"))) return rc;
+            CU(launch_step(e, k_slice_sum<real>, blocks_for(nbins, 32), 256, 0, st, nbins, sb ? eblocks : 0,
+                           (const real*)e->d_slice_part, (const unsigned*)e->d_slice_cnt, sp.pair));
+            if ((rc = check_launch(e, "k_slice_sum"))) return rc;
+        }
         CU(launch_step(e, k_slice_pairs<real>, e->sms * 4, kSliceBlock, smem, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
-                       (const double*)e->d_x[b], sp, sb));
+                       (const double*)e->d_x[b], sp, sb, L, (int)(listed ? kSliceFallback : kSliceOne)));
         if ((rc = check_launch(e, "k_slice_pairs"))) return rc;
         e->slice_sampled = true;
     }
@@ -1490,12 +1517,28 @@ int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t nbondtyp
         CU(cudaMemcpy(e->d_slice_bpt, bondpair_type, sizeof(int) * e->topo_na, cudaMemcpyHostToDevice));
     }
     CU(cudaMemset(e->d_slice, 0, slice_bins(e) * sizeof(double)));
+    // the pair list (best effort: without it the profile is built by one kernel)
+    if (ensure(e, &e->d_slice_list, e->cap_slice_list, (size_t)kSliceListPerBead * (size_t)e->n, &moved) != DPD_OK ||
+        ensure(e, &e->d_slice_cnt, e->cap_slice_cnt, 2, &moved) != DPD_OK ||
+        ensure(e, &e->d_slice_part, e->cap_slice_part,
+               (size_t)e->sms * kSliceEvalBlocksPerSM * (size_t)nslices * e->ntypes * e->ntypes * 9, &moved) !=
+            DPD_OK) {
+        dfree(e, e->d_slice_list);
+        e->d_slice_list = nullptr;
+        e->cap_slice_list = 0;
+    }
     // dynamic shared memory of the pair part: bins (when they fit) and hit lists
     const int KT = e->ntypes * e->ntypes;
-    const size_t sf = slice_smem_bytes<float>(nslices, KT, slice_smem_bytes<float>(nslices, KT, true) <= kSliceSmemMax);
-    const size_t sd = slice_smem_bytes<double>(nslices, KT, slice_smem_bytes<double>(nslices, KT, true) <= kSliceSmemMax);
-    CU(cudaFuncSetAttribute(k_slice_pairs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf));
-    CU(cudaFuncSetAttribute(k_slice_pairs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sd));
+    const bool bf = slice_smem_bytes<float>(nslices, KT, true) <= kSliceSmemMax;
+    const bool bd = slice_smem_bytes<double>(nslices, KT, true) <= kSliceSmemMax;
+    CU(cudaFuncSetAttribute(k_slice_pairs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)slice_smem_bytes<float>(nslices, KT, bf)));
+    CU(cudaFuncSetAttribute(k_slice_pairs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)slice_smem_bytes<double>(nslices, KT, bd)));
+    CU(cudaFuncSetAttribute(k_slice_eval<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)slice_eval_smem_bytes<float>(nslices, KT, bf)));
+    CU(cudaFuncSetAttribute(k_slice_eval<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)slice_eval_smem_bytes<double>(nslices, KT, bd)));
     return DPD_OK;
 }
 
