@@ -18,6 +18,9 @@ SYSTEMS = {
     "binary": (lambda: W.binary_mixture(cells=(8, 9, 10)), 10),
     "bilayer": (lambda: W.bilayer(cells=(12, 12, 12), nlipids=60, with_htt=True, phi0_deg=30.0), 24),
     "polymer": (lambda: W.polymer_solution(cells=(12, 12, 12)), 6),
+    # density 10: ~21 pairs a bead, more than the engine's pair list holds
+    # (16 a bead), so the profile is built by its one-kernel fallback
+    "water_dense": (lambda: W.water(5, density=10.0), 5),
 }
 
 
