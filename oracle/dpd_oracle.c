@@ -1,6 +1,6 @@
 /* dpd_oracle.c -- CPU restatement of Osprey-DPD's per-timestep DPD loop.
  *
- * TEST INFRASTRUCTURE ONLY (the checker).  See dpd_oracle.h for the list of
+ * TEST INFRASTRUCTURE ONLY (the oracle).  See dpd_oracle.h for the list of
  * reference functions restated here.  The code keeps the reference's data
  * structures where they fix the floating-point operation order: one doubly
  * linked bead list per CNT cell with push_front insertion, cells visited in

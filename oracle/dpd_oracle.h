@@ -1,6 +1,6 @@
 /* dpd_oracle.h -- CPU restatement of Osprey-DPD's per-timestep DPD loop.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA engine is compared
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle the CUDA engine is compared
  * against; the engine never links, loads or calls it.
  *
  * It restates, in plain C and in the reference's own operation order:

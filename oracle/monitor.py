@@ -1,5 +1,5 @@
 """numpy restatement of the reference's CMonitor sample data, applied to a
-state (positions, unPBC positions) -- the checker for dpd_engine_monitor.
+state (positions, unPBC positions) -- the oracle for dpd_engine_monitor.
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, never by the engine.
 

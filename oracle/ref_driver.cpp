@@ -1,6 +1,6 @@
 // ref_driver.cpp -- test harness around the UNMODIFIED Osprey-DPD reference.
 //
-// This file is test infrastructure (the checker), never part of the engine.
+// This file is test infrastructure (it pins the oracle to the reference), never part of the engine.
 // It is linked against the reference's own objects, compiled from the
 // reference's src/*.cpp by oracle/Makefile, and drives the reference through
 // its public classes exactly as CSimulation::Initialize/Run do

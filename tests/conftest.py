@@ -1,6 +1,6 @@
 """Shared test set-up: markers, import paths and small systems.
 
-The CPU oracle (oracle/) is the checker for every parity test; it is imported
+The CPU oracle (oracle/) is the oracle of every parity test; it is imported
 only here and in the tests."""
 import os
 import sys
