@@ -94,7 +94,11 @@ struct dpd_engine {
     uint32_t* d_up_img = nullptr;
     double* d_up_off = nullptr;
     int* d_up_perm = nullptr;
-    int* d_up_err = nullptr;
+    int* d_up_err = nullptr;           // error slots, residual flag, changed bits, type counts
+    int64_t* d_prev_id = nullptr;      // ids and types of the last upload (upload order)
+    int* d_prev_type = nullptr;
+    size_t cap_prev_id = 0, cap_prev_type = 0;
+    int64_t prev_n = -1;               // bead count whose d_prev_* hold a complete upload (-1: none)
     size_t cap_up_cell = 0, cap_up_img = 0, cap_up_off = 0, cap_up_perm = 0, cap_up_err = 0;
     bool ahead_enabled = true;
     bool pdl = true;             // programmatic dependent launch of the step kernels
@@ -130,6 +134,16 @@ struct dpd_engine {
     std::vector<int64_t> type_count;      // beads per type at the last upload
     std::vector<int64_t> h_id;            // bead ids and types by upload index (restart files)
     std::vector<int32_t> h_type;
+    uint64_t ids_version = 0;             // advanced when an upload brings other bead ids
+    // the inputs of the last topology build, which the staging buffer still
+    // holds: an identical upload for the same bead ids reuses it
+    struct TopoInputs {
+        std::vector<int64_t> bh, bt, f, sc;
+        std::vector<double> k2, l0, k3, phi0;
+        uint64_t ids_version = ~0ull;
+        int64_t n = 0, nbl = 0;
+        bool valid = false;
+    } topo_in;
     // restart-file layout: file order of the beads (upload indices), their polymer id and type
     std::vector<int64_t> rs_order, rs_poly_id;
     std::vector<int32_t> rs_poly_type;
@@ -722,6 +736,7 @@ void release_topology(dpd_engine* e)
     double** dp[] = {&e->d_bond_k2, &e->d_bond_l0, &e->d_ang_k3, &e->d_ang_cos0, &e->d_ang_sin0};
     for (auto q : dp) { dfree(e, *q); *q = nullptr; }
     e->cap_csr_ptr = e->cap_csr_term = e->cap_bond = e->cap_ang = 0;
+    e->topo_in.valid = false;
 }
 
 // Empty topology: csr_ptr all zero.  With keep_bonded (same bead count as
@@ -738,6 +753,7 @@ int empty_topology(dpd_engine* e, bool keep_bonded)
         drop_graphs(e);
         e->nbb = 0;
     }
+    if (moved || !keep_bonded) e->topo_in.valid = false;
     e->topo_nb = e->topo_na = 0;
     return DPD_OK;
 }
@@ -997,7 +1013,11 @@ static int stage_buffers(dpd_engine* e, int64_t n)
     if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, (size_t)n, &smoved))) return rc;
     if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * (size_t)n, &smoved))) return rc;
     if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 1, &smoved))) return rc;
+    if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 2 + kMaxTypes, &smoved))) return rc;
+    bool pmoved = false;
+    if ((rc = ensure(e, &e->d_prev_id, e->cap_prev_id, (size_t)n, &pmoved))) return rc;
+    if ((rc = ensure(e, &e->d_prev_type, e->cap_prev_type, (size_t)n, &pmoved))) return rc;
+    if (pmoved) e->prev_n = -1;
     return DPD_OK;
 }
 
@@ -1048,16 +1068,24 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     int rc;
     // validation and binning (CSimBox::AssignBeadstoCells, SimBox.cpp:715-762:
     // ix = (long)(x/w), box-local coordinates); nothing of the state changes yet
-    int herr[kUpErrors + 1];
+    // herr: the first bead of each error kind, any residual unPBC offset,
+    // the bits of ids / types that differ from the previous upload, and the
+    // beads per type
+    int herr[kUpErrors + 2 + kMaxTypes];
     for (int k = 0; k < kUpErrors; ++k) herr[k] = INT_MAX;
-    herr[kUpErrors] = 0;   // any residual unPBC offset
+    for (int k = kUpErrors; k < kUpErrors + 2 + kMaxTypes; ++k) herr[k] = 0;
     CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
+    const UploadPrev prev{e->d_prev_id, e->d_prev_type, reinterpret_cast<unsigned*>(e->d_up_err + kUpErrors + 1),
+                          e->d_up_err + kUpErrors + 2};
+    const bool prev_ok = e->prev_n == n;   // d_prev_* hold the last complete upload of n beads
     k_up_check<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, (int)e->hboxes.size(), e->ntypes, e->d_boxes, in,
                                                             e->d_up_cell, e->d_up_img, e->d_up_off, e->d_count,
-                                                            e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors);
+                                                            e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors,
+                                                            prev);
     if ((rc = check_launch(e, "k_up_check"))) return rc;
     CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
+    e->prev_n = -1;   // d_prev_* now hold this upload, complete only once it succeeds
     int bad = INT_MAX, kind = -1;
     for (int k = 0; k < kUpErrors; ++k)
         if (herr[k] < bad) { bad = herr[k]; kind = k; }
@@ -1150,15 +1178,21 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     e->off_active = any_off;
     CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)n, st));
     CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
+    // host copies of ids and types, refreshed only when the device saw them
+    // change; beads per type counted by k_up_check
+    const unsigned changed = prev_ok ? (unsigned)herr[kUpErrors + 1] : 3u;
+    e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
+    if ((changed & 1u) || e->h_id.size() != (size_t)n) {
+        e->h_id.assign(id, id + n);
+        ++e->ids_version;
+    }
+    if ((changed & 2u) || e->h_type.size() != (size_t)n) e->h_type.assign(type, type + n);
     CU(cudaStreamSynchronize(st));
     *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine is in flight after the sync
     rc = empty_topology(e, same_n);
     if (rc) return rc;
     e->uploaded = true;
-    e->type_count.assign((size_t)e->ntypes, 0);
-    for (int64_t b = 0; b < n; ++b) e->type_count[(size_t)type[b]]++;
-    e->h_id.assign(id, id + n);
-    e->h_type.assign(type, type + n);
+    e->prev_n = n;
     e->rs_order.clear();   // the restart layout refers to the old beads
     e->mon_set = false;   // the monitor's polymers and initial positions refer to the old beads
     e->stepped = false;
@@ -1362,6 +1396,23 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     int* cnt = reinterpret_cast<int*>(carve((size_t)n + 1, 4));
     int* terms = reinterpret_cast<int*>(carve(nterm, 4));
     int* bbl = reinterpret_cast<int*>(carve((size_t)n, 4));
+    // The same topology for the same bead ids as the last build: the staging
+    // buffer still holds that build, so only the copies are made again (a
+    // bead upload clears the term offsets and the bonded flags).
+    dpd_engine::TopoInputs& tin = e->topo_in;
+    auto same_i = [](const std::vector<int64_t>& v, const int64_t* q, int64_t k) {
+        return (int64_t)v.size() == k && (k == 0 || memcmp(v.data(), q, sizeof(int64_t) * (size_t)k) == 0);
+    };
+    auto same_d = [](const std::vector<double>& v, const double* q, int64_t k) {
+        return (int64_t)v.size() == k && (k == 0 || memcmp(v.data(), q, sizeof(double) * (size_t)k) == 0);
+    };
+    const bool reuse = tin.valid && tin.ids_version == e->ids_version && tin.n == n &&
+                       same_i(tin.bh, bond_head_id, nb) && same_i(tin.bt, bond_tail_id, nb) &&
+                       same_d(tin.k2, k2, nb) && same_d(tin.l0, l0, nb) && same_i(tin.f, first_bond, na) &&
+                       same_i(tin.sc, second_bond, na) && same_d(tin.k3, k3, na) && same_d(tin.phi0, phi0, na);
+    int64_t nbl = reuse ? tin.nbl : 0;
+    if (!reuse) {
+    tin.valid = false;   // the staging buffer is rewritten below
     // bead id -> upload index (the ids kept from the bead upload)
     const std::vector<int64_t>& hpid = e->h_id;
     bool identity = true;
@@ -1412,9 +1463,9 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         terms[fillp[a4[i]]++] = (int)(i * 8 + kAngle1);         // middle bead:       force [1]
         terms[fillp[a4[2 * na + i]]++] = (int)(i * 8 + kAngle2);  // second bond's head: force [2]
     }
-    int64_t nbl = 0;
     for (int64_t b = 0; b < n; ++b)
         if (cnt[b + 1] > cnt[b]) bbl[nbl++] = (int)b;
+    }
     bool moved = false;
     int rc;
     cudaStream_t st = e->s();
@@ -1472,6 +1523,20 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
         e->h_ang_phi0.assign(phi0, phi0 + na);
     }
     CU(cudaStreamSynchronize(st));   // the staging buffer is reused by the next call
+    if (!reuse) {
+        tin.bh.assign(bond_head_id, bond_head_id + nb);
+        tin.bt.assign(bond_tail_id, bond_tail_id + nb);
+        tin.k2.assign(k2, k2 + nb);
+        tin.l0.assign(l0, l0 + nb);
+        tin.f.assign(first_bond, first_bond + na);
+        tin.sc.assign(second_bond, second_bond + na);
+        tin.k3.assign(k3, k3 + na);
+        tin.phi0.assign(phi0, phi0 + na);
+        tin.ids_version = e->ids_version;
+        tin.n = n;
+        tin.nbl = nbl;
+        tin.valid = true;
+    }
     e->topo_nb = nb;
     e->topo_na = na;
     e->mon_set = false;   // the monitor's bond types refer to the previous topology

@@ -29,55 +29,84 @@ struct UploadIn {
     const unsigned char* movable;   // or null
 };
 
+// The previous upload's bead ids and types (upload order), compared with
+// the new ones so the host refreshes its copies only when they change.
+struct UploadPrev {
+    int64_t* id;           // n entries, overwritten with the new ids
+    int* type;
+    unsigned* changed;     // bit 0: an id differs, bit 1: a type differs
+    int* type_count;       // beads per type (ntypes entries, zeroed by the caller)
+};
+
+// Validation and binning of an uploaded bead set: cell[b] receives the bead's
+// CNT cell and the cells are counted; the first bead of each error kind is
+// recorded in err; every valid bead's type is counted (block histogram).
 __global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes, const Box* __restrict__ boxes,
                                                   UploadIn in, int* __restrict__ cell, uint32_t* __restrict__ img,
                                                   double* __restrict__ off, int* __restrict__ count,
                                                   int* __restrict__ block_count, int* __restrict__ err,
-                                                  int* __restrict__ any_off)
+                                                  int* __restrict__ any_off, UploadPrev prev)
 {
+    __shared__ int hist[kMaxTypes];
+    for (int k = threadIdx.x; k < ntypes; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n) return;
-    const int t = in.type[b];
-    if (t < 0 || t >= ntypes) { atomicMin(&err[kUpType], b); return; }
-    const int64_t idv = in.id[b];
-    if (idv < 1 || idv > 0x7fffffff) { atomicMin(&err[kUpId], b); return; }
-    const int bx = in.box ? in.box[b] : 0;
-    if (bx < 0 || bx >= nboxes) { atomicMin(&err[kUpBox], b); return; }
-    const Box& B = boxes[bx];
-    long long ci[3];
+    unsigned diff = 0;
+    if (b < n) {
+        const int t = in.type[b];
+        const int64_t idv = in.id[b];
+        diff = (prev.id[b] != idv ? 1u : 0u) | (prev.type[b] != t ? 2u : 0u);
+        prev.id[b] = idv;
+        prev.type[b] = t;
+        do {
+            if (t < 0 || t >= ntypes) { atomicMin(&err[kUpType], b); break; }
+            if (idv < 1 || idv > 0x7fffffff) { atomicMin(&err[kUpId], b); break; }
+            const int bx = in.box ? in.box[b] : 0;
+            if (bx < 0 || bx >= nboxes) { atomicMin(&err[kUpBox], b); break; }
+            const Box& B = boxes[bx];
+            long long ci[3];
+            bool bad = false;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double xv = in.x[3 * b + d];
-        if (!isfinite(xv) || !isfinite(in.v[3 * b + d])) { atomicMin(&err[kUpNonFinite], b); return; }
-        ci[d] = (long long)(xv / B.w[d]);
-        if (xv < 0.0 || ci[d] < 0 || ci[d] >= B.nc[d]) { atomicMin(&err[kUpOutside], b); return; }
+            for (int d = 0; d < 3; ++d) {
+                const double xv = in.x[3 * b + d];
+                if (!isfinite(xv) || !isfinite(in.v[3 * b + d])) { atomicMin(&err[kUpNonFinite], b); bad = true; break; }
+                ci[d] = (long long)(xv / B.w[d]);
+                if (xv < 0.0 || ci[d] < 0 || ci[d] >= B.nc[d]) { atomicMin(&err[kUpOutside], b); bad = true; break; }
+            }
+            if (bad) break;
+            int ii[3] = {0, 0, 0};
+            bool residual = false;
+            double r[3] = {0.0, 0.0, 0.0};
+            if (in.u) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double du = in.u[3 * b + d] - in.x[3 * b + d];
+                    const double k = nearbyint(du / B.L[d]);
+                    if (!(fabs(k) <= 511.0)) { atomicMin(&err[kUpImage], b); bad = true; break; }
+                    ii[d] = (int)k;
+                    r[d] = du - k * B.L[d];
+                    residual |= r[d] != 0.0;
+                }
+            }
+            if (bad) break;
+            const int c = (int)(B.cell_base + ci[0] + (long long)B.nc[0] * (ci[1] + (long long)B.nc[1] * ci[2]));
+            cell[b] = c;
+            img[b] = img_pack(ii[0], ii[1], ii[2]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) off[(size_t)d * n + b] = r[d];
+            if (residual) *any_off = 1;
+            atomicAdd(&count[c], 1);
+            atomicAdd(&block_count[c / kScanChunk], 1);
+            atomicAdd(&hist[t], 1);
+        } while (false);
     }
-    int ii[3] = {0, 0, 0};
-    bool residual = false;
-    double r[3] = {0.0, 0.0, 0.0};
-    if (in.u) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double du = in.u[3 * b + d] - in.x[3 * b + d];
-            const double k = nearbyint(du / B.L[d]);
-            if (!(fabs(k) <= 511.0)) { atomicMin(&err[kUpImage], b); return; }
-            ii[d] = (int)k;
-            r[d] = du - k * B.L[d];
-            residual |= r[d] != 0.0;
-        }
-    }
-    const int c = (int)(B.cell_base + ci[0] + (long long)B.nc[0] * (ci[1] + (long long)B.nc[1] * ci[2]));
-    cell[b] = c;
-    img[b] = img_pack(ii[0], ii[1], ii[2]);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) off[(size_t)d * n + b] = r[d];
-    if (residual) *any_off = 1;
-    atomicAdd(&count[c], 1);
-    atomicAdd(&block_count[c / kScanChunk], 1);
+    const unsigned wdiff = __reduce_or_sync(0xffffffffu, diff);
+    if ((threadIdx.x & 31) == 0 && wdiff) atomicOr(prev.changed, wdiff);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ntypes; k += blockDim.x)
+        if (hist[k]) atomicAdd(&prev.type_count[k], hist[k]);
 }
 
-// Any slot of the bead's cell range, taken with an atomic cursor (count, zero
-// on entry); k_up_place fixes the order inside the cell.
 __global__ void __launch_bounds__(256) k_up_scatter(int n, const int* __restrict__ cell,
                                                     const int* __restrict__ start, int* __restrict__ cursor,
                                                     int* __restrict__ perm)

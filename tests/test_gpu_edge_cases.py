@@ -261,6 +261,39 @@ def test_step_counter_follows_the_calls(engine_mod, oracle_mod, precision):
     assert eng.status() == 0
 
 
+def test_reuploaded_topology_equals_a_fresh_engine(engine_mod):
+    """Re-uploading the same beads and topology (the engine reuses its last
+    topology build), a changed topology and changed bead ids (both rebuilt)
+    all step exactly as a fresh engine given the same state (full shell:
+    bitwise reproducible)."""
+    s = W.bilayer(cells=(12, 12, 12), nlipids=60)
+    topo = (s.bond_head, s.bond_tail, s.bond_k2, s.bond_l0, s.angle_first, s.angle_second, s.angle_k3,
+            s.angle_phi0)
+
+    def run(eng, ids=s.ids, t=topo):
+        eng.upload_beads(ids, s.types, s.movable, s.x, s.unpbc, s.v, s.f)
+        eng.upload_topology(*t)
+        eng.step(1, 4)
+        return eng.download()["f"]
+
+    fresh = engine_mod.DpdEngine.from_system(s, precision=1, topology=False)
+    want = run(fresh)
+    a = engine_mod.DpdEngine.from_system(s, precision=1, topology=False)
+    run(a)
+    assert np.array_equal(run(a), want)                     # same topology, same ids: reused
+    k2 = np.array(s.bond_k2, copy=True)
+    k2[::3] *= 1.5
+    t2 = (s.bond_head, s.bond_tail, k2) + topo[3:]
+    fresh2 = engine_mod.DpdEngine.from_system(s, precision=1, topology=False)
+    assert np.array_equal(run(a, t=t2), run(fresh2, t=t2))  # changed spring constants: rebuilt
+    assert not np.array_equal(run(a), run(a, t=t2))
+    ids = np.asarray(s.ids) + 7                              # other ids, same bonds by id: rebuilt
+    t3 = (np.asarray(s.bond_head) + 7, np.asarray(s.bond_tail) + 7) + topo[2:]
+    fresh3 = engine_mod.DpdEngine.from_system(s, precision=1, topology=False)
+    assert np.array_equal(run(a, ids=ids, t=t3), run(fresh3, ids=ids, t=t3))
+    assert a.status() == 0
+
+
 def test_step_returns_the_fatal_status_without_waiting(engine_mod):
     """A non-finite state raised on the device is returned by a later
     dpd_engine_step (DPD_E_STATUS, no further work queued) without a
