@@ -53,7 +53,10 @@ extern "C" {
 #define DPD_STATUS_NONFINITE      0x2u  /* a non-finite position, velocity or force       */
 #define DPD_STATUS_IMAGE_OVERFLOW 0x4u  /* a periodic image counter left +-511 box lengths */
 #define DPD_STATUS_INTERNAL       0x8u  /* an internal capacity check tripped (a bug): results invalid */
-#define DPD_STATUS_FATAL_MASK     (DPD_STATUS_NONFINITE | DPD_STATUS_IMAGE_OVERFLOW | DPD_STATUS_INTERNAL)
+#define DPD_STATUS_SLAB_REACH     0x10u /* a slab's owned bead lost a bond or bond pair: its partner
+                                           lies beyond the ghost layers (dpd_engine_slab_*)      */
+#define DPD_STATUS_FATAL_MASK     (DPD_STATUS_NONFINITE | DPD_STATUS_IMAGE_OVERFLOW | DPD_STATUS_INTERNAL | \
+                                   DPD_STATUS_SLAB_REACH)
 
 /* Kernel ids for dpd_engine_profile_read (the kernels of one step, in order). */
 #define DPD_KERNEL_UPDATE_POS   0   /* UpdatePos drift + cell move             */
@@ -228,6 +231,11 @@ DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
 DPD_API int dpd_engine_download(dpd_engine* e, double* x3, double* unpbc3, double* v3, double* f3,
                         double* stress9);
 
+/* Bead ids and types in upload order (n entries each; either may be NULL):
+ * the caller's arrays as uploaded, or after dpd_engine_slab_unpack the
+ * local box's beads as the exchange formed them. */
+DPD_API int dpd_engine_bead_ids(dpd_engine* e, int64_t* id, int32_t* type);
+
 /* Index of the CNT cell each bead is filed in (nx*(ny*iz+iy)+ix). */
 DPD_API int dpd_engine_cells(dpd_engine* e, int32_t* cell);
 
@@ -369,6 +377,59 @@ DPD_API int dpd_batch_upload_beads(dpd_engine* e, int64_t n, const int32_t* box,
 
 /* Single-bead sums of one box (the virial from its latest sample step). */
 DPD_API int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out);
+
+/* ---- z-slab decomposition, slab resident on the device ------------------
+ * Replaces the reference's spatial decomposition over processors (the mps*
+ * boxes: SimBox.cpp:481-567, mpsSimBox.cpp:796-860, CNTCell.cpp:3598
+ * UpdateForceP) for a box split into slabs of whole CNT cell layers along z,
+ * one per rank.  Each rank's engine is created for its local box: the global
+ * box's nx, ny and widths, and z1 - z0 + 2*ghost layers (its own layers
+ * [z0, z1) of the global nz_global, plus ghost layers on either side), with
+ * positions in the local frame (global z minus (z0 - ghost) * wz, wrapped
+ * into the global box; unPBC z minus the same).  The owned beads are
+ * uploaded with dpd_engine_upload_beads; then every exchange is
+ *   dpd_engine_slab_pack -> the caller sends send_below to the rank below and
+ *   send_above to the rank above and receives the matching buffers
+ *   (ncclSend/ncclRecv or any transport; the buffers are device memory) ->
+ *   dpd_engine_slab_unpack,
+ * once after setup (the first ghosts) and once after every
+ * dpd_engine_step(e, t, 1).  The pair noise is keyed on bead ids and the step,
+ * so every owned bead sees exactly the forces it sees in the whole box and no
+ * force travels back.  In upload order the local beads are the owned ones
+ * first (dpd_engine_download returns them in the first n_owned rows), then
+ * the ghosts. */
+
+/* Turns an engine holding its slab's owned beads (the first n_owned of the
+ * upload; all of them normally) into a slab, and takes the WHOLE box's
+ * topology (bead ids 1..id_max): each exchange keeps the bonds and bond pairs
+ * whose beads are all in the local box, on the device.  Needs ghost >= 1,
+ * z1 - z0 >= 2*ghost and (z1 - z0) + 2*ghost <= nz_global.  Captured graphs
+ * are off for a slab (its bead count changes every step). */
+DPD_API int dpd_engine_slab_setup(dpd_engine* e, int32_t nz_global, int32_t z0, int32_t z1, int32_t ghost,
+                                  int64_t n_owned, int64_t id_max, int64_t nb, const int64_t* bond_head_id,
+                                  const int64_t* bond_tail_id, const double* k2, const double* l0, int64_t na,
+                                  const int64_t* first_bond, const int64_t* second_bond, const double* k3,
+                                  const double* phi0);
+
+/* Packs the beads to send (asynchronous, on the engine's stream): migrants
+ * (owned beads that left [z0, z1)) and the next step's ghosts (owned beads
+ * within ghost layers of a face), as records of 16 doubles (id, type,
+ * movable, kind, x[3], unPBC[3], v[3], F[3]; global frame) after a header
+ * record (beads, of them migrants first, overflow flag).  Each buffer holds
+ * (capacity + 1) * 16 doubles, 16-byte aligned, device memory. */
+DPD_API int dpd_engine_slab_pack(dpd_engine* e, double* send_below, double* send_above, int64_t capacity);
+
+/* Forms the next local box from this rank's staying beads and the two
+ * received buffers (device memory; recv_below came from the rank below) and
+ * uploads it on the device (no host copy of bead data; the call waits once
+ * for the sizes).  Returns the owned and local bead counts.  DPD_E_LIMIT when
+ * either side's beads overflowed a buffer, DPD_E_STATUS when the step before
+ * set a fatal status bit (the state is then left as the step made it). */
+DPD_API int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, const double* recv_above,
+                                   int64_t* n_owned, int64_t* n_local);
+
+/* The current owned and local bead counts. */
+DPD_API int dpd_engine_slab_counts(dpd_engine* e, int64_t* n_owned, int64_t* n_local);
 
 /* ---- Pair forces without any allocation ---------------------------------
  * This entry point has no counterpart in the reference.  It is for callers

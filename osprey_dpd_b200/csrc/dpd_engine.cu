@@ -26,6 +26,7 @@
 #include "monitor.cuh"
 #include "upload.cuh"
 #include "builder.cuh"
+#include "slab.cuh"
 #include <climits>
 
 using namespace dpd;
@@ -39,6 +40,32 @@ inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) /
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+};
+
+// One z-slab of a decomposed box (dpd_engine_slab_*): the geometry, the pack's
+// scratch and the whole box's topology on the device.
+struct SlabState {
+    SlabGeom geom{};
+    int* d_bcount = nullptr;             // kSlabOuts block counts, then their offsets
+    size_t cap_bcount = 0;
+    int* d_total = nullptr;              // kSlabOuts stream totals
+    double* d_keep = nullptr;            // staying owned beads' records (local frame)
+    double* d_mine = nullptr;            // own migrants' records (local frame)
+    size_t cap_keep = 0, cap_mine = 0;
+    int* h_sizes = nullptr;              // k_slab_sizes' output, mapped pinned memory
+    int* d_sizes = nullptr;
+    bool packed = false;                 // a pack waits for its unpack
+    // topology of the whole box, by bond / bond-pair index and by bead id
+    bool topo = false;
+    int nb = 0, na = 0, id_max = 0;
+    size_t nterm = 0;
+    int *d_head_id = nullptr, *d_tail_id = nullptr, *d_first = nullptr, *d_second = nullptr;
+    int *d_gptr = nullptr, *d_gterm = nullptr;
+    unsigned long long* d_idmap = nullptr;
+    unsigned version = 0;
+    int* d_cnt = nullptr;
+    int* d_bsum = nullptr;
+    size_t cap_cnt = 0, cap_bsum = 0, cap_bb = 0;
 };
 
 }  // namespace
@@ -56,6 +83,10 @@ struct dpd_engine {
     int64_t ncell = 0;
     int nchunk = 0;
     int64_t n = 0;
+    int64_t cap_n = 0;          // beads the per-bead buffers hold
+    double n_headroom = 1.0;    // their growth factor (a slab's bead count changes every step)
+    SlabState* slab = nullptr;  // set by dpd_engine_slab_setup
+    bool host_ids_stale = false;   // h_id / h_type lag an upload from device memory
     int64_t launches = 0;
     bool uploaded = false;
     bool stepped = false;
@@ -758,6 +789,21 @@ int empty_topology(dpd_engine* e, bool keep_bonded)
     return DPD_OK;
 }
 
+// The host copies of the bead ids and types, fetched after an upload from
+// device memory (d_prev_id / d_prev_type hold the last upload's, upload order).
+int host_ids(dpd_engine* e)
+{
+    if (!e->host_ids_stale) return DPD_OK;
+    const size_t n = (size_t)e->n;
+    e->h_id.resize(n);
+    e->h_type.resize(n);
+    CU(cudaMemcpyAsync(e->h_id.data(), e->d_prev_id, n * sizeof(int64_t), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaMemcpyAsync(e->h_type.data(), e->d_prev_type, n * sizeof(int), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    e->host_ids_stale = false;
+    return DPD_OK;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -902,6 +948,10 @@ void dpd_engine_destroy(dpd_engine* e)
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
     for (void* p : e->allocations) cudaFree(p);
     e->allocations.clear();
+    if (e->slab) {
+        if (e->slab->h_sizes) cudaFreeHost(e->slab->h_sizes);
+        delete e->slab;
+    }
     if (e->h_status) cudaFreeHost(e->h_status);
     if (e->h_obs) cudaFreeHost(e->h_obs);
     if (e->h_stage) cudaFreeHost(e->h_stage);
@@ -1099,19 +1149,25 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
             case kUpNonFinite: return fail(e, DPD_E_BOX, "non-finite bead state");
             case kUpOutside: {
                 char msg[160];
-                snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)bad,
-                         (long long)id[bad]);
+                if (id)
+                    snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)bad,
+                             (long long)id[bad]);
+                else
+                    snprintf(msg, sizeof msg, "bead %lld lies outside the box", (long long)bad);
                 return fail(e, DPD_E_BOX, msg);
             }
             default: return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
         }
     }
     const bool any_off = herr[kUpErrors] != 0;
-    // (re)allocate per-bead buffers; new addresses invalidate the captured graphs
+    // (re)allocate per-bead buffers when they are too small (strides follow the
+    // bead count, so smaller counts fit); new addresses or another bead count
+    // invalidate the captured graphs
     const bool same_n = e->n == n;
-    if (e->n != n) {
-        drop_graphs(e);
-        release_topology(e);
+    if (!same_n) drop_graphs(e);
+    if (n > e->cap_n) {
+        // a slab keeps the whole box's topology arrays across its uploads
+        if (!e->slab) release_topology(e);
         void** bufs[] = {(void**)&e->d_x[0], (void**)&e->d_x[1], (void**)&e->d_v[0], (void**)&e->d_v[1],
                          (void**)&e->d_bid[0], (void**)&e->d_bid[1], (void**)&e->d_tf[0], (void**)&e->d_tf[1],
                          (void**)&e->d_img[0], (void**)&e->d_img[1], (void**)&e->d_cell[0], (void**)&e->d_cell[1],
@@ -1122,32 +1178,35 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
                          (void**)&e->d_cella};
         for (auto q : bufs) { dfree(e, *q); *q = nullptr; }
         const size_t rs = real_size(e);
+        const int64_t cap = std::max<int64_t>(n, (int64_t)((double)n * e->n_headroom));
+        e->cap_n = 0;
         int rc;
-        if ((rc = dalloc(e, &e->d_xa, 3 * (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_imga, (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_cella, (size_t)n))) return rc;
+        if ((rc = dalloc(e, &e->d_xa, 3 * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_imga, (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_cella, (size_t)cap))) return rc;
         for (int k = 0; k < 2; ++k) {
-            if ((rc = dalloc(e, &e->d_x[k], 3 * (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_v[k], 3 * (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_bid[k], (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_tf[k], (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_img[k], (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_cell[k], (size_t)n))) return rc;
-            if ((rc = dalloc(e, &e->d_pid[k], (size_t)n))) return rc;
+            if ((rc = dalloc(e, &e->d_x[k], 3 * (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_v[k], 3 * (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_bid[k], (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_tf[k], (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_img[k], (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_cell[k], (size_t)cap))) return rc;
+            if ((rc = dalloc(e, &e->d_pid[k], (size_t)cap))) return rc;
         }
-        if ((rc = dalloc(e, (char**)&e->d_F, 3 * rs * (size_t)n))) return rc;
-        if ((rc = dalloc(e, (char**)&e->d_Fold, 3 * rs * (size_t)n))) return rc;
-        if ((rc = dalloc(e, (char**)&e->d_stress, 9 * rs * (size_t)n))) return rc;
-        if ((rc = dalloc(e, (char**)&e->d_pos4, 4 * rs * (size_t)n))) return rc;
-        if ((rc = dalloc(e, (char**)&e->d_vel4, 4 * rs * (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_rank, (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_perm, (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_pid_of, (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(n, kThreads) * kObsTerms))) return rc;
-        if ((rc = dalloc(e, &e->d_out, 21 * (size_t)n))) return rc;
-        if ((rc = dalloc(e, &e->d_out_cell, (size_t)n))) return rc;
-        e->n = n;
+        if ((rc = dalloc(e, (char**)&e->d_F, 3 * rs * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_Fold, 3 * rs * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_stress, 9 * rs * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_pos4, 4 * rs * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, (char**)&e->d_vel4, 4 * rs * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_rank, (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_perm, (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_pid_of, (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_partials, (size_t)blocks_for(cap, kThreads) * kObsTerms))) return rc;
+        if ((rc = dalloc(e, &e->d_out, 21 * (size_t)cap))) return rc;
+        if ((rc = dalloc(e, &e->d_out_cell, (size_t)cap))) return rc;
+        e->cap_n = cap;
     }
+    e->n = n;
     // cell starts, then the slot order: by cell, inside a cell by upload index
     k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start,
                                                      (const unsigned*)e->d_status, (unsigned*)nullptr);
@@ -1182,11 +1241,20 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     // change; beads per type counted by k_up_check
     const unsigned changed = prev_ok ? (unsigned)herr[kUpErrors + 1] : 3u;
     e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
-    if ((changed & 1u) || e->h_id.size() != (size_t)n) {
-        e->h_id.assign(id, id + n);
-        ++e->ids_version;
+    if (!id || !type) {
+        // an upload from device memory: the host copies are fetched when needed
+        if (changed & 3u) {
+            e->host_ids_stale = true;
+            ++e->ids_version;
+        }
+    } else {
+        if (e->host_ids_stale || (changed & 1u) || e->h_id.size() != (size_t)n) {
+            e->h_id.assign(id, id + n);
+            ++e->ids_version;
+        }
+        if (e->host_ids_stale || (changed & 2u) || e->h_type.size() != (size_t)n) e->h_type.assign(type, type + n);
+        e->host_ids_stale = false;
     }
-    if ((changed & 2u) || e->h_type.size() != (size_t)n) e->h_type.assign(type, type + n);
     CU(cudaStreamSynchronize(st));
     *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine is in flight after the sync
     rc = empty_topology(e, same_n);
@@ -1362,8 +1430,10 @@ int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_he
     if (nb < 0 || na < 0 || (nb && (!bond_head_id || !bond_tail_id || !k2 || !l0)) ||
         (na && (!first_bond || !second_bond || !k3 || !phi0)))
         return fail(e, DPD_E_ARG, "bad topology arrays");
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab takes its topology in dpd_engine_slab_setup");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
+    if (int rc0 = host_ids(e)) return rc0;
     const int64_t n = e->n;
     // The device arrays are built on the host in one pinned staging buffer
     // and copied asynchronously; the call waits once, at the end.
@@ -1828,6 +1898,7 @@ int dpd_engine_write_restart(dpd_engine* e, const char* path, int32_t wall, int3
     std::vector<double> x(3 * n), u(3 * n), v(3 * n), f(3 * n);
     int rc = run_download(e, x.data(), u.data(), v.data(), f.data(), nullptr, nullptr);
     if (rc) return rc;
+    if ((rc = host_ids(e))) return rc;
     const double* L = e->hboxes[0].L;
     // CRestartState::CheckBeadWithinBox (RestartState.cpp:488-530): a
     // coordinate past the box length is an error, one within 0.001 of a face
@@ -1939,6 +2010,7 @@ int dpd_engine_write_paraview(dpd_engine* e, const char* path, const uint8_t* ty
     std::vector<int32_t> cell((size_t)n);
     int rc = run_download(e, x.data(), nullptr, nullptr, nullptr, nullptr, cell.data());
     if (rc) return rc;
+    if ((rc = host_ids(e))) return rc;
     // CSimBox::GetAllBeadsInCNTCells (SimBox.cpp:5883-5895): cells in index
     // order; inside a cell the reference keeps its list order, the engine the
     // upload order.  Beads of invisible types are left out (CurrentState.cpp:
@@ -2057,10 +2129,11 @@ int dpd_engine_step(dpd_engine* e, int64_t first_step, int32_t nsteps)
     const unsigned seen = *(volatile unsigned*)e->h_seen;
     if (seen & DPD_STATUS_FATAL_MASK) {
         char msg[160];
-        snprintf(msg, sizeof msg, "device status 0x%x: %s%s%s", seen,
+        snprintf(msg, sizeof msg, "device status 0x%x: %s%s%s%s", seen,
                  (seen & DPD_STATUS_NONFINITE) ? "non-finite position, velocity or force; " : "",
                  (seen & DPD_STATUS_IMAGE_OVERFLOW) ? "periodic image counter overflow; " : "",
-                 (seen & DPD_STATUS_INTERNAL) ? "internal capacity check" : "");
+                 (seen & DPD_STATUS_INTERNAL) ? "internal capacity check; " : "",
+                 (seen & DPD_STATUS_SLAB_REACH) ? "a bond reaches beyond the slab's ghost layers" : "");
         return fail(e, DPD_E_STATUS, msg);
     }
     if (nsteps == 0) return DPD_OK;
@@ -2197,6 +2270,17 @@ int dpd_engine_download(dpd_engine* e, double* x3, double* unpbc3, double* v3, d
     return run_download(e, x3, unpbc3, v3, f3, stress9, nullptr);
 }
 
+int dpd_engine_bead_ids(dpd_engine* e, int64_t* id, int32_t* type)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
+    CU(cudaSetDevice(e->device));
+    if (int rc = host_ids(e)) return rc;
+    if (id) memcpy(id, e->h_id.data(), sizeof(int64_t) * (size_t)e->n);
+    if (type) memcpy(type, e->h_type.data(), sizeof(int32_t) * (size_t)e->n);
+    return DPD_OK;
+}
+
 int dpd_engine_cells(dpd_engine* e, int32_t* cell)
 {
     if (!e) return DPD_E_ARG;
@@ -2291,6 +2375,327 @@ int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out)
     const double v2 = out->sum_v2[0] + out->sum_v2[1] + out->sum_v2[2];
     out->kT = nbox > 0 ? v2 / (3.0 * (double)nbox) : 0.0;
     out->pressure = 0.3333333333 * (1.0 / V) * (v2 + out->virial[0] + out->virial[4] + out->virial[8]);
+    return DPD_OK;
+}
+
+// ===================================================== z-slab decomposition
+
+// The local box's bonds and bond pairs: the whole box's terms whose beads are
+// all in the local box, per bead in the single-box build's order, with the
+// bead indices of the current upload (k_slab_* in slab.cuh).  With check, an
+// owned bead that loses a term sets DPD_STATUS_SLAB_REACH (not at setup,
+// before the first exchange has brought the ghosts).
+static int slab_topology(dpd_engine* e, bool check)
+{
+    SlabState& S = *e->slab;
+    const int n = (int)e->n;
+    cudaStream_t st = e->s();
+    int rc;
+    bool moved = false;
+    if (++S.version == 0) {   // the map's entries carry the version: a wrap clears it
+        CU(cudaMemsetAsync(S.d_idmap, 0, sizeof(unsigned long long) * ((size_t)S.id_max + 1), st));
+        S.version = 1;
+    }
+    const SlabTopo T{S.nb, S.na, S.id_max, S.d_head_id, S.d_tail_id, S.d_first, S.d_second, S.d_gptr, S.d_gterm};
+    k_slab_idmap<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, S.id_max, e->d_pid_of, S.version, S.d_idmap);
+    if ((rc = check_launch(e, "k_slab_idmap"))) return rc;
+    const int m = std::max(S.nb, S.na);
+    if (m > 0) {
+        k_slab_endpoints<<<blocks_for(m, kThreads), kThreads, 0, st>>>(T, S.d_idmap, S.version, e->d_bond_h,
+                                                                      e->d_bond_t, e->d_ang[0], e->d_ang[1],
+                                                                      e->d_ang[2], e->d_ang[3]);
+        if ((rc = check_launch(e, "k_slab_endpoints"))) return rc;
+    }
+    const int nblk = blocks_for(n, kThreads);
+    const size_t room = (size_t)((double)n * e->n_headroom);   // the count changes every step
+    if ((rc = ensure(e, &S.d_cnt, S.cap_cnt, room, &moved))) return rc;
+    if ((rc = ensure(e, &S.d_bsum, S.cap_bsum, (size_t)blocks_for(room, kThreads), &moved))) return rc;
+    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, room + 1, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, std::max<size_t>(S.nterm, 1), &moved))) return rc;
+    k_slab_term_count<<<nblk, kThreads, 0, st>>>(n, check ? S.geom.n_owned : 0, T, e->d_pid_of, e->d_bond_h, e->d_bond_t,
+                                                 e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], S.d_cnt,
+                                                 e->d_status);
+    if ((rc = check_launch(e, "k_slab_term_count"))) return rc;
+    k_scan_block_sums<<<nblk, kThreads, 0, st>>>(n, S.d_cnt, S.d_bsum);
+    if ((rc = check_launch(e, "k_scan_block_sums"))) return rc;
+    k_scan_top<<<1, 1024, 0, st>>>(nblk, S.d_bsum);
+    if ((rc = check_launch(e, "k_scan_top"))) return rc;
+    k_scan_apply<<<nblk, kThreads, 0, st>>>(n, S.d_cnt, S.d_bsum, e->d_csr_ptr);
+    if ((rc = check_launch(e, "k_scan_apply"))) return rc;
+    k_slab_term_write<<<nblk, kThreads, 0, st>>>(n, T, e->d_pid_of, e->d_bond_h, e->d_bond_t, e->d_ang[0],
+                                                 e->d_ang[1], e->d_ang[2], e->d_ang[3], e->d_csr_ptr, e->d_csr_term,
+                                                 (int)std::min<size_t>(e->cap_csr_term, INT_MAX));
+    if ((rc = check_launch(e, "k_slab_term_write"))) return rc;
+    // every local bead runs through the bonded kernel (beads without terms
+    // leave it at once): the bonded-bead list is 0..n-1
+    if ((rc = ensure(e, &e->d_ubuf, e->cap_ubuf, room, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_Fb, e->cap_Fb, room, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_Sb, e->cap_Sb, 9 * room, &moved))) return rc;
+    if (!e->d_bb || S.cap_bb < (size_t)n) {
+        if ((rc = ensure(e, &e->d_bb, e->cap_bb, room, &moved))) return rc;
+        k_iota<<<blocks_for(e->cap_bb, kThreads), kThreads, 0, st>>>((int)e->cap_bb, e->d_bb);
+        if ((rc = check_launch(e, "k_iota"))) return rc;
+        S.cap_bb = e->cap_bb;
+    }
+    e->nbb = n;
+    k_mark_bonded<<<nblk, kThreads, 0, st>>>(n, e->d_bid[e->cur], e->d_csr_ptr, e->d_tf[e->cur]);
+    if ((rc = check_launch(e, "k_mark_bonded"))) return rc;
+    e->topo_nb = S.nb;
+    e->topo_na = S.na;
+    return DPD_OK;
+}
+
+int dpd_engine_slab_setup(dpd_engine* e, int32_t nz_global, int32_t z0, int32_t z1, int32_t ghost, int64_t n_owned,
+                          int64_t id_max, int64_t nb, const int64_t* bond_head_id, const int64_t* bond_tail_id,
+                          const double* k2, const double* l0, int64_t na, const int64_t* first_bond,
+                          const int64_t* second_bond, const double* k3, const double* phi0)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->uploaded) return fail(e, DPD_E_STATE, "upload the slab's owned beads first");
+    if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "a slab is a single-box engine");
+    if (e->slab) return fail(e, DPD_E_STATE, "the engine is a slab already");
+    const Box& B = e->hboxes[0];
+    const int own = z1 - z0;
+    if (ghost < 1 || z0 < 0 || own < 2 * ghost || z1 > nz_global || own + 2 * ghost > nz_global ||
+        B.nc[2] != own + 2 * ghost)
+        return fail(e, DPD_E_ARG, "slab layers: 0 <= z0, 2*ghost <= z1 - z0, (z1 - z0) + 2*ghost <= nz_global, "
+                                  "and the engine's box holds z1 - z0 + 2*ghost layers");
+    if (n_owned < 0 || n_owned > e->n) return fail(e, DPD_E_ARG, "owned beads outside 0..n");
+    if (nb < 0 || na < 0 || (nb && (!bond_head_id || !bond_tail_id || !k2 || !l0)) ||
+        (na && (!first_bond || !second_bond || !k3 || !phi0)))
+        return fail(e, DPD_E_ARG, "bad topology arrays");
+    if ((nb || na) && (id_max < 1 || id_max > 0x7fffffff)) return fail(e, DPD_E_ARG, "id_max outside 1..2^31-1");
+    if (nb * 2 + na * 3 > ((int64_t)1 << 28)) return fail(e, DPD_E_ARG, "topology too large");
+    for (int64_t i = 0; i < nb; ++i)
+        if (bond_head_id[i] < 1 || bond_head_id[i] > id_max || bond_tail_id[i] < 1 || bond_tail_id[i] > id_max ||
+            bond_head_id[i] == bond_tail_id[i])
+            return fail(e, DPD_E_ARG, "bond refers to a bead id outside 1..id_max or joins a bead to itself");
+    for (int64_t i = 0; i < na; ++i)
+        if (first_bond[i] < 0 || first_bond[i] >= nb || second_bond[i] < 0 || second_bond[i] >= nb)
+            return fail(e, DPD_E_ARG, "bond pair refers to an unknown bond");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    if (int rc0 = drop_ahead(e)) return rc0;
+    drop_graphs(e);
+    release_topology(e);
+    if (int rc0 = empty_topology(e, false)) return rc0;
+    std::unique_ptr<SlabState> S(new SlabState());
+    S->geom.z0 = z0;
+    S->geom.z1 = z1;
+    S->geom.g = ghost;
+    S->geom.nzg = nz_global;
+    S->geom.w = B.w[2];
+    S->geom.Lz = (double)nz_global * B.w[2];
+    S->geom.c = (double)(z0 - ghost) * B.w[2];
+    S->geom.n_owned = (int)n_owned;
+    if (cudaHostAlloc((void**)&S->h_sizes, 16 * sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+        return fail(e, DPD_E_CUDA, "pinned allocation failed");
+    if (cudaHostGetDevicePointer((void**)&S->d_sizes, S->h_sizes, 0) != cudaSuccess) {
+        cudaFreeHost(S->h_sizes);
+        return fail(e, DPD_E_CUDA, "mapped pinned memory unavailable");
+    }
+    memset(S->h_sizes, 0, 16 * sizeof(int));
+    int rc;
+    if ((rc = dalloc(e, &S->d_total, (size_t)kSlabOuts))) { cudaFreeHost(S->h_sizes); return rc; }
+    S->topo = nb > 0 || na > 0;
+    if (S->topo) {
+        S->nb = (int)nb;
+        S->na = (int)na;
+        S->id_max = (int)id_max;
+        // the whole box's term lists by bead id, in the single-box build's
+        // order (bonds by index, head and tail; then bond pairs by index)
+        std::vector<int> cnt((size_t)id_max + 2, 0);
+        for (int64_t i = 0; i < nb; ++i) { cnt[(size_t)bond_head_id[i] + 1]++; cnt[(size_t)bond_tail_id[i] + 1]++; }
+        for (int64_t i = 0; i < na; ++i) {
+            cnt[(size_t)bond_tail_id[first_bond[i]] + 1]++;
+            cnt[(size_t)bond_head_id[first_bond[i]] + 1]++;
+            cnt[(size_t)bond_head_id[second_bond[i]] + 1]++;
+        }
+        for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
+        S->nterm = (size_t)cnt.back();
+        std::vector<int> gterm(std::max<size_t>(S->nterm, 1)), fillp(cnt.begin(), cnt.end() - 1);
+        for (int64_t i = 0; i < nb; ++i) {
+            gterm[(size_t)fillp[(size_t)bond_head_id[i]]++] = (int)(i * 8 + kBondHead);
+            gterm[(size_t)fillp[(size_t)bond_tail_id[i]]++] = (int)(i * 8 + kBondTail);
+        }
+        for (int64_t i = 0; i < na; ++i) {
+            gterm[(size_t)fillp[(size_t)bond_tail_id[first_bond[i]]]++] = (int)(i * 8 + kAngle0);
+            gterm[(size_t)fillp[(size_t)bond_head_id[first_bond[i]]]++] = (int)(i * 8 + kAngle1);
+            gterm[(size_t)fillp[(size_t)bond_head_id[second_bond[i]]]++] = (int)(i * 8 + kAngle2);
+        }
+        std::vector<int> hid((size_t)std::max<int64_t>(nb, 1)), tid((size_t)std::max<int64_t>(nb, 1));
+        for (int64_t i = 0; i < nb; ++i) { hid[(size_t)i] = (int)bond_head_id[i]; tid[(size_t)i] = (int)bond_tail_id[i]; }
+        std::vector<int> fb((size_t)std::max<int64_t>(na, 1)), sb((size_t)std::max<int64_t>(na, 1));
+        std::vector<double> ak(3 * (size_t)std::max<int64_t>(na, 1));
+        for (int64_t i = 0; i < na; ++i) {
+            fb[(size_t)i] = (int)first_bond[i];
+            sb[(size_t)i] = (int)second_bond[i];
+            // as the single-box build: cos/sin of phi0, sin0 = 0 selecting the phi0 <= 0 branch
+            ak[(size_t)i] = k3[i];
+            ak[(size_t)na + i] = phi0[i] > 0.0 ? std::cos(phi0[i]) : 1.0;
+            ak[2 * (size_t)na + i] = phi0[i] > 0.0 ? std::sin(phi0[i]) : 0.0;
+        }
+        const size_t nbs = (size_t)std::max<int64_t>(nb, 1), nas = (size_t)std::max<int64_t>(na, 1);
+        bool moved = false;
+        size_t c;
+        if ((rc = dalloc(e, &S->d_head_id, nbs)) || (rc = dalloc(e, &S->d_tail_id, nbs)) ||
+            (rc = dalloc(e, &S->d_first, nas)) || (rc = dalloc(e, &S->d_second, nas)) ||
+            (rc = dalloc(e, &S->d_gptr, cnt.size())) || (rc = dalloc(e, &S->d_gterm, gterm.size())) ||
+            (rc = dalloc(e, &S->d_idmap, (size_t)id_max + 1))) {
+            cudaFreeHost(S->h_sizes);
+            return rc;
+        }
+        c = 0; if ((rc = ensure(e, &e->d_bond_h, c, nbs, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        c = 0; if ((rc = ensure(e, &e->d_bond_t, c, nbs, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        c = 0; if ((rc = ensure(e, &e->d_bond_k2, c, nbs, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        c = 0; if ((rc = ensure(e, &e->d_bond_l0, c, nbs, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        e->cap_bond = nbs;
+        for (int k = 0; k < 4; ++k) {
+            c = 0;
+            if ((rc = ensure(e, &e->d_ang[k], c, nas, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        }
+        c = 0; if ((rc = ensure(e, &e->d_ang_k3, c, nas, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        c = 0; if ((rc = ensure(e, &e->d_ang_cos0, c, nas, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        c = 0; if ((rc = ensure(e, &e->d_ang_sin0, c, nas, &moved))) { cudaFreeHost(S->h_sizes); return rc; }
+        e->cap_ang = nas;
+        cudaStream_t st = e->s();
+        CU(cudaMemcpyAsync(S->d_head_id, hid.data(), nbs * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S->d_tail_id, tid.data(), nbs * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S->d_first, fb.data(), nas * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S->d_second, sb.data(), nas * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S->d_gptr, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(S->d_gterm, gterm.data(), gterm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CU(cudaMemsetAsync(S->d_idmap, 0, sizeof(unsigned long long) * ((size_t)id_max + 1), st));
+        if (nb) {
+            CU(cudaMemcpyAsync(e->d_bond_k2, k2, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(e->d_bond_l0, l0, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        if (na) {
+            CU(cudaMemcpyAsync(e->d_ang_k3, ak.data(), (size_t)na * sizeof(double), cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(e->d_ang_cos0, ak.data() + na, (size_t)na * sizeof(double), cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(e->d_ang_sin0, ak.data() + 2 * (size_t)na, (size_t)na * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+            e->h_ang_phi0.assign(phi0, phi0 + na);
+        }
+        CU(cudaStreamSynchronize(st));
+    }
+    // every step's bead set is new: no captured graphs, and no drift done
+    // ahead by the last k_update_mom (the upload would discard it)
+    e->graphs_enabled = false;
+    e->ahead_enabled = false;
+    e->n_headroom = 1.25;
+    e->mon_set = false;
+    if (e->slice_S) e->slice_S = 0;
+    e->slab = S.release();
+    if (e->slab->topo) {
+        if ((rc = slab_topology(e, false))) return rc;
+        CU(cudaStreamSynchronize(e->s()));
+    }
+    return DPD_OK;
+}
+
+int dpd_engine_slab_pack(dpd_engine* e, double* send_below, double* send_above, int64_t capacity)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->slab) return fail(e, DPD_E_STATE, "not a slab (dpd_engine_slab_setup)");
+    if (!send_below || !send_above || send_below == send_above || capacity < 1 || capacity > (1 << 26) ||
+        ((uintptr_t)send_below & 15) || ((uintptr_t)send_above & 15))
+        return fail(e, DPD_E_ARG, "two distinct 16-byte aligned send buffers of capacity >= 1 records");
+    SlabState& S = *e->slab;
+    CU(cudaSetDevice(e->device));
+    const int n = (int)e->n;
+    const int nblk = blocks_for(n, kThreads);
+    int rc;
+    bool moved = false;
+    if ((rc = ensure(e, &S.d_bcount, S.cap_bcount, (size_t)kSlabOuts * nblk, &moved))) return rc;
+    const size_t room = (size_t)((double)n * e->n_headroom);   // the count changes every step
+    if ((rc = ensure(e, &S.d_keep, S.cap_keep, (size_t)kSlabRec * room, &moved))) return rc;
+    if ((rc = ensure(e, &S.d_mine, S.cap_mine, (size_t)kSlabRec * room, &moved))) return rc;
+    S.geom.cap = (int)capacity;
+    cudaStream_t st = e->s();
+    const int c = e->cur;
+    k_slab_count<<<nblk, kThreads, 0, st>>>(n, S.geom, e->d_x[c], e->d_bid[c], S.d_bcount);
+    if ((rc = check_launch(e, "k_slab_count"))) return rc;
+    k_slab_offsets<<<1, 1024, 0, st>>>(nblk, S.d_bcount, S.d_total, send_below, send_above, (int)capacity);
+    if ((rc = check_launch(e, "k_slab_offsets"))) return rc;
+    const double* off = e->off_active ? e->d_off : nullptr;
+    if (e->precision == DPD_PRECISION_FP64)
+        k_slab_write<double><<<nblk, kThreads, 0, st>>>(n, S.geom, e->d_boxes, e->d_x[c], e->d_v[c],
+                                                         (const double*)e->d_F, e->d_img[c], off, e->d_tf[c],
+                                                         e->d_bid[c], e->d_pid[c], S.d_bcount, S.d_total, send_below,
+                                                         send_above, S.d_keep, S.d_mine);
+    else
+        k_slab_write<float><<<nblk, kThreads, 0, st>>>(n, S.geom, e->d_boxes, e->d_x[c], e->d_v[c],
+                                                        (const float*)e->d_F, e->d_img[c], off, e->d_tf[c],
+                                                        e->d_bid[c], e->d_pid[c], S.d_bcount, S.d_total, send_below,
+                                                        send_above, S.d_keep, S.d_mine);
+    if ((rc = check_launch(e, "k_slab_write"))) return rc;
+    S.packed = true;
+    return DPD_OK;
+}
+
+int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, const double* recv_above, int64_t* n_owned,
+                           int64_t* n_local)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->slab) return fail(e, DPD_E_STATE, "not a slab (dpd_engine_slab_setup)");
+    SlabState& S = *e->slab;
+    if (!S.packed) return fail(e, DPD_E_STATE, "dpd_engine_slab_pack first");
+    if (!recv_below || !recv_above || ((uintptr_t)recv_below & 15) || ((uintptr_t)recv_above & 15))
+        return fail(e, DPD_E_ARG, "two 16-byte aligned receive buffers");
+    CU(cudaSetDevice(e->device));
+    cudaStream_t st = e->s();
+    k_slab_sizes<<<1, 1, 0, st>>>(recv_below, recv_above, S.d_total, e->d_status, S.geom.cap, S.d_sizes);
+    int rc = check_launch(e, "k_slab_sizes");
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(st));
+    int hs[16];
+    memcpy(hs, (const void*)S.h_sizes, sizeof hs);
+    S.packed = false;
+    if (hs[2] || hs[3] || hs[11] || hs[6] + hs[8] > S.geom.cap || hs[7] + hs[9] > S.geom.cap)
+        return fail(e, DPD_E_LIMIT, "more boundary beads than the exchange buffers hold");
+    const unsigned status = (unsigned)hs[4];
+    if (status & DPD_STATUS_FATAL_MASK) {
+        *(volatile unsigned*)e->h_seen = status;
+        char msg[96];
+        snprintf(msg, sizeof msg, "fatal device status 0x%x before the exchange", status);
+        return fail(e, DPD_E_STATUS, msg);
+    }
+    const int64_t nn = hs[1];
+    if (nn < 1) return fail(e, DPD_E_STATE, "the slab would hold no beads");
+    if ((rc = drop_ahead(e))) return rc;
+    if ((rc = stage_buffers(e, nn))) return rc;
+    double* up = e->d_up;
+    k_slab_place<<<blocks_for(nn, kThreads), kThreads, 0, st>>>((int)nn, S.geom, S.d_sizes + 5, S.d_keep,
+                                                                recv_below, recv_above, S.d_mine, up);
+    if ((rc = check_launch(e, "k_slab_place"))) return rc;
+    UploadIn in{};
+    in.x = up;
+    in.u = up + 3 * (size_t)nn;
+    in.v = up + 6 * (size_t)nn;
+    in.f = up + 9 * (size_t)nn;
+    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)nn);
+    const int* upi = reinterpret_cast<const int*>(up + 13 * (size_t)nn);
+    in.type = upi;
+    in.movable = reinterpret_cast<const unsigned char*>(upi + 2 * (size_t)nn);
+    if ((rc = upload_staged(e, nn, nullptr, nullptr, nullptr, in))) return rc;
+    if (status) {   // the step's non-fatal bits (cell skips) survive the exchange
+        k_slab_status<<<1, 1, 0, st>>>(e->d_status, status);
+        if ((rc = check_launch(e, "k_slab_status"))) return rc;
+    }
+    S.geom.n_owned = hs[0];
+    if (S.topo && (rc = slab_topology(e, true))) return rc;
+    if (n_owned) *n_owned = hs[0];
+    if (n_local) *n_local = nn;
+    return DPD_OK;
+}
+
+int dpd_engine_slab_counts(dpd_engine* e, int64_t* n_owned, int64_t* n_local)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->slab) return fail(e, DPD_E_STATE, "not a slab (dpd_engine_slab_setup)");
+    if (n_owned) *n_owned = e->slab->geom.n_owned;
+    if (n_local) *n_local = e->n;
     return DPD_OK;
 }
 

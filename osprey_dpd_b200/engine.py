@@ -24,6 +24,10 @@ FP64 = 1
 STATUS_CELL_SKIP = 0x1
 STATUS_NONFINITE = 0x2
 STATUS_IMAGE_OVERFLOW = 0x4
+STATUS_INTERNAL = 0x8
+STATUS_SLAB_REACH = 0x10
+
+SLAB_RECORD = 16         # doubles per bead record of a slab exchange buffer
 
 PAIR_FULL_SHELL = 0      # default: bitwise reproducible forces
 PAIR_HALF_SHELL = 1      # each pair once, partner force by atomics
@@ -40,6 +44,8 @@ EXPORTED = [
     "dpd_engine_set_slice_stress", "dpd_engine_slice_stress", "dpd_engine_set_monitor", "dpd_engine_monitor",
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
     "dpd_write_paraview", "dpd_engine_write_paraview", "dpd_engine_renormalise_mom",
+    "dpd_engine_slab_setup", "dpd_engine_slab_pack", "dpd_engine_slab_unpack", "dpd_engine_slab_counts",
+    "dpd_engine_bead_ids",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -128,6 +134,12 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_batch_create.argtypes = [C.POINTER(DpdParams), C.c_int32, C.POINTER(DpdBox), C.POINTER(vp)]
     L.dpd_batch_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 8
     L.dpd_batch_observables.argtypes = [vp, C.c_int32, C.POINTER(DpdObs)]
+    L.dpd_engine_slab_setup.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
+                                        C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
+    L.dpd_engine_slab_pack.argtypes = [vp, vp, vp, C.c_int64]
+    L.dpd_engine_slab_unpack.argtypes = [vp, vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.dpd_engine_slab_counts.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.dpd_engine_bead_ids.argtypes = [vp, vp, vp]
     L.dpd_engine_destroy.argtypes = [vp]
     L.dpd_engine_destroy.restype = None
     _lib = L
@@ -254,6 +266,37 @@ class DpdEngine:
                                                       len(t[4]), _p(t[4]), _p(t[5]), _p(t[6]), _p(t[7])),
                     "upload_topology")
 
+    def slab_setup(self, nz_global: int, z0: int, z1: int, ghost: int, n_owned: int, id_max: int, head, tail, k2,
+                   l0, first, second, k3, phi0) -> None:
+        """dpd_engine_slab_setup: this engine becomes the slab [z0, z1) of a box
+        of nz_global layers; the topology is the whole box's, by bead id."""
+        t = [np.ascontiguousarray(head, np.int64), np.ascontiguousarray(tail, np.int64),
+             np.ascontiguousarray(k2, np.float64), np.ascontiguousarray(l0, np.float64),
+             np.ascontiguousarray(first, np.int64), np.ascontiguousarray(second, np.int64),
+             np.ascontiguousarray(k3, np.float64), np.ascontiguousarray(phi0, np.float64)]
+        self._check(load().dpd_engine_slab_setup(self.h, int(nz_global), int(z0), int(z1), int(ghost), int(n_owned),
+                                                 int(id_max), len(t[0]), _p(t[0]), _p(t[1]), _p(t[2]), _p(t[3]),
+                                                 len(t[4]), _p(t[4]), _p(t[5]), _p(t[6]), _p(t[7])), "slab_setup")
+
+    def slab_pack(self, send_below: int, send_above: int, capacity: int) -> None:
+        """dpd_engine_slab_pack into two device buffers (addresses) of
+        (capacity + 1) * SLAB_RECORD doubles."""
+        self._check(load().dpd_engine_slab_pack(self.h, C.c_void_p(int(send_below)), C.c_void_p(int(send_above)),
+                                                int(capacity)), "slab_pack")
+
+    def slab_unpack(self, recv_below: int, recv_above: int) -> tuple:
+        """dpd_engine_slab_unpack from two device buffers; returns (owned, local) bead counts."""
+        no, nl = C.c_int64(0), C.c_int64(0)
+        self._check(load().dpd_engine_slab_unpack(self.h, C.c_void_p(int(recv_below)), C.c_void_p(int(recv_above)),
+                                                  C.byref(no), C.byref(nl)), "slab_unpack")
+        self.n = int(nl.value)
+        return int(no.value), int(nl.value)
+
+    def slab_counts(self) -> tuple:
+        no, nl = C.c_int64(0), C.c_int64(0)
+        self._check(load().dpd_engine_slab_counts(self.h, C.byref(no), C.byref(nl)), "slab_counts")
+        return int(no.value), int(nl.value)
+
     def set_pair_params(self, a, gamma) -> None:
         a = np.ascontiguousarray(a, np.float64)
         g = np.ascontiguousarray(gamma, np.float64)
@@ -289,6 +332,13 @@ class DpdEngine:
 
     def download_into(self, x=None, unpbc=None, v=None, f=None, stress=None) -> None:
         self._check(load().dpd_engine_download(self.h, _p(x), _p(unpbc), _p(v), _p(f), _p(stress)), "download")
+
+    def bead_ids(self) -> tuple:
+        """(ids, types) in upload order."""
+        ids = np.zeros(self.n, np.int64)
+        types = np.zeros(self.n, np.int32)
+        self._check(load().dpd_engine_bead_ids(self.h, _p(ids), _p(types)), "bead_ids")
+        return ids, types
 
     def cells(self) -> np.ndarray:
         c = np.zeros(self.n, dtype=np.int32)

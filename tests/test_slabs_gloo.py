@@ -1,6 +1,7 @@
 """The z-slab decomposition (osprey_dpd_b200.slabs) on the CPU: two and three
 gloo ranks, each stepping its slab plus ghost layers with the oracle (Philox
-pair noise), exchange ghosts and migrants every step; the gathered box
+pair noise), exchange ghosts and migrants every step (in two exchanges, or in
+the one combined exchange the device slab engine makes); the gathered box
 equals the single-box oracle run to rounding (the summation order inside a
 cell list differs).  A polymer solution (bonds across the slab faces and the
 global z face) and a bilayer centred on a slab face (bonds and angles across
@@ -45,7 +46,7 @@ def _free_port() -> int:
         return sk.getsockname()[1]
 
 
-def _worker(rank, world, port, q, kind="polymer"):
+def _worker(rank, world, port, q, kind="polymer", combined=False):
     os.environ.update(WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
                       MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
@@ -55,8 +56,13 @@ def _worker(rank, world, port, q, kind="polymer"):
         g = R.open_ranks("gloo", "cpu", timeout_s=120)
         dec = slabs.SlabDecomposition(_system(kind), g, ghost=2)
         counts = []
+        if combined:
+            dec.start_combined()
         for t in range(1, STEPS + 1):
-            dec.step(t, _oracle_engine, lambda e: e.state())
+            if combined:
+                dec.step_combined(t, _oracle_engine, lambda e: e.state())
+            else:
+                dec.step(t, _oracle_engine, lambda e: e.state())
             counts.append(len(dec.owned))
         out = dec.gather()
         g.close()
@@ -66,12 +72,12 @@ def _worker(rank, world, port, q, kind="polymer"):
         q.put((rank, "error", traceback.format_exc()))
 
 
-def _run(world, kind="polymer"):
+def _run(world, kind="polymer", combined=False):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q, kind)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, kind, combined)) for r in range(world)]
     for p in procs:
         p.start()
     res = {}
@@ -99,6 +105,31 @@ def test_slabs_equal_single_box(world, kind):
     res = _run(world, kind)
     _compare(res[0][1], ref, ids)
     assert sum(res[r][2][-1] for r in range(world)) == len(ids)   # every bead owned once
+
+
+@pytest.mark.parametrize("world,kind", [(2, "polymer"), (3, "polymer"), (2, "bilayer")])
+def test_combined_exchange_equals_single_box(world, kind):
+    """One exchange per step (migrants and the next ghosts together, the
+    device slab engine's form) gives the same box."""
+    ref, ids = _single_box(kind)
+    res = _run(world, kind, combined=True)
+    _compare(res[0][1], ref, ids)
+    assert sum(res[r][2][-1] for r in range(world)) == len(ids)
+
+
+def test_classify_rule():
+    sys.path.insert(0, ROOT)
+    from osprey_dpd_b200 import slabs as S
+    g, own = 2, 5                       # local layers 0..8: ghosts 0,1 and 7,8
+    lz = np.arange(-0, 9)
+    m = S.classify(lz, np.ones(9, bool), g, own)
+    bit = lambda k: [int(v) for v in (m >> k) & 1]
+    assert bit(S.TO_BELOW_MIG) == [1, 1, 0, 0, 0, 0, 0, 0, 0]
+    assert bit(S.TO_ABOVE_MIG) == [0, 0, 0, 0, 0, 0, 0, 1, 1]
+    assert bit(S.KEEP) == [0, 0, 1, 1, 1, 1, 1, 0, 0]
+    assert bit(S.TO_BELOW_GHOST) == [0, 0, 1, 1, 0, 0, 0, 0, 0]
+    assert bit(S.TO_ABOVE_GHOST) == [0, 0, 0, 0, 0, 1, 1, 0, 0]
+    assert not S.classify(lz, np.zeros(9, bool), g, own).any()   # ghosts go nowhere
 
 
 def test_single_rank_is_the_box(monkeypatch):
