@@ -301,20 +301,26 @@ void dfree(dpd_engine* e, void* p)
     }
 }
 
-// Grows *p to hold count elements; sets *moved when the address changes.
+// Grows *p to hold count elements (allocating max(count, room) when it grows);
+// sets *moved when the address changes.
 template <typename T>
-int ensure(dpd_engine* e, T** p, size_t& cap, size_t count, bool* moved)
+int ensure(dpd_engine* e, T** p, size_t& cap, size_t count, bool* moved, size_t room = 0)
 {
     if (*p && count <= cap) return DPD_OK;
     dfree(e, *p);
     *p = nullptr;
     cap = 0;
-    const int rc = dalloc(e, p, count ? count : 1);
+    const size_t want = std::max<size_t>(std::max<size_t>(count, room), 1);
+    const int rc = dalloc(e, p, want);
     if (rc) return rc;
-    cap = count ? count : 1;
+    cap = want;
     *moved = true;
     return DPD_OK;
 }
+
+// The allocation for count elements of a buffer whose count changes every
+// upload (a slab): n_headroom times count.
+size_t with_room(const dpd_engine* e, size_t count) { return (size_t)((double)count * e->n_headroom); }
 
 size_t real_size(const dpd_engine* e) { return e->precision == DPD_PRECISION_FP64 ? sizeof(double) : sizeof(float); }
 
@@ -779,7 +785,7 @@ int empty_topology(dpd_engine* e, bool keep_bonded)
     bool moved = false;
     int rc;
     if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved))) return rc;
-    CU(cudaMemset(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1)));
+    CU(cudaMemsetAsync(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1), e->s()));
     if (moved || (e->nbb && !keep_bonded)) {
         drop_graphs(e);
         e->nbb = 0;
@@ -1058,15 +1064,17 @@ static int stage_buffers(dpd_engine* e, int64_t n)
 {
     int rc;
     bool smoved = false;
-    if ((rc = ensure(e, &e->d_up, e->cap_up, 15 * (size_t)n + 8, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_cell, e->cap_up_cell, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * (size_t)n, &smoved))) return rc;
-    if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, (size_t)n, &smoved))) return rc;
+    // room for the bead counts of the next uploads too when they change every step (a slab)
+    const size_t m = (size_t)n;
+    if ((rc = ensure(e, &e->d_up, e->cap_up, 15 * m + 8, &smoved, 15 * with_room(e, m) + 8))) return rc;
+    if ((rc = ensure(e, &e->d_up_cell, e->cap_up_cell, m, &smoved, with_room(e, m)))) return rc;
+    if ((rc = ensure(e, &e->d_up_img, e->cap_up_img, m, &smoved, with_room(e, m)))) return rc;
+    if ((rc = ensure(e, &e->d_up_off, e->cap_up_off, 3 * m, &smoved, 3 * with_room(e, m)))) return rc;
+    if ((rc = ensure(e, &e->d_up_perm, e->cap_up_perm, m, &smoved, with_room(e, m)))) return rc;
     if ((rc = ensure(e, &e->d_up_err, e->cap_up_err, (size_t)kUpErrors + 2 + kMaxTypes, &smoved))) return rc;
     bool pmoved = false;
-    if ((rc = ensure(e, &e->d_prev_id, e->cap_prev_id, (size_t)n, &pmoved))) return rc;
-    if ((rc = ensure(e, &e->d_prev_type, e->cap_prev_type, (size_t)n, &pmoved))) return rc;
+    if ((rc = ensure(e, &e->d_prev_id, e->cap_prev_id, m, &pmoved, with_room(e, m)))) return rc;
+    if ((rc = ensure(e, &e->d_prev_type, e->cap_prev_type, m, &pmoved, with_room(e, m)))) return rc;
     if (pmoved) e->prev_n = -1;
     return DPD_OK;
 }
@@ -1228,7 +1236,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     CU(cudaMemsetAsync(e->d_count, 0, sizeof(int) * (size_t)e->ncell, st));
     if (any_off) {
         bool moved = false;
-        if ((rc = ensure(e, &e->d_off, e->cap_off, 3 * (size_t)n, &moved))) return rc;
+        if ((rc = ensure(e, &e->d_off, e->cap_off, 3 * (size_t)e->cap_n, &moved))) return rc;
         CU(cudaMemcpyAsync(e->d_off, e->d_up_off, 3 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
         if (moved || !e->off_active) drop_graphs(e);
     } else if (e->off_active) {
@@ -2407,10 +2415,10 @@ static int slab_topology(dpd_engine* e, bool check)
         if ((rc = check_launch(e, "k_slab_endpoints"))) return rc;
     }
     const int nblk = blocks_for(n, kThreads);
-    const size_t room = (size_t)((double)n * e->n_headroom);   // the count changes every step
-    if ((rc = ensure(e, &S.d_cnt, S.cap_cnt, room, &moved))) return rc;
-    if ((rc = ensure(e, &S.d_bsum, S.cap_bsum, (size_t)blocks_for(room, kThreads), &moved))) return rc;
-    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, room + 1, &moved))) return rc;
+    const size_t room = with_room(e, (size_t)n);   // the count changes every step
+    if ((rc = ensure(e, &S.d_cnt, S.cap_cnt, (size_t)n, &moved, room))) return rc;
+    if ((rc = ensure(e, &S.d_bsum, S.cap_bsum, (size_t)nblk, &moved, (size_t)blocks_for(room, kThreads)))) return rc;
+    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)n + 1, &moved, room + 1))) return rc;
     if ((rc = ensure(e, &e->d_csr_term, e->cap_csr_term, std::max<size_t>(S.nterm, 1), &moved))) return rc;
     k_slab_term_count<<<nblk, kThreads, 0, st>>>(n, check ? S.geom.n_owned : 0, T, e->d_pid_of, e->d_bond_h, e->d_bond_t,
                                                  e->d_ang[0], e->d_ang[1], e->d_ang[2], e->d_ang[3], S.d_cnt,
@@ -2428,11 +2436,11 @@ static int slab_topology(dpd_engine* e, bool check)
     if ((rc = check_launch(e, "k_slab_term_write"))) return rc;
     // every local bead runs through the bonded kernel (beads without terms
     // leave it at once): the bonded-bead list is 0..n-1
-    if ((rc = ensure(e, &e->d_ubuf, e->cap_ubuf, room, &moved))) return rc;
-    if ((rc = ensure(e, &e->d_Fb, e->cap_Fb, room, &moved))) return rc;
-    if ((rc = ensure(e, &e->d_Sb, e->cap_Sb, 9 * room, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_ubuf, e->cap_ubuf, (size_t)n, &moved, room))) return rc;
+    if ((rc = ensure(e, &e->d_Fb, e->cap_Fb, (size_t)n, &moved, room))) return rc;
+    if ((rc = ensure(e, &e->d_Sb, e->cap_Sb, 9 * (size_t)n, &moved, 9 * room))) return rc;
     if (!e->d_bb || S.cap_bb < (size_t)n) {
-        if ((rc = ensure(e, &e->d_bb, e->cap_bb, room, &moved))) return rc;
+        if ((rc = ensure(e, &e->d_bb, e->cap_bb, (size_t)n, &moved, room))) return rc;
         k_iota<<<blocks_for(e->cap_bb, kThreads), kThreads, 0, st>>>((int)e->cap_bb, e->d_bb);
         if ((rc = check_launch(e, "k_iota"))) return rc;
         S.cap_bb = e->cap_bb;
@@ -2607,10 +2615,12 @@ int dpd_engine_slab_pack(dpd_engine* e, double* send_below, double* send_above, 
     const int nblk = blocks_for(n, kThreads);
     int rc;
     bool moved = false;
-    if ((rc = ensure(e, &S.d_bcount, S.cap_bcount, (size_t)kSlabOuts * nblk, &moved))) return rc;
-    const size_t room = (size_t)((double)n * e->n_headroom);   // the count changes every step
-    if ((rc = ensure(e, &S.d_keep, S.cap_keep, (size_t)kSlabRec * room, &moved))) return rc;
-    if ((rc = ensure(e, &S.d_mine, S.cap_mine, (size_t)kSlabRec * room, &moved))) return rc;
+    const size_t room = with_room(e, (size_t)n);   // the count changes every step
+    if ((rc = ensure(e, &S.d_bcount, S.cap_bcount, (size_t)kSlabOuts * nblk, &moved,
+                     (size_t)kSlabOuts * blocks_for(room, kThreads))))
+        return rc;
+    if ((rc = ensure(e, &S.d_keep, S.cap_keep, (size_t)kSlabRec * n, &moved, (size_t)kSlabRec * room))) return rc;
+    if ((rc = ensure(e, &S.d_mine, S.cap_mine, (size_t)kSlabRec * n, &moved, (size_t)kSlabRec * room))) return rc;
     S.geom.cap = (int)capacity;
     cudaStream_t st = e->s();
     const int c = e->cur;

@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes,
     __syncthreads();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned diff = 0;
+    int c = -1;   // the bead's cell once it has passed every check
     if (b < n) {
         const int t = in.type[b];
         const int64_t idv = in.id[b];
@@ -89,16 +90,25 @@ __global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes,
                 }
             }
             if (bad) break;
-            const int c = (int)(B.cell_base + ci[0] + (long long)B.nc[0] * (ci[1] + (long long)B.nc[1] * ci[2]));
+            c = (int)(B.cell_base + ci[0] + (long long)B.nc[0] * (ci[1] + (long long)B.nc[1] * ci[2]));
             cell[b] = c;
             img[b] = img_pack(ii[0], ii[1], ii[2]);
 #pragma unroll
             for (int d = 0; d < 3; ++d) off[(size_t)d * n + b] = r[d];
             if (residual) *any_off = 1;
-            atomicAdd(&count[c], 1);
-            atomicAdd(&block_count[c / kScanChunk], 1);
             atomicAdd(&hist[t], 1);
         } while (false);
+    }
+    // cell and chunk counts, one atomic per distinct cell (chunk) and warp:
+    // beads uploaded in cell order (a slab's exchange) share them
+    const unsigned act = __ballot_sync(0xffffffffu, c >= 0);
+    if (c >= 0) {
+        const int lane = threadIdx.x & 31;
+        const unsigned peers = __match_any_sync(act, c);
+        if (lane == __ffs(peers) - 1) atomicAdd(&count[c], __popc(peers));
+        const int chunk = c / kScanChunk;
+        const unsigned cpeers = __match_any_sync(act, chunk);
+        if (lane == __ffs(cpeers) - 1) atomicAdd(&block_count[chunk], __popc(cpeers));
     }
     const unsigned wdiff = __reduce_or_sync(0xffffffffu, diff);
     if ((threadIdx.x & 31) == 0 && wdiff) atomicOr(prev.changed, wdiff);
