@@ -3,10 +3,11 @@ collectives a timed run takes -- a barrier on both sides of each timed
 region and the maximum of the ranks' device times -- plus the whole-job
 throughput computed from them.
 
-The step path does not shard across GPUs in this engine: every rank steps
-its own independent replica of the workload (its own seed), so the only
-cross-rank traffic is these timing collectives.  The same code drives NCCL
-between GPUs and gloo between CPU processes (the tests)."""
+In bench.py's multi-GPU runs every rank steps its own independent replica of
+the workload (its own seed), so the only cross-rank traffic there is these
+timing collectives; one box split over ranks is osprey_dpd_b200.slabs.  The
+same code drives NCCL between GPUs and gloo between CPU processes (the
+tests)."""
 from __future__ import annotations
 
 import datetime
