@@ -431,6 +431,17 @@ DPD_API int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, cons
 /* The current owned and local bead counts. */
 DPD_API int dpd_engine_slab_counts(dpd_engine* e, int64_t* n_owned, int64_t* n_local);
 
+/* Single-bead sums over this slab's owned beads, taken after a step and
+ * before its exchange (synchronous): n (owned beads), sum_v, sum_v2, sum_x,
+ * ang_mom (local frame), and the virial when the step was a sample step of
+ * the full-shell pair scheme (has_virial; each bead of a pair holds half of
+ * its virial there, so the ranks' sums count every pair once; bonds and bond
+ * pairs count at the one bead that holds them).  kT and pressure are left 0:
+ * the caller sums n, sum_v, sum_v2 and virial over the ranks (the FP64
+ * all-reduce of CMonitor::CalculateSingleBeadData's terms) and forms
+ * kT = sum_v2 / (3 n) and P = (sum_v2 + trace virial) / (3 V) of the whole box. */
+DPD_API int dpd_engine_slab_observables(dpd_engine* e, dpd_obs* out);
+
 /* ---- Pair forces without any allocation ---------------------------------
  * This entry point has no counterpart in the reference.  It is for callers
  * that may not allocate device memory at the moment they need forces: a host

@@ -2700,6 +2700,50 @@ int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, const double
     return DPD_OK;
 }
 
+int dpd_engine_slab_observables(dpd_engine* e, dpd_obs* out)
+{
+    if (!e) return DPD_E_ARG;
+    if (!e->slab) return fail(e, DPD_E_STATE, "not a slab (dpd_engine_slab_setup)");
+    if (!out) return fail(e, DPD_E_ARG, "null output");
+    if (e->slab->packed) return fail(e, DPD_E_STATE, "the sums are taken after a step, before the exchange");
+    CU(cudaSetDevice(e->device));
+    const int n = (int)e->n;
+    const int nb = blocks_for(n, kThreads);
+    // the virial of the latest step when it was a sample step; a pair's counts
+    // once over the ranks only when both beads hold half of it (full shell)
+    const bool virial = e->sampled && e->stepped && e->pair_scheme == DPD_PAIR_FULL_SHELL;
+    const int c = e->cur;
+    if (e->precision == DPD_PRECISION_FP64)
+        k_slab_obs_partials<double><<<nb, kThreads, 0, e->s()>>>(n, e->slab->geom.n_owned, e->d_bid[c], e->d_x[c],
+                                                                e->d_v[c],
+                                                                virial ? (const double*)e->d_stress : nullptr,
+                                                                e->d_partials);
+    else
+        k_slab_obs_partials<float><<<nb, kThreads, 0, e->s()>>>(n, e->slab->geom.n_owned, e->d_bid[c], e->d_x[c],
+                                                               e->d_v[c], virial ? (const float*)e->d_stress : nullptr,
+                                                               e->d_partials);
+    int rc = check_launch(e, "k_slab_obs_partials");
+    if (rc) return rc;
+    k_reduce_obs<<<1, 32 * kObsTerms, 0, e->s()>>>(nb, e->d_partials, e->d_obs);
+    if ((rc = check_launch(e, "k_reduce_obs"))) return rc;
+    CU(cudaMemcpyAsync(e->h_obs, e->d_obs, kObsTerms * sizeof(double), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    e->obs_valid = false;   // d_obs now holds the owned beads' sums
+    const double* h = e->h_obs;
+    memset(out, 0, sizeof *out);
+    out->step = e->stepped ? e->last_step : 0;
+    out->n = e->slab->geom.n_owned;
+    for (int d = 0; d < 3; ++d) {
+        out->sum_v[d] = h[d];
+        out->sum_v2[d] = h[3 + d];
+        out->sum_x[d] = h[15 + d];
+        out->ang_mom[d] = h[18 + d];
+    }
+    out->has_virial = virial ? 1 : 0;
+    for (int q = 0; q < 9; ++q) out->virial[q] = virial ? h[6 + q] : 0.0;
+    return DPD_OK;   // kT and pressure are the whole box's: left to the caller's sums over the ranks
+}
+
 int dpd_engine_slab_counts(dpd_engine* e, int64_t* n_owned, int64_t* n_local)
 {
     if (!e) return DPD_E_ARG;

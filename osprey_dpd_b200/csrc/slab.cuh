@@ -314,6 +314,58 @@ __global__ void __launch_bounds__(256) k_slab_place(int n, SlabGeom G, const int
 
 __global__ void k_slab_status(unsigned* __restrict__ status, unsigned bits) { *status |= bits; }
 
+// Single-bead sums over the owned beads only (upload indices below n_owned),
+// per block and term (term-major, the layout k_reduce_obs reads): momentum,
+// squared momentum, the per-bead virial (when stress is given), position and
+// angular momentum.  Summed over the ranks they are the whole box's: every
+// bead is owned once, and the per-bead virial counts a pair once when each
+// bead of it holds half (the full-shell kernel) and a bond or bond pair at
+// the one bead that holds it.
+template <typename real>
+__global__ void __launch_bounds__(256) k_slab_obs_partials(int n, int n_owned, const int* __restrict__ bid,
+                                                           const double* __restrict__ x,
+                                                           const double* __restrict__ v,
+                                                           const real* __restrict__ stress,
+                                                           double* __restrict__ partials)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[kObsTerms];
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) acc[q] = 0.0;
+    if (s < n && bid[s] < n_owned) {
+        const double xs[3] = {x[s], x[n + s], x[2 * (size_t)n + s]};
+        const double vs[3] = {v[s], v[n + s], v[2 * (size_t)n + s]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            acc[d] = vs[d];
+            acc[3 + d] = vs[d] * vs[d];
+            acc[15 + d] = xs[d];
+        }
+        if (stress) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) acc[6 + q] = (double)stress[(size_t)q * n + s];
+        }
+        acc[18] = xs[1] * vs[2] - xs[2] * vs[1];
+        acc[19] = -xs[0] * vs[2] + xs[2] * vs[0];
+        acc[20] = xs[0] * vs[1] - xs[1] * vs[0];
+    }
+    __shared__ double red[8][kObsTerms];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kObsTerms; ++q) {
+        double a = acc[q];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) red[wid][q] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsTerms) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += red[w][threadIdx.x];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = a;
+    }
+}
+
 // ---------------------------------------------------------- topology filter
 
 // The whole box's topology, by bond and bond-pair index and by bead id.

@@ -45,7 +45,7 @@ EXPORTED = [
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
     "dpd_write_paraview", "dpd_engine_write_paraview", "dpd_engine_renormalise_mom",
     "dpd_engine_slab_setup", "dpd_engine_slab_pack", "dpd_engine_slab_unpack", "dpd_engine_slab_counts",
-    "dpd_engine_bead_ids",
+    "dpd_engine_bead_ids", "dpd_engine_slab_observables",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -140,6 +140,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_slab_unpack.argtypes = [vp, vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.dpd_engine_slab_counts.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.dpd_engine_bead_ids.argtypes = [vp, vp, vp]
+    L.dpd_engine_slab_observables.argtypes = [vp, C.POINTER(DpdObs)]
     L.dpd_engine_destroy.argtypes = [vp]
     L.dpd_engine_destroy.restype = None
     _lib = L
@@ -291,6 +292,13 @@ class DpdEngine:
                                                   C.byref(no), C.byref(nl)), "slab_unpack")
         self.n = int(nl.value)
         return int(no.value), int(nl.value)
+
+    def slab_observables(self) -> dict:
+        """dpd_engine_slab_observables: the owned beads' single-bead sums
+        (after a step, before the exchange)."""
+        o = DpdObs()
+        self._check(load().dpd_engine_slab_observables(self.h, C.byref(o)), "slab_observables")
+        return o.as_dict()
 
     def slab_counts(self) -> tuple:
         no, nl = C.c_int64(0), C.c_int64(0)

@@ -447,15 +447,55 @@ class DeviceSlabs:
             sl.unpack()
 
     @staticmethod
-    def step_local(slabs, t: int) -> None:
+    def combine(parts, volume: float) -> Dict[str, float]:
+        """The whole box's single-bead observables from the slabs' owned sums
+        (dpd_engine_slab_observables): n, momentum, kT = sum v^2 / (3 n),
+        the virial and P = (sum v^2 + trace virial) / (3 V) (CMonitor::
+        CalculateSingleBeadData, Monitor.cpp:979-982)."""
+        n = sum(p["n"] for p in parts)
+        sv = np.sum([p["sum_v"] for p in parts], axis=0)
+        sv2 = np.sum([p["sum_v2"] for p in parts], axis=0)
+        vir = np.sum([p["virial"] for p in parts], axis=0)
+        v2 = float(np.sum(sv2))
+        has = all(p["has_virial"] for p in parts)
+        return {"n": int(n), "sum_v": sv, "sum_v2": sv2, "virial": vir if has else None, "kT": v2 / (3.0 * n),
+                "pressure": (v2 + vir[0] + vir[4] + vir[8]) / (3.0 * volume) if has else None}
+
+    def volume(self) -> float:
+        return float(np.prod(np.asarray(self.sys.cells, float) * np.asarray(self.sys.widths, float)))
+
+    @staticmethod
+    def step_local(slabs, t: int, observe: bool = False):
+        """Step t of every slab held by this process, then the exchange; with
+        observe, the whole box's observables of the step (combine)."""
         for sl in slabs:
             sl.eng.step(t, 1)
+        obs = DeviceSlabs.combine([sl.eng.slab_observables() for sl in slabs], slabs[0].volume()) if observe \
+            else None
         DeviceSlabs.exchange_local(slabs)
+        return obs
 
-    def step(self, t: int) -> None:
-        """Step t of the local box, then the exchange (one slab per rank)."""
+    def step(self, t: int, observe: bool = False):
+        """Step t of the local box, then the exchange (one slab per rank);
+        with observe, the whole box's observables of the step (the owned sums
+        all-reduced in FP64 over the process group)."""
         self.eng.step(t, 1)
+        obs = self._observe() if observe else None
         self._exchange()
+        return obs
+
+    def _observe(self) -> Dict[str, float]:
+        import torch
+        p = self.eng.slab_observables()
+        vec = np.concatenate([[p["n"]], p["sum_v"], p["sum_v2"], p["virial"], [1.0 if p["has_virial"] else 0.0]])
+        dev = self.g.device if self.g.device is not None else "cpu"
+        with torch.cuda.stream(self.stream):
+            t = torch.tensor(vec, dtype=torch.float64, device=dev)
+            self.g.dist.all_reduce(t)
+            r = t.cpu().numpy()
+        whole = {"n": int(round(r[0])), "sum_v": r[1:4], "sum_v2": r[4:7], "virial": r[7:16],
+                 "has_virial": r[16] == self.world}
+        return DeviceSlabs.combine([whole], self.volume())
 
     # -------------------------------------------------------------- state
     def owned_state(self) -> Dict[str, np.ndarray]:

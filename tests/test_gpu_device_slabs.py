@@ -82,6 +82,29 @@ def test_device_slabs_equal_single_box(world, kind):
     _compare(got, ref, ids)
 
 
+def test_device_slab_observables():
+    """The slabs' owned-bead sums combined (kT, pressure, virial; full-shell
+    FP64, every step a sample step) equal the whole box's observables."""
+    from osprey_dpd_b200 import engine as E, slabs as S
+    s = _system("bilayer")
+    e = E.DpdEngine.from_system(s, precision=E.FP64, device=0)
+    e.step(1, 4)
+    ref = e.observables()
+    e.close()
+    slabs = [S.DeviceSlabs(s, None, device=0, rank=r, world=2, precision=E.FP64) for r in range(2)]
+    S.DeviceSlabs.exchange_local(slabs)
+    for t in range(1, 5):
+        obs = S.DeviceSlabs.step_local(slabs, t, observe=True)
+    for sl in slabs:
+        sl.close()
+    assert obs["n"] == s.n
+    assert abs(obs["kT"] - ref["kT"]) <= 1e-10 * ref["kT"]
+    assert abs(obs["pressure"] - ref["pressure"]) <= 1e-9 * abs(ref["pressure"])
+    scale = float(np.max(np.abs(ref["virial"])))
+    np.testing.assert_allclose(obs["virial"], ref["virial"], rtol=0, atol=1e-9 * scale)
+    np.testing.assert_allclose(obs["sum_v"], ref["sum_v"], rtol=0, atol=1e-9)
+
+
 def test_device_slabs_mixed_precision():
     """Mixed precision, half-shell pair scheme: 3 steps within the
     mixed-precision bounds of the parity tests (1e-4 of the RMS)."""
@@ -181,20 +204,26 @@ def _worker(rank, world, port, q):
         g = R.open_ranks("gloo", "cpu", timeout_s=300)
         dec = slabs.DeviceSlabs(_system(), g, device=0, precision=E.FP64)
         for t in range(1, STEPS + 1):
-            dec.step(t)
+            obs = dec.step(t, observe=(t == STEPS))
         out = dec.gather()
         dec.close()
         g.close()
-        q.put((rank, out))
+        q.put((rank, out, obs))
     except Exception:
         import traceback
         q.put((rank, "error", traceback.format_exc()))
 
 
 def test_device_slabs_over_gloo_ranks():
+    """Two ranks, buffers through host copies; the observables of the last
+    step all-reduced over the group equal the whole box's."""
     from osprey_dpd_b200 import engine as E
     s = _system()
     ref, ids = _single_box(s, E.FP64)
+    e = E.DpdEngine.from_system(s, precision=E.FP64, device=0)
+    e.step(1, STEPS)
+    ref_obs = e.observables()
+    e.close()
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -211,3 +240,8 @@ def test_device_slabs_over_gloo_ranks():
     for r in range(2):
         assert res[r][1] != "error", res[r][2]
     _compare(res[0][1], ref, ids)
+    for r in range(2):
+        obs = res[r][2]
+        assert obs["n"] == s.n
+        assert abs(obs["kT"] - ref_obs["kT"]) <= 1e-9 * ref_obs["kT"]
+        assert abs(obs["pressure"] - ref_obs["pressure"]) <= 1e-8 * abs(ref_obs["pressure"])
