@@ -661,10 +661,11 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
             CU(cudaMemsetAsync(e->d_stress, 0, (size_t)9 * n * sizeof(real), st));
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
-        const int tiles = blocks_for(n, kPairBlock);
+        const int block = e->pair_scheme == DPD_PAIR_HALF_SHELL ? kHalfBlock : kPairBlock;
+        const int tiles = blocks_for(n, block);
         const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
-        CU(launch_step(e, kern, blocks_for(tiles, tpb), kPairBlock, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
+        CU(launch_step(e, kern, blocks_for(tiles, tpb), block, dyn, st, n, e->d_K, e->d_boxes, e->d_step,
                        (const real*)e->d_tab, e->d_cell[b], e->d_start, (const V4*)e->d_pos4, (const V4*)e->d_vel4,
                        (real*)e->d_F, (real*)e->d_stress, e->pair_hitcap, tpb, e->d_status,
                        (const double*)e->d_x[b]));

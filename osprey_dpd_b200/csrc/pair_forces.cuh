@@ -25,11 +25,19 @@
 namespace dpd {
 
 constexpr int kPairWarps = 4;
-constexpr int kPairBlock = 32 * kPairWarps;
+constexpr int kPairBlock = 32 * kPairWarps;   // full-shell and staged tiles
+// Half-shell tiles: two warps.  Measured on the B200 against four and eight
+// warps (same registers per SM): the mixed-precision kernel 2-3 % faster
+// (bilayer 77.1 vs 79.2 us, melt 886 vs 901 us), FP64 even; one warp slower.
+constexpr int kHalfBlock = 64;
 // Resident blocks per SM the pair kernels are compiled for: 8 (64 registers,
 // 32 warps) in FP32; the FP64 variants keep 6 to limit spills.
 template <typename real, bool MULTI = false> struct PairOcc {
     static constexpr int value = sizeof(real) == 8 ? 6 : 8;
+};
+// The same warps per SM for the half-shell kernel's smaller blocks.
+template <typename real, bool MULTI = false> struct HalfOcc {
+    static constexpr int value = PairOcc<real, MULTI>::value * kPairBlock / kHalfBlock;
 };
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
 // Cell pruning threshold on the squared distance to a cell's nearest point:
@@ -126,10 +134,10 @@ __host__ __device__ constexpr size_t pair_tables_bytes(int nt)
 {
     return ((3 * sizeof(real) * (size_t)nt * nt + 15) / 16) * 16;
 }
-template <typename real>
+template <typename real, int BLOCK = kPairBlock>
 __host__ __device__ constexpr size_t pair_smem_bytes(int nt, int hitcap, bool multi)
 {
-    return (multi ? 0 : pair_tables_bytes<real>(nt)) + sizeof(uint32_t) * hitcap * kPairBlock;
+    return (multi ? 0 : pair_tables_bytes<real>(nt)) + sizeof(uint32_t) * hitcap * BLOCK;
 }
 
 // Hit entry: candidate slot in bits 0..25, cell offsets + 1 (x, y, z) in
@@ -350,11 +358,11 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
 // counts with their exclusive prefix.
 template <typename real>
 struct HalfShared {
-    typename Vec4<real>::type* hpos;   // kPairBlock entries
-    typename Vec4<real>::type* hvel;   // kPairBlock entries
-    real* hxw;                         // kPairBlock entries (staged scheme only)
-    int* wcnt;                         // kPairBlock entries: hits of each thread
-    int* wexc;                         // kPairBlock entries: exclusive prefix inside the warp
+    typename Vec4<real>::type* hpos;   // one entry per thread of the block
+    typename Vec4<real>::type* hvel;   // one entry per thread
+    real* hxw;                         // one entry per thread (staged scheme only)
+    int* wcnt;                         // hits of each thread
+    int* wexc;                         // exclusive prefix of the hits inside the warp
 };
 
 // Hit-list entry formats of the two half-shell kernels.
@@ -379,7 +387,7 @@ __device__ __forceinline__ void stg_row_shift(int r, int& dy, int& dz)
 // w0 holds the cell widths of a single-box engine; a replica batch (MULTI)
 // reloads widths, tables and noise key per owner.  F (and on sample steps
 // stress) must be zero before the kernel.
-template <typename real, bool VIRIAL, bool MULTI, bool STAGED>
+template <typename real, bool VIRIAL, bool MULTI, bool STAGED, int BLOCK = kPairBlock>
 __device__ __forceinline__ void balanced_force_pass(
     int cnt, const uint32_t* __restrict__ lists, const HalfShared<real>& sh,
     const typename Vec4<real>::type* stg, int tile_base, const Box* __restrict__ boxes, const real* Tsh,
@@ -468,7 +476,7 @@ __device__ __forceinline__ void balanced_force_pass(
                 co = wcnt[o];
                 load_owner(o);
             }
-            const uint32_t ent = lists[e * kPairBlock + wbase + o];
+            const uint32_t ent = lists[e * BLOCK + wbase + o];
             ++e;
             int j;
             real dx, dy, dz;
@@ -531,7 +539,7 @@ __device__ __forceinline__ void balanced_force_pass(
 
 // This lane's listed pairs, each evaluated once: the force goes to the lane's
 // own accumulator and, negated, to the partner through atomics.
-template <typename real, bool VIRIAL>
+template <typename real, bool VIRIAL, int BLOCK>
 __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __restrict__ list,
                                                      const typename Vec4<real>::type& pi,
                                                      const typename Vec4<real>::type& vi, const real* __restrict__ T,
@@ -548,7 +556,7 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
     const int m2 = nt * nt;
     for (int k = 0; k < trip; ++k) {
         if (k < cnt) {
-            const uint32_t e = list[k * kPairBlock];
+            const uint32_t e = list[k * BLOCK];
             const int j = (int)(e & 0x03FFFFFFu);
             const V4 pj = pos4[j];
             const V4 vj = vel4[j];
@@ -585,7 +593,7 @@ __device__ __forceinline__ void pair_force_pass_half(int cnt, const uint32_t* __
 // its busiest lane) and keeps bead i's force in registers.  Measured faster
 // than the balanced pass for the FP64 and replica-batch variants, whose
 // register budgets the balanced pass exceeds.
-template <typename real, bool VIRIAL, bool MULTI>
+template <typename real, bool VIRIAL, bool MULTI, int BLOCK>
 __device__ __forceinline__ void half_shell_tile_lanes(
     int tile, int n, int nt, const Box* __restrict__ boxes, int64_t step, const real* __restrict__ tab,
     const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
@@ -595,7 +603,7 @@ __device__ __forceinline__ void half_shell_tile_lanes(
     typedef typename Vec4<real>::type V4;
     uint32_t* list = lists + threadIdx.x;
     {
-        const int i = tile * kPairBlock + threadIdx.x;
+        const int i = tile * BLOCK + threadIdx.x;
         const bool live = i < n;
         V4 pi, vi;
         int cx = 0, cy = 0, cz = 0;
@@ -674,7 +682,7 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                 for (int base = 0; base < trip; base += hitcap) {
                     const int clen = min(max(len - base, 0), hitcap);
                     if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
-                        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4,
+                        pair_force_pass_half<real, VIRIAL, BLOCK>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4,
                                                            acc, F, n, xs, i, B.L);
                         cnt = 0;
                     }
@@ -698,7 +706,7 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                             const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
                             const real ddy = piy - p[q].y, ddz = piz - p[q].z;
                             const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                            list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                            list[cnt * BLOCK] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
                             cnt += (r2 < real(1) && r2 > real(1e-18) && q < rem) ? 1 : 0;
                         }
                     }
@@ -709,13 +717,13 @@ __device__ __forceinline__ void half_shell_tile_lanes(
                         const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - pq.x;
                         const real ddy = piy - pq.y, ddz = piz - pq.z;
                         const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                        list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                        list[cnt * BLOCK] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
                         cnt += (r2 < real(1) && r2 > real(1e-18) && t < lim) ? 1 : 0;
                     }
                 }
             }
         }
-        pair_force_pass_half<real, VIRIAL>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n, xs, i,
+        pair_force_pass_half<real, VIRIAL, BLOCK>(cnt, list, pi, vi, T, nt, wx, wy, wz, keys, pos4, vel4, acc, F, n, xs, i,
                                            B.L);
         if (live) {
             atomicAdd(F + i, acc[0]);
@@ -735,12 +743,12 @@ __device__ __forceinline__ void half_shell_tile_lanes(
 template <typename real>
 __host__ __device__ constexpr size_t half_scratch_bytes()
 {
-    return (2 * 4 * sizeof(real) + 2 * sizeof(int)) * (size_t)kPairBlock;
+    return (2 * 4 * sizeof(real) + 2 * sizeof(int)) * (size_t)kHalfBlock;
 }
 template <typename real>
 __host__ __device__ constexpr size_t half_smem_bytes(int nt, int hitcap, bool multi)
 {
-    return pair_smem_bytes<real>(nt, hitcap + 1, multi) + half_scratch_bytes<real>();
+    return pair_smem_bytes<real, kHalfBlock>(nt, hitcap + 1, multi) + half_scratch_bytes<real>();
 }
 template <typename real>
 __device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
@@ -748,10 +756,10 @@ __device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
     typedef typename Vec4<real>::type V4;
     HalfShared<real> sh;
     sh.hpos = reinterpret_cast<V4*>(base);
-    sh.hvel = sh.hpos + kPairBlock;
+    sh.hvel = sh.hpos + kHalfBlock;
     sh.hxw = nullptr;
-    sh.wcnt = reinterpret_cast<int*>(sh.hvel + kPairBlock);
-    sh.wexc = sh.wcnt + kPairBlock;
+    sh.wcnt = reinterpret_cast<int*>(sh.hvel + kHalfBlock);
+    sh.wexc = sh.wcnt + kHalfBlock;
     return sh;
 }
 
@@ -764,11 +772,11 @@ __device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
 // The partner's share is added with global atomics, so the FP32 summation
 // order (and the last bits) vary from run to run.  The pair virial goes whole
 // to bead i, the reference's convention (CNTCell.cpp:1283-1301).
-// One tile of kPairBlock slots; `lists` the block's hit lists (this thread's
+// One tile of BLOCK slots; `lists` the block's hit lists (this thread's
 // column at lists + threadIdx.x), Tsh the staged pair tables (single box), sh
 // the balanced pass's scratch.  Called by every thread of the block for the
 // same tile.
-template <typename real, bool VIRIAL, bool MULTI>
+template <typename real, bool VIRIAL, bool MULTI, int BLOCK>
 __device__ __forceinline__ void half_shell_tile(
     int tile, int n, int nt, const Box* __restrict__ boxes, int64_t step, const real* __restrict__ tab,
     const real* Tsh, const int* __restrict__ cell, const int* __restrict__ start,
@@ -778,7 +786,7 @@ __device__ __forceinline__ void half_shell_tile(
 {
     typedef typename Vec4<real>::type V4;
     uint32_t* list = lists + threadIdx.x;
-    const int i = tile * kPairBlock + threadIdx.x;
+    const int i = tile * BLOCK + threadIdx.x;
     const bool live = i < n;
     V4 pi, vi;
     int cx = 0, cy = 0, cz = 0;
@@ -803,7 +811,7 @@ __device__ __forceinline__ void half_shell_tile(
     const real wx = (real)B.w[0], wy = (real)B.w[1], wz = (real)B.w[2];
     const real w0[3] = {wx, wy, wz};   // the box of a single-box engine (MULTI reloads per owner)
     const real pxm = pi.x + wx, px0 = pi.x, pxp = pi.x - wx;
-    const int tile_base = tile * kPairBlock;
+    const int tile_base = tile * BLOCK;
     int cnt = 0;
     // a row's second segment (the cell across the periodic x boundary) exists
     // only for beads in the first or last cell column: warps with none skip it
@@ -857,7 +865,7 @@ __device__ __forceinline__ void half_shell_tile(
             for (int base = 0; base < trip; base += hitcap) {
                 const int clen = min(max(len - base, 0), hitcap);
                 if (__any_sync(0xffffffffu, cnt + clen > hitcap)) {
-                    balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh,
+                    balanced_force_pass<real, VIRIAL, MULTI, false, BLOCK>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh,
                                                                     tab, nt, keys0, w0, step, pos4, vel4, F, stress,
                                                                     n, xs);
                     cnt = 0;
@@ -889,7 +897,7 @@ __device__ __forceinline__ void half_shell_tile(
                         const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - p[q].x;
                         const real ddy = piy - p[q].y, ddz = piz - p[q].z;
                         const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                        list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                        list[cnt * BLOCK] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
                         cnt += (r2 < real(1) && q < rem) ? 1 : 0;
                     }
                 }
@@ -900,13 +908,13 @@ __device__ __forceinline__ void half_shell_tile(
                     const real ddx = (ge2 ? pxp : (ge1 ? px0 : pxm)) - pq.x;
                     const real ddy = piy - pq.y, ddz = piz - pq.z;
                     const real r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                    list[cnt * kPairBlock] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
+                    list[cnt * BLOCK] = (uint32_t)jq | (ge2 ? code_p : (ge1 ? code_0 : code_m));
                     cnt += (r2 < real(1) && t < lim) ? 1 : 0;
                 }
             }
         }
     }
-    balanced_force_pass<real, VIRIAL, MULTI, false>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh, tab, nt, keys0,
+    balanced_force_pass<real, VIRIAL, MULTI, false, BLOCK>(cnt, lists, sh, nullptr, tile_base, boxes, Tsh, tab, nt, keys0,
                                                     w0, step, pos4, vel4, F, stress, n, xs);
 }
 
@@ -918,7 +926,7 @@ constexpr bool kHalfBalanced = sizeof(real) == 4 && !MULTI;
 
 // F must be zero on entry, and on sample steps (VIRIAL) the stress array too.
 template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pair_forces_half(
+__global__ void __launch_bounds__(kHalfBlock, HalfOcc<real, MULTI>::value) k_pair_forces_half(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
@@ -932,9 +940,9 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     real* Tsh = reinterpret_cast<real*>(pair_dyn);
     unsigned char* lbase = pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt));
     uint32_t* lists = reinterpret_cast<uint32_t*>(lbase);
-    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)(hitcap + 1) * kPairBlock);
+    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)(hitcap + 1) * kHalfBlock);
     if (!MULTI)
-        for (int k = threadIdx.x; k < 3 * nt * nt; k += kPairBlock) Tsh[k] = tab[k];
+        for (int k = threadIdx.x; k < 3 * nt * nt; k += kHalfBlock) Tsh[k] = tab[k];
     const int64_t step = *step_ptr;
     uint32_t keys0[10];
     {
@@ -945,12 +953,12 @@ __global__ void __launch_bounds__(kPairBlock, PairOcc<real, MULTI>::value) k_pai
     __syncthreads();   // tables
     const int tile0 = blockIdx.x * tiles_per_block;
     for (int tile = tile0; tile < tile0 + tiles_per_block; ++tile) {
-        if (tile * kPairBlock >= n) break;
+        if (tile * kHalfBlock >= n) break;
         if (kHalfBalanced<real, MULTI>)
-            half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
+            half_shell_tile<real, VIRIAL, MULTI, kHalfBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
                                                  stress, hitcap, lists, sh, keys0, xs);
         else
-            half_shell_tile_lanes<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
+            half_shell_tile_lanes<real, VIRIAL, MULTI, kHalfBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
                                                        F, stress, hitcap, lists, xs);
     }
 }

@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
             before += w < warp ? v : 0;
         }
         if (H > kStgRows) {   // block-uniform
-            half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
-                                                 stress, hitcap, lists, sh, keys0, xs);
+            half_shell_tile<real, VIRIAL, MULTI, kPairBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4,
+                                                             vel4, F, stress, hitcap, lists, sh, keys0, xs);
             continue;
         }
         const int h = before + __popc(fb & ((2u << lane) - 1u)) - 1;
@@ -205,8 +205,8 @@ __global__ void __launch_bounds__(kPairBlock, StgOcc<real>::value) k_pair_forces
         }
         const int S = (int)(all >> 32), NT = (int)(all & 0xFFFFFFFFll);
         if (S > cap || NT > kStgCells) {   // block-uniform
-            half_shell_tile<real, VIRIAL, MULTI>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
-                                                 stress, hitcap, lists, sh, keys0, xs);
+            half_shell_tile<real, VIRIAL, MULTI, kPairBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4,
+                                                             vel4, F, stress, hitcap, lists, sh, keys0, xs);
             continue;
         }
         if (t < 5 * H) {
