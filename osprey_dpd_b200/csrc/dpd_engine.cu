@@ -87,6 +87,7 @@ struct dpd_engine {
     double n_headroom = 1.0;    // their growth factor (a slab's bead count changes every step)
     SlabState* slab = nullptr;  // set by dpd_engine_slab_setup
     bool host_ids_stale = false;   // h_id / h_type lag an upload from device memory
+    bool type_count_stale = false;  // type_count lags a trusted upload (still in d_up_err)
     int64_t launches = 0;
     bool uploaded = false;
     bool stepped = false;
@@ -811,6 +812,19 @@ int host_ids(dpd_engine* e)
     return DPD_OK;
 }
 
+// Beads per type of the last upload, read from the validation's counts when a
+// trusted upload left them on the device.
+int host_type_count(dpd_engine* e)
+{
+    if (!e->type_count_stale) return DPD_OK;
+    std::vector<int> h((size_t)e->ntypes);
+    CU(cudaMemcpyAsync(h.data(), e->d_up_err + kUpErrors + 2, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, e->s()));
+    CU(cudaStreamSynchronize(e->s()));
+    e->type_count.assign(h.begin(), h.end());
+    e->type_count_stale = false;
+    return DPD_OK;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1081,7 +1095,7 @@ static int stage_buffers(dpd_engine* e, int64_t n)
 }
 
 static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
-                         const UploadIn& in);
+                         const UploadIn& in, bool trusted = false);
 
 static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
                        const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
@@ -1119,9 +1133,13 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
 }
 
 // Validation, binning and placement of a staged bead set (in: device arrays
-// in the staging buffers; id and type: the same beads on the host).
+// in the staging buffers; id and type: the same beads on the host, or null
+// for an upload from device memory).  trusted: records the engine formed
+// itself (a slab's exchange); the host then neither reads the validation
+// back nor waits at the end (a failing bead sets DPD_STATUS_INTERNAL on the
+// device instead), so the upload is queued without a host wait.
 static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
-                         const UploadIn& in)
+                         const UploadIn& in, bool trusted)
 {
     cudaStream_t st = e->s();
     int rc;
@@ -1133,17 +1151,25 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     int herr[kUpErrors + 2 + kMaxTypes];
     for (int k = 0; k < kUpErrors; ++k) herr[k] = INT_MAX;
     for (int k = kUpErrors; k < kUpErrors + 2 + kMaxTypes; ++k) herr[k] = 0;
-    CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
+    if (trusted) {
+        // no error is read back: a large sentinel for the atomicMin slots, zero for the rest
+        CU(cudaMemsetAsync(e->d_up_err, 0x7f, sizeof(int) * kUpErrors, st));
+        CU(cudaMemsetAsync(e->d_up_err + kUpErrors, 0, sizeof(int) * (2 + kMaxTypes), st));
+    } else {
+        CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
+    }
     const UploadPrev prev{e->d_prev_id, e->d_prev_type, reinterpret_cast<unsigned*>(e->d_up_err + kUpErrors + 1),
                           e->d_up_err + kUpErrors + 2};
     const bool prev_ok = e->prev_n == n;   // d_prev_* hold the last complete upload of n beads
     k_up_check<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, (int)e->hboxes.size(), e->ntypes, e->d_boxes, in,
                                                             e->d_up_cell, e->d_up_img, e->d_up_off, e->d_count,
                                                             e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors,
-                                                            prev);
+                                                            prev, trusted ? e->d_status : (unsigned*)nullptr);
     if ((rc = check_launch(e, "k_up_check"))) return rc;
-    CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
+    if (!trusted) {
+        CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+    }
     e->prev_n = -1;   // d_prev_* now hold this upload, complete only once it succeeds
     int bad = INT_MAX, kind = -1;
     for (int k = 0; k < kUpErrors; ++k)
@@ -1168,7 +1194,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
             default: return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
         }
     }
-    const bool any_off = herr[kUpErrors] != 0;
+    const bool any_off = trusted || herr[kUpErrors] != 0;   // trusted: not read back, so always carried
     // (re)allocate per-bead buffers when they are too small (strides follow the
     // bead count, so smaller counts fit); new addresses or another bead count
     // invalidate the captured graphs
@@ -1245,11 +1271,17 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     }
     e->off_active = any_off;
     CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)n, st));
-    CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
+    // a trusted upload's failing beads are reported through the status word
+    if (!trusted) CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
     // host copies of ids and types, refreshed only when the device saw them
-    // change; beads per type counted by k_up_check
-    const unsigned changed = prev_ok ? (unsigned)herr[kUpErrors + 1] : 3u;
-    e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
+    // change; beads per type counted by k_up_check (read later when trusted)
+    const unsigned changed = (prev_ok && !trusted) ? (unsigned)herr[kUpErrors + 1] : 3u;
+    if (trusted) {
+        e->type_count_stale = true;
+    } else {
+        e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
+        e->type_count_stale = false;
+    }
     if (!id || !type) {
         // an upload from device memory: the host copies are fetched when needed
         if (changed & 3u) {
@@ -1264,8 +1296,9 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         if (e->host_ids_stale || (changed & 2u) || e->h_type.size() != (size_t)n) e->h_type.assign(type, type + n);
         e->host_ids_stale = false;
     }
-    CU(cudaStreamSynchronize(st));
-    *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine is in flight after the sync
+    // (trusted: the caller waited for every kernel before the upload was queued)
+    if (!trusted) CU(cudaStreamSynchronize(st));
+    *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine that publishes the status is in flight
     rc = empty_topology(e, same_n);
     if (rc) return rc;
     e->uploaded = true;
@@ -1799,6 +1832,7 @@ int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bon
     if (!out) return fail(e, DPD_E_ARG, "null output");
     if (!e->mon_set) return fail(e, DPD_E_STATE, "dpd_engine_set_monitor has not been called for these beads");
     CU(cudaSetDevice(e->device));
+    if (int rc0 = host_type_count(e)) return rc0;
     const int n = (int)e->n, T = e->ntypes;
     const size_t nsums = 6 + (size_t)T + e->mon_nbt + 2 + e->mon_npt + 5 * (size_t)e->mon_nbpt;
     CU(cudaMemsetAsync(e->d_mon_sums, 0, nsums * sizeof(double), e->s()));
@@ -2689,11 +2723,13 @@ int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, const double
     const int* upi = reinterpret_cast<const int*>(up + 13 * (size_t)nn);
     in.type = upi;
     in.movable = reinterpret_cast<const unsigned char*>(upi + 2 * (size_t)nn);
-    if ((rc = upload_staged(e, nn, nullptr, nullptr, nullptr, in))) return rc;
-    if (status) {   // the step's non-fatal bits (cell skips) survive the exchange
+    // the status word starts the next step with the step's non-fatal bits (cell skips)
+    CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
+    if (status) {
         k_slab_status<<<1, 1, 0, st>>>(e->d_status, status);
         if ((rc = check_launch(e, "k_slab_status"))) return rc;
     }
+    if ((rc = upload_staged(e, nn, nullptr, nullptr, nullptr, in, true))) return rc;
     S.geom.n_owned = hs[0];
     if (S.topo && (rc = slab_topology(e, true))) return rc;
     if (n_owned) *n_owned = hs[0];
