@@ -344,6 +344,83 @@ def e2e_run(engine_mod, system, precision: int, reps: int, dev, torch, shape=Non
     return times, (h2d + topo_bytes) / E2E_PERIOD, d2h / E2E_PERIOD
 
 
+def run_slab_exchange(args, dev, torch):
+    """The device slab engine on one GPU: the workload split into
+    args.slab_exchange z-slabs, every slab held by this process
+    (DeviceSlabs.step_local, buffers swapped by device copies).  Wall clock
+    per phase with the slabs' streams drained in between: the steps of all
+    slabs, the pack, the buffer swap and the unpack (next local box, upload,
+    topology filter); the whole box in one engine beside it (single-step
+    calls).  On several GPUs the slabs' steps and exchanges run concurrently;
+    this measures what one exchange costs, not a scaling curve."""
+    import time
+    from osprey_dpd_b200 import engine as E, slabs as S
+    system, desc = workload(args.workload)
+    prec = E.FP64 if args.precision == "fp64" else E.MIXED
+    scheme = {"full": E.PAIR_FULL_SHELL, "staged": E.PAIR_STAGED}.get(args.pair_scheme, E.PAIR_HALF_SHELL)
+    W = args.slab_exchange
+    dn = dev.index
+    e = E.DpdEngine.from_system(system, precision=prec, device=dn)
+    e.set_pair_scheme(scheme)
+    e.step(1, args.warmup)
+    e.status()
+    t0 = time.perf_counter()
+    for t in range(args.warmup + 1, args.warmup + 1 + args.steps):
+        e.step(t, 1)
+    e.status()
+    single = (time.perf_counter() - t0) / args.steps * 1e3
+    e.close()
+    sl = [S.DeviceSlabs(system, None, device=dn, rank=r, world=W, precision=prec, pair_scheme=scheme)
+          for r in range(W)]
+    S.DeviceSlabs.exchange_local(sl)
+    for t in range(1, args.warmup + 1):
+        S.DeviceSlabs.step_local(sl, t)
+    ph = {"steps": 0.0, "pack": 0.0, "swap": 0.0, "unpack": 0.0}
+
+    def drain():
+        for x in sl:
+            x.stream.synchronize()
+
+    for t in range(args.warmup + 1, args.warmup + 1 + args.steps):
+        a = time.perf_counter()
+        for x in sl:
+            x.eng.step(t, 1)
+        drain()
+        b = time.perf_counter()
+        for x in sl:
+            x.pack()
+        drain()
+        c = time.perf_counter()
+        for r, x in enumerate(sl):
+            with torch.cuda.stream(x.stream):
+                x.bufs[2].copy_(sl[(r - 1) % W].bufs[1])
+                x.bufs[3].copy_(sl[(r + 1) % W].bufs[0])
+        drain()
+        d = time.perf_counter()
+        for x in sl:
+            x.unpack()
+        drain()
+        f = time.perf_counter()
+        ph["steps"] += b - a
+        ph["pack"] += c - b
+        ph["swap"] += d - c
+        ph["unpack"] += f - d
+    status = [x.eng.status() for x in sl]
+    owned = sum(x.n_owned for x in sl)
+    local = [x.n_local for x in sl]
+    for x in sl:
+        x.close()
+    ms = {k: v / args.steps * 1e3 for k, v in ph.items()}
+    return {"metric": "device slab engine on one GPU: ms per step and per exchange, all slabs together",
+            "impl": "slab_exchange", "config": {"workload": desc, "slabs": W, "ghost_layers": 2,
+                                                "precision": args.precision if args.precision != "both" else "mixed",
+                                                "pair_scheme": pair_scheme_name((0, 0, 0, scheme))},
+            "steps": args.steps, "warmup": args.warmup, "single_box_ms_per_step": single,
+            "slabs_ms": ms, "exchange_ms": ms["pack"] + ms["swap"] + ms["unpack"],
+            "owned_beads": owned, "local_beads": local, "status_bits": status,
+            "timing": "wall clock per phase, every slab's stream drained between phases; one process, one GPU"}
+
+
 def run_replica_sweep(args, dev, torch, E):
     """512 independent A/B replicas (box edges 8..24, A fraction 0.1..0.5,
     a_AB 25 -> 60, own seeds): one batch advanced as a captured 100-step CUDA
@@ -556,6 +633,9 @@ def main():
                     help="skip the 6.3M-bead melt and the 512-replica sweep keys of the default line")
     ap.add_argument("--slices", type=int, default=0,
                     help="also time the slice stress profile over this many z slices on sample steps")
+    ap.add_argument("--slab-exchange", type=int, default=0,
+                    help="time the device slab engine instead: the workload split into this many z-slabs held "
+                         "by this process on its one GPU (steps and exchanges, wall clock per phase)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -571,6 +651,12 @@ def main():
     group = R.open_ranks("nccl", dev)
     from osprey_dpd_b200 import engine as E
 
+    if args.slab_exchange:
+        line = run_slab_exchange(args, dev, torch)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        group.close()
+        return 0
     if args.workload == "replicas":
         line = run_replica_sweep(args, dev, torch, __import__("osprey_dpd_b200.engine", fromlist=["x"]))
         if rank == 0:

@@ -786,7 +786,8 @@ int empty_topology(dpd_engine* e, bool keep_bonded)
 {
     bool moved = false;
     int rc;
-    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_csr_ptr, e->cap_csr_ptr, (size_t)e->n + 1, &moved, with_room(e, (size_t)e->n) + 1)))
+        return rc;
     CU(cudaMemsetAsync(e->d_csr_ptr, 0, sizeof(int) * ((size_t)e->n + 1), e->s()));
     if (moved || (e->nbb && !keep_bonded)) {
         drop_graphs(e);
