@@ -87,7 +87,6 @@ struct dpd_engine {
     double n_headroom = 1.0;    // their growth factor (a slab's bead count changes every step)
     SlabState* slab = nullptr;  // set by dpd_engine_slab_setup
     bool host_ids_stale = false;   // h_id / h_type lag an upload from device memory
-    bool type_count_stale = false;  // type_count lags a trusted upload (still in d_up_err)
     int64_t launches = 0;
     bool uploaded = false;
     bool stepped = false;
@@ -813,19 +812,6 @@ int host_ids(dpd_engine* e)
     return DPD_OK;
 }
 
-// Beads per type of the last upload, read from the validation's counts when a
-// trusted upload left them on the device.
-int host_type_count(dpd_engine* e)
-{
-    if (!e->type_count_stale) return DPD_OK;
-    std::vector<int> h((size_t)e->ntypes);
-    CU(cudaMemcpyAsync(h.data(), e->d_up_err + kUpErrors + 2, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, e->s()));
-    CU(cudaStreamSynchronize(e->s()));
-    e->type_count.assign(h.begin(), h.end());
-    e->type_count_stale = false;
-    return DPD_OK;
-}
-
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1096,111 +1082,15 @@ static int stage_buffers(dpd_engine* e, int64_t n)
 }
 
 static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
-                         const UploadIn& in, bool trusted = false);
+                         const UploadIn& in);
 
-static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
-                       const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
-                       const double* f3)
+// The per-bead state buffers for n beads: (re)allocated when too small
+// (strides follow the bead count, so smaller counts fit; n_headroom leaves
+// room for counts that change every upload); new addresses or another bead
+// count invalidate the captured graphs.
+static int ensure_beads(dpd_engine* e, int64_t n)
 {
-    if (!e) return DPD_E_ARG;
-    if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
-    if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
-    CU(cudaSetDevice(e->device));
-    if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
-    CU(cudaStreamSynchronize(e->s()));
-    cudaStream_t st = e->s();
-    // the caller's arrays, copied as they are (pinned buffers make these DMA
-    // copies) into the staging buffers
-    int rc;
-    if ((rc = stage_buffers(e, n))) return rc;
-    double* up = e->d_up;
-    int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
-    unsigned char* upm = reinterpret_cast<unsigned char*>(upi + 2 * (size_t)n);
-    const size_t v3b = 3 * sizeof(double) * (size_t)n;
-    UploadIn in{};
-    in.x = up;
-    CU(cudaMemcpyAsync(up, x3, v3b, cudaMemcpyHostToDevice, st));
-    if (unpbc3) { in.u = up + 3 * (size_t)n; CU(cudaMemcpyAsync(up + 3 * (size_t)n, unpbc3, v3b, cudaMemcpyHostToDevice, st)); }
-    in.v = up + 6 * (size_t)n;
-    CU(cudaMemcpyAsync(up + 6 * (size_t)n, v3, v3b, cudaMemcpyHostToDevice, st));
-    if (f3) { in.f = up + 9 * (size_t)n; CU(cudaMemcpyAsync(up + 9 * (size_t)n, f3, v3b, cudaMemcpyHostToDevice, st)); }
-    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)n);
-    CU(cudaMemcpyAsync(up + 12 * (size_t)n, id, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
-    in.type = upi;
-    CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
-    if (box) { in.box = upi + n; CU(cudaMemcpyAsync(upi + n, box, sizeof(int) * n, cudaMemcpyHostToDevice, st)); }
-    if (movable) { in.movable = upm; CU(cudaMemcpyAsync(upm, movable, (size_t)n, cudaMemcpyHostToDevice, st)); }
-    return upload_staged(e, n, box, id, type, in);
-}
-
-// Validation, binning and placement of a staged bead set (in: device arrays
-// in the staging buffers; id and type: the same beads on the host, or null
-// for an upload from device memory).  trusted: records the engine formed
-// itself (a slab's exchange); the host then neither reads the validation
-// back nor waits at the end (a failing bead sets DPD_STATUS_INTERNAL on the
-// device instead), so the upload is queued without a host wait.
-static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
-                         const UploadIn& in, bool trusted)
-{
-    cudaStream_t st = e->s();
-    int rc;
-    // validation and binning (CSimBox::AssignBeadstoCells, SimBox.cpp:715-762:
-    // ix = (long)(x/w), box-local coordinates); nothing of the state changes yet
-    // herr: the first bead of each error kind, any residual unPBC offset,
-    // the bits of ids / types that differ from the previous upload, and the
-    // beads per type
-    int herr[kUpErrors + 2 + kMaxTypes];
-    for (int k = 0; k < kUpErrors; ++k) herr[k] = INT_MAX;
-    for (int k = kUpErrors; k < kUpErrors + 2 + kMaxTypes; ++k) herr[k] = 0;
-    if (trusted) {
-        // no error is read back: a large sentinel for the atomicMin slots, zero for the rest
-        CU(cudaMemsetAsync(e->d_up_err, 0x7f, sizeof(int) * kUpErrors, st));
-        CU(cudaMemsetAsync(e->d_up_err + kUpErrors, 0, sizeof(int) * (2 + kMaxTypes), st));
-    } else {
-        CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
-    }
-    const UploadPrev prev{e->d_prev_id, e->d_prev_type, reinterpret_cast<unsigned*>(e->d_up_err + kUpErrors + 1),
-                          e->d_up_err + kUpErrors + 2};
-    const bool prev_ok = e->prev_n == n;   // d_prev_* hold the last complete upload of n beads
-    k_up_check<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, (int)e->hboxes.size(), e->ntypes, e->d_boxes, in,
-                                                            e->d_up_cell, e->d_up_img, e->d_up_off, e->d_count,
-                                                            e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors,
-                                                            prev, trusted ? e->d_status : (unsigned*)nullptr);
-    if ((rc = check_launch(e, "k_up_check"))) return rc;
-    if (!trusted) {
-        CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-    }
-    e->prev_n = -1;   // d_prev_* now hold this upload, complete only once it succeeds
-    int bad = INT_MAX, kind = -1;
-    for (int k = 0; k < kUpErrors; ++k)
-        if (herr[k] < bad) { bad = herr[k]; kind = k; }
-    if (kind >= 0) {
-        CU(cudaMemset(e->d_count, 0, sizeof(int) * (size_t)e->ncell));
-        CU(cudaMemset(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk));
-        switch (kind) {
-            case kUpType: return fail(e, DPD_E_ARG, "bead type out of range");
-            case kUpId: return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
-            case kUpBox: return fail(e, DPD_E_ARG, "bead box index out of range");
-            case kUpNonFinite: return fail(e, DPD_E_BOX, "non-finite bead state");
-            case kUpOutside: {
-                char msg[160];
-                if (id)
-                    snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)bad,
-                             (long long)id[bad]);
-                else
-                    snprintf(msg, sizeof msg, "bead %lld lies outside the box", (long long)bad);
-                return fail(e, DPD_E_BOX, msg);
-            }
-            default: return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
-        }
-    }
-    const bool any_off = trusted || herr[kUpErrors] != 0;   // trusted: not read back, so always carried
-    // (re)allocate per-bead buffers when they are too small (strides follow the
-    // bead count, so smaller counts fit); new addresses or another bead count
-    // invalidate the captured graphs
-    const bool same_n = e->n == n;
-    if (!same_n) drop_graphs(e);
+    if (n != e->n) drop_graphs(e);
     if (n > e->cap_n) {
         // a slab keeps the whole box's topology arrays across its uploads
         if (!e->slab) release_topology(e);
@@ -1242,6 +1132,99 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         if ((rc = dalloc(e, &e->d_out_cell, (size_t)cap))) return rc;
         e->cap_n = cap;
     }
+    return DPD_OK;
+}
+
+
+static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                       const uint8_t* movable, const double* x3, const double* unpbc3, const double* v3,
+                       const double* f3)
+{
+    if (!e) return DPD_E_ARG;
+    if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
+    if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
+    CU(cudaSetDevice(e->device));
+    if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
+    CU(cudaStreamSynchronize(e->s()));
+    cudaStream_t st = e->s();
+    // the caller's arrays, copied as they are (pinned buffers make these DMA
+    // copies) into the staging buffers
+    int rc;
+    if ((rc = stage_buffers(e, n))) return rc;
+    double* up = e->d_up;
+    int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
+    unsigned char* upm = reinterpret_cast<unsigned char*>(upi + 2 * (size_t)n);
+    const size_t v3b = 3 * sizeof(double) * (size_t)n;
+    UploadIn in{};
+    in.x = up;
+    CU(cudaMemcpyAsync(up, x3, v3b, cudaMemcpyHostToDevice, st));
+    if (unpbc3) { in.u = up + 3 * (size_t)n; CU(cudaMemcpyAsync(up + 3 * (size_t)n, unpbc3, v3b, cudaMemcpyHostToDevice, st)); }
+    in.v = up + 6 * (size_t)n;
+    CU(cudaMemcpyAsync(up + 6 * (size_t)n, v3, v3b, cudaMemcpyHostToDevice, st));
+    if (f3) { in.f = up + 9 * (size_t)n; CU(cudaMemcpyAsync(up + 9 * (size_t)n, f3, v3b, cudaMemcpyHostToDevice, st)); }
+    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)n);
+    CU(cudaMemcpyAsync(up + 12 * (size_t)n, id, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    in.type = upi;
+    CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    if (box) { in.box = upi + n; CU(cudaMemcpyAsync(upi + n, box, sizeof(int) * n, cudaMemcpyHostToDevice, st)); }
+    if (movable) { in.movable = upm; CU(cudaMemcpyAsync(upm, movable, (size_t)n, cudaMemcpyHostToDevice, st)); }
+    return upload_staged(e, n, box, id, type, in);
+}
+
+// Validation, binning and placement of a staged bead set (in: device arrays
+// in the staging buffers; id and type: the same beads on the host, or null
+// for an upload from device memory).
+static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int64_t* id, const int32_t* type,
+                         const UploadIn& in)
+{
+    cudaStream_t st = e->s();
+    int rc;
+    // validation and binning (CSimBox::AssignBeadstoCells, SimBox.cpp:715-762:
+    // ix = (long)(x/w), box-local coordinates); nothing of the state changes yet
+    // herr: the first bead of each error kind, any residual unPBC offset,
+    // the bits of ids / types that differ from the previous upload, and the
+    // beads per type
+    int herr[kUpErrors + 2 + kMaxTypes];
+    for (int k = 0; k < kUpErrors; ++k) herr[k] = INT_MAX;
+    for (int k = kUpErrors; k < kUpErrors + 2 + kMaxTypes; ++k) herr[k] = 0;
+    CU(cudaMemcpyAsync(e->d_up_err, herr, sizeof herr, cudaMemcpyHostToDevice, st));
+    const UploadPrev prev{e->d_prev_id, e->d_prev_type, reinterpret_cast<unsigned*>(e->d_up_err + kUpErrors + 1),
+                          e->d_up_err + kUpErrors + 2};
+    const bool prev_ok = e->prev_n == n;   // d_prev_* hold the last complete upload of n beads
+    k_up_check<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, (int)e->hboxes.size(), e->ntypes, e->d_boxes, in,
+                                                            e->d_up_cell, e->d_up_img, e->d_up_off, e->d_count,
+                                                            e->d_block_count, e->d_up_err, e->d_up_err + kUpErrors,
+                                                            prev);
+    if ((rc = check_launch(e, "k_up_check"))) return rc;
+    CU(cudaMemcpyAsync(herr, e->d_up_err, sizeof herr, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    e->prev_n = -1;   // d_prev_* now hold this upload, complete only once it succeeds
+    int bad = INT_MAX, kind = -1;
+    for (int k = 0; k < kUpErrors; ++k)
+        if (herr[k] < bad) { bad = herr[k]; kind = k; }
+    if (kind >= 0) {
+        CU(cudaMemset(e->d_count, 0, sizeof(int) * (size_t)e->ncell));
+        CU(cudaMemset(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk));
+        switch (kind) {
+            case kUpType: return fail(e, DPD_E_ARG, "bead type out of range");
+            case kUpId: return fail(e, DPD_E_ARG, "bead id outside 1..2^31-1");
+            case kUpBox: return fail(e, DPD_E_ARG, "bead box index out of range");
+            case kUpNonFinite: return fail(e, DPD_E_BOX, "non-finite bead state");
+            case kUpOutside: {
+                char msg[160];
+                if (id)
+                    snprintf(msg, sizeof msg, "bead %lld (id %lld) lies outside the box", (long long)bad,
+                             (long long)id[bad]);
+                else
+                    snprintf(msg, sizeof msg, "bead %lld lies outside the box", (long long)bad);
+                return fail(e, DPD_E_BOX, msg);
+            }
+            default: return fail(e, DPD_E_ARG, "unPBC more than 511 box lengths from x");
+        }
+    }
+    const bool any_off = herr[kUpErrors] != 0;
+    const bool same_n = e->n == n;
+    if ((rc = ensure_beads(e, n))) return rc;
     e->n = n;
     // cell starts, then the slot order: by cell, inside a cell by upload index
     k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start,
@@ -1272,17 +1255,11 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     }
     e->off_active = any_off;
     CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)n, st));
-    // a trusted upload's failing beads are reported through the status word
-    if (!trusted) CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
+    CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
     // host copies of ids and types, refreshed only when the device saw them
-    // change; beads per type counted by k_up_check (read later when trusted)
-    const unsigned changed = (prev_ok && !trusted) ? (unsigned)herr[kUpErrors + 1] : 3u;
-    if (trusted) {
-        e->type_count_stale = true;
-    } else {
-        e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
-        e->type_count_stale = false;
-    }
+    // change; beads per type counted by k_up_check
+    const unsigned changed = prev_ok ? (unsigned)herr[kUpErrors + 1] : 3u;
+    e->type_count.assign(herr + kUpErrors + 2, herr + kUpErrors + 2 + e->ntypes);
     if (!id || !type) {
         // an upload from device memory: the host copies are fetched when needed
         if (changed & 3u) {
@@ -1297,9 +1274,8 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
         if (e->host_ids_stale || (changed & 2u) || e->h_type.size() != (size_t)n) e->h_type.assign(type, type + n);
         e->host_ids_stale = false;
     }
-    // (trusted: the caller waited for every kernel before the upload was queued)
-    if (!trusted) CU(cudaStreamSynchronize(st));
-    *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine that publishes the status is in flight
+    CU(cudaStreamSynchronize(st));
+    *(volatile unsigned*)e->h_seen = 0u;   // no kernel of the engine is in flight after the sync
     rc = empty_topology(e, same_n);
     if (rc) return rc;
     e->uploaded = true;
@@ -1743,6 +1719,7 @@ int dpd_engine_set_monitor(dpd_engine* e, int32_t nbondtypes, const int32_t* bon
 {
     if (!e) return DPD_E_ARG;
     if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads (and the topology) before the monitor");
+    if (e->slab) return fail(e, DPD_E_STATE, "the monitor covers a whole box; a slab also holds ghosts");
     if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "the monitor needs a single-box engine");
     if (nbondtypes < 0 || nbptypes < 0 || npolytypes < 0 || npoly < 0 || nbondtypes > 65536 || nbptypes > 65536 ||
         npolytypes > 65536 || (e->topo_nb && !bond_type) || (e->topo_na && !bondpair_type) ||
@@ -1833,7 +1810,6 @@ int dpd_engine_monitor(dpd_engine* e, dpd_monitor* out, double* msd, double* bon
     if (!out) return fail(e, DPD_E_ARG, "null output");
     if (!e->mon_set) return fail(e, DPD_E_STATE, "dpd_engine_set_monitor has not been called for these beads");
     CU(cudaSetDevice(e->device));
-    if (int rc0 = host_type_count(e)) return rc0;
     const int n = (int)e->n, T = e->ntypes;
     const size_t nsums = 6 + (size_t)T + e->mon_nbt + 2 + e->mon_npt + 5 * (size_t)e->mon_nbpt;
     CU(cudaMemsetAsync(e->d_mon_sums, 0, nsums * sizeof(double), e->s()));
@@ -2709,28 +2685,50 @@ int dpd_engine_slab_unpack(dpd_engine* e, const double* recv_below, const double
     }
     const int64_t nn = hs[1];
     if (nn < 1) return fail(e, DPD_E_STATE, "the slab would hold no beads");
+    // The next local box goes straight into the step's input arrays in upload
+    // order; the next step's drift, cell scan and gather bin it (no upload
+    // kernels, no further host wait).  The drift of a slab's steps is never
+    // done ahead, so the arrival counts are zero here.
     if ((rc = drop_ahead(e))) return rc;
-    if ((rc = stage_buffers(e, nn))) return rc;
-    double* up = e->d_up;
-    k_slab_place<<<blocks_for(nn, kThreads), kThreads, 0, st>>>((int)nn, S.geom, S.d_sizes + 5, S.d_keep,
-                                                                recv_below, recv_above, S.d_mine, up);
-    if ((rc = check_launch(e, "k_slab_place"))) return rc;
-    UploadIn in{};
-    in.x = up;
-    in.u = up + 3 * (size_t)nn;
-    in.v = up + 6 * (size_t)nn;
-    in.f = up + 9 * (size_t)nn;
-    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)nn);
-    const int* upi = reinterpret_cast<const int*>(up + 13 * (size_t)nn);
-    in.type = upi;
-    in.movable = reinterpret_cast<const unsigned char*>(upi + 2 * (size_t)nn);
+    const bool same_n = e->n == nn;
+    if ((rc = ensure_beads(e, nn))) return rc;
+    bool moved = false;
+    if ((rc = ensure(e, &e->d_off, e->cap_off, 3 * (size_t)e->cap_n, &moved))) return rc;
+    if ((rc = ensure(e, &e->d_prev_id, e->cap_prev_id, (size_t)nn, &moved, with_room(e, (size_t)nn)))) return rc;
+    if ((rc = ensure(e, &e->d_prev_type, e->cap_prev_type, (size_t)nn, &moved, with_room(e, (size_t)nn)))) return rc;
     // the status word starts the next step with the step's non-fatal bits (cell skips)
     CU(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), st));
     if (status) {
         k_slab_status<<<1, 1, 0, st>>>(e->d_status, status);
         if ((rc = check_launch(e, "k_slab_status"))) return rc;
     }
-    if ((rc = upload_staged(e, nn, nullptr, nullptr, nullptr, in, true))) return rc;
+    const int c = e->cur;
+    if (e->precision == DPD_PRECISION_FP64)
+        k_slab_place_state<double><<<blocks_for(nn, kThreads), kThreads, 0, st>>>(
+            (int)nn, e->ntypes, S.geom, e->d_boxes, S.d_sizes + 5, S.d_keep, recv_below, recv_above, S.d_mine,
+            e->d_x[c], e->d_v[c], (double*)e->d_F, e->d_bid[c], e->d_tf[c], e->d_cell[c], e->d_img[c], e->d_pid[c],
+            e->d_pid_of, e->d_off, e->d_prev_id, e->d_prev_type, e->d_status);
+    else
+        k_slab_place_state<float><<<blocks_for(nn, kThreads), kThreads, 0, st>>>(
+            (int)nn, e->ntypes, S.geom, e->d_boxes, S.d_sizes + 5, S.d_keep, recv_below, recv_above, S.d_mine,
+            e->d_x[c], e->d_v[c], (float*)e->d_F, e->d_bid[c], e->d_tf[c], e->d_cell[c], e->d_img[c], e->d_pid[c],
+            e->d_pid_of, e->d_off, e->d_prev_id, e->d_prev_type, e->d_status);
+    if ((rc = check_launch(e, "k_slab_place_state"))) return rc;
+    CU(cudaMemsetAsync(e->d_stress, 0, 9 * real_size(e) * (size_t)nn, st));
+    e->n = nn;
+    e->off_active = true;
+    e->host_ids_stale = true;   // bead_ids() reads d_prev_id
+    ++e->ids_version;
+    e->prev_n = nn;
+    *(volatile unsigned*)e->h_seen = 0u;   // every kernel before the exchange has finished (the size read)
+    if ((rc = empty_topology(e, same_n))) return rc;
+    e->uploaded = true;
+    e->rs_order.clear();
+    e->mon_set = false;
+    e->stepped = false;
+    e->sampled = false;
+    e->obs_valid = false;
+    e->box_obs_valid = false;
     S.geom.n_owned = hs[0];
     if (S.topo && (rc = slab_topology(e, true))) return rc;
     if (n_owned) *n_owned = hs[0];

@@ -20,8 +20,8 @@
 // Kernels here: classification and ordered compaction of the records to
 // send (k_slab_count / k_slab_offsets / k_slab_write, slot order, so the
 // result does not depend on thread timing), the sizes of the next local box
-// (k_slab_sizes), its placement into the engine's upload staging
-// (k_slab_place), and the device topology filter that keeps the bonds and
+// (k_slab_sizes), its placement into the step's input arrays
+// (k_slab_place_state), and the device topology filter that keeps the bonds and
 // bond pairs whose beads are all in the local box (k_slab_idmap,
 // k_slab_endpoints, k_slab_term_count, k_slab_term_write, with the scan
 // kernels k_scan_*).
@@ -258,18 +258,27 @@ __global__ void k_slab_sizes(const double* __restrict__ recv_below, const double
     out[11] = total[kToBelowMig] + total[kToBelowGhost] > cap || total[kToAboveMig] + total[kToAboveGhost] > cap;
 }
 
-// Bead o of the next local box from its record, into the upload staging
-// layout (x, unPBC, v, F interleaved by bead; ids; types; movable flags).
-// Order: kept owned beads, migrants from below, from above (the owned
-// beads), ghosts from below, from above, this rank's own migrants.
-// Received records come in the global frame: z - c, wrapped into [0, Lz)
-// (a ghost from across the global z face takes the periodic shift), unPBC
-// z - c.
-__global__ void __launch_bounds__(256) k_slab_place(int n, SlabGeom G, const int* __restrict__ seg,
-                                                    const double* __restrict__ keep,
-                                                    const double* __restrict__ recv_below,
-                                                    const double* __restrict__ recv_above,
-                                                    const double* __restrict__ mine, double* __restrict__ up)
+// The next local box written straight into the step's input arrays in
+// upload order (slot o = upload index o; the next step's drift, cell scan
+// and gather bin them, as after any step): the record's x, v and F, its
+// type and movability, its CNT cell by the upload's rule ix = (long)(x/w),
+// its periodic images (unPBC - x in whole box lengths) and the residual in
+// off, its id (noise id, pid_of, and the previous-upload copy the host reads
+// ids from).  Order of the beads: the kept owned beads, migrants from below,
+// from above (the owned beads), ghosts from below, from above, this rank's
+// own migrants; received records come in the global frame: z - c, wrapped
+// into [0, Lz) (a ghost from across the global z face takes the periodic
+// shift), unPBC z - c.  The records are the engine's own: a bead outside the
+// box, of an unknown type or with an image count beyond +-511 is filed in
+// range and sets DPD_STATUS_INTERNAL.
+template <typename real>
+__global__ void __launch_bounds__(256) k_slab_place_state(
+    int n, int ntypes, SlabGeom G, const Box* __restrict__ boxes, const int* __restrict__ seg,
+    const double* __restrict__ keep, const double* __restrict__ recv_below, const double* __restrict__ recv_above,
+    const double* __restrict__ mine, double* __restrict__ x, double* __restrict__ v, real* __restrict__ F,
+    int* __restrict__ bid, int* __restrict__ tf, int* __restrict__ cell, uint32_t* __restrict__ img,
+    int* __restrict__ pid, int* __restrict__ pid_of, double* __restrict__ off, int64_t* __restrict__ prev_id,
+    int* __restrict__ prev_type, unsigned* __restrict__ status)
 {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
@@ -298,18 +307,40 @@ __global__ void __launch_bounds__(256) k_slab_place(int n, SlabGeom G, const int
         r[kRecX + 2] = z;
         r[kRecU + 2] -= G.c;
     }
+    const Box& B = boxes[0];
+    bool bad = false;
+    int ci[3], ii[3];
     const size_t N = (size_t)n;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        up[3 * (size_t)o + d] = r[kRecX + d];
-        up[3 * N + 3 * (size_t)o + d] = r[kRecU + d];
-        up[6 * N + 3 * (size_t)o + d] = r[kRecV + d];
-        up[9 * N + 3 * (size_t)o + d] = r[kRecF + d];
+        const double xv = r[kRecX + d];
+        long long c = (long long)(xv / B.w[d]);
+        if (!(xv >= 0.0) || c < 0 || c >= B.nc[d]) {
+            bad = true;
+            c = c < 0 ? 0 : (c >= B.nc[d] ? B.nc[d] - 1 : c);
+        }
+        ci[d] = (int)c;
+        const double du = r[kRecU + d] - xv;
+        double kk = nearbyint(du / B.L[d]);
+        if (!(fabs(kk) <= 511.0)) { bad = true; kk = 0.0; }
+        ii[d] = (int)kk;
+        off[(size_t)d * N + o] = du - kk * B.L[d];
+        x[(size_t)d * N + o] = xv;
+        v[(size_t)d * N + o] = r[kRecV + d];
+        F[(size_t)d * N + o] = (real)r[kRecF + d];
     }
-    reinterpret_cast<int64_t*>(up + 12 * N)[o] = (int64_t)r[kRecId];
-    int* upi = reinterpret_cast<int*>(up + 13 * N);
-    upi[o] = (int)r[kRecType];
-    reinterpret_cast<unsigned char*>(upi + 2 * N)[o] = r[kRecMovable] != 0.0 ? 1 : 0;
+    int t = (int)r[kRecType];
+    if (t < 0 || t >= ntypes) { bad = true; t = 0; }
+    const int id = (int)r[kRecId];
+    bid[o] = o;
+    tf[o] = t | (r[kRecMovable] != 0.0 ? 0 : kFlagFrozen);
+    cell[o] = B.cell_base + ci[0] + B.nc[0] * (ci[1] + B.nc[1] * ci[2]);
+    img[o] = img_pack(ii[0], ii[1], ii[2]);
+    pid[o] = id;
+    pid_of[o] = id;
+    prev_id[o] = id;
+    prev_type[o] = t;
+    if (bad) atomicOr(status, 0x8u);
 }
 
 __global__ void k_slab_status(unsigned* __restrict__ status, unsigned bits) { *status |= bits; }

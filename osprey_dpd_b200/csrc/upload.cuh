@@ -41,15 +41,11 @@ struct UploadPrev {
 // Validation and binning of an uploaded bead set: cell[b] receives the bead's
 // CNT cell and the cells are counted; the first bead of each error kind is
 // recorded in err; every valid bead's type is counted (block histogram).
-// With trusted (records the engine formed itself, placed without the host
-// reading err) a failing bead is filed in the first cell instead, so every
-// later kernel stays in bounds, and DPD_STATUS_INTERNAL is set in *trusted.
 __global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes, const Box* __restrict__ boxes,
                                                   UploadIn in, int* __restrict__ cell, uint32_t* __restrict__ img,
                                                   double* __restrict__ off, int* __restrict__ count,
                                                   int* __restrict__ block_count, int* __restrict__ err,
-                                                  int* __restrict__ any_off, UploadPrev prev,
-                                                  unsigned* __restrict__ trusted)
+                                                  int* __restrict__ any_off, UploadPrev prev)
 {
     __shared__ int hist[kMaxTypes];
     for (int k = threadIdx.x; k < ntypes; k += blockDim.x) hist[k] = 0;
@@ -102,14 +98,6 @@ __global__ void __launch_bounds__(256) k_up_check(int n, int nboxes, int ntypes,
             if (residual) *any_off = 1;
             atomicAdd(&hist[t], 1);
         } while (false);
-        if (trusted && c < 0) {
-            c = boxes[0].cell_base;
-            cell[b] = c;
-            img[b] = img_pack(0, 0, 0);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) off[(size_t)d * n + b] = 0.0;
-            atomicOr(trusted, 0x8u);
-        }
     }
     // cell and chunk counts, one atomic per distinct cell (chunk) and warp:
     // beads uploaded in cell order (a slab's exchange) share them
