@@ -221,6 +221,10 @@ DPD_API int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t p
 #define DPD_PAIR_STAGED     2
 DPD_API int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme);
 
+/* Beads per block (tile) of the half-shell pair kernel: 64 (default, 0) or
+ * 128, the same warps per SM either way; an autotuned axis. */
+DPD_API int dpd_engine_set_pair_tile(dpd_engine* e, int32_t beads_per_block);
+
 /* Waits for queued work; returns the device status bits seen so far. */
 DPD_API int dpd_engine_status(dpd_engine* e, uint32_t* status_bits);
 

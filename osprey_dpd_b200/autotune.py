@@ -2,7 +2,8 @@
 
 The shape of the force kernel (hit-list capacity per bead, persistent grid
 or one tile per block, shared-memory carveout, and where the caller allows
-run-to-run variation in the last bits, the half-shell pair scheme) is chosen by timing candidate
+run-to-run variation in the last bits, the half-shell pair scheme with its
+tile of 64 or 128 beads per block) is chosen by timing candidate
 shapes on the live workload: for each candidate the engine advances a scratch
 copy of the system by a few captured multi-step calls and the fastest shape
 wins.  Results are cached in a JSON file keyed by the GPU name and a
@@ -16,15 +17,17 @@ import os
 import time
 from typing import Callable, Dict, Iterable, Optional, Tuple
 
-Shape = Tuple[int, ...]     # (hitcap, persistent blocks per SM, carveout[, pair scheme])
+Shape = Tuple[int, ...]     # (hitcap, persistent blocks per SM, carveout[, pair scheme[, half-shell tile]])
 
 # full-shell shapes: bitwise reproducible forces
 DEFAULT_CANDIDATES: Tuple[Shape, ...] = (
     (32, 0, -1), (40, 0, -1), (24, 0, -1), (48, 0, -1), (32, 0, 100), (32, 4, -1), (32, 8, -1),
 )
-# half-shell shapes (pair scheme 1): each pair once, atomics, last bits vary
+# half-shell shapes (pair scheme 1): each pair once, atomics, last bits vary;
+# tiles of 64 (two warps) and 128 beads (four warps) per block
 HALF_SHELL_CANDIDATES: Tuple[Shape, ...] = (
-    (32, 0, -1, 1), (24, 0, -1, 1), (32, 0, 100, 1), (24, 0, 100, 1), (40, 0, 100, 1),
+    (32, 0, -1, 1, 64), (24, 0, -1, 1, 64), (32, 0, 100, 1, 64), (24, 0, 100, 1, 64), (40, 0, 100, 1, 64),
+    (32, 0, -1, 1, 128), (24, 0, 100, 1, 128),
 )
 # staged half-shell shape (pair scheme 2): smaller hit lists leave room for the staged rows
 STAGED_CANDIDATES: Tuple[Shape, ...] = ((16, 0, 100, 2),)
@@ -39,10 +42,13 @@ def signature(gpu: str, n: int, ncells: int, ntypes: int, precision: int, nboxes
 
 
 def apply_shape(eng, shape: Shape) -> None:
-    """Sets a tuned shape on an engine (the scheme only when the shape names one)."""
+    """Sets a tuned shape on an engine (the scheme and the half-shell tile only
+    when the shape names them)."""
     eng.set_launch_shape(*shape[:3])
     if len(shape) > 3:
         eng.set_pair_scheme(shape[3])
+    if len(shape) > 4:
+        eng.set_pair_tile(shape[4])
 
 
 def _load(path: str) -> Dict[str, dict]:

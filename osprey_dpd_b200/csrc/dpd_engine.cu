@@ -262,6 +262,7 @@ struct dpd_engine {
     int pair_bps = 0;          // resident blocks per SM for the persistent grid
     int pair_carveout = -1;    // preferred shared-memory carveout in percent, -1 = driver default
     int pair_scheme = DPD_PAIR_FULL_SHELL;   // DPD_PAIR_*: full shell (reproducible), half shell, staged half shell
+    int pair_tile = kHalfBlock;              // beads per block of the half-shell kernel (64 or 128)
     bool pair_attr_set[2][2] = {{false, false}, {false, false}};   // [fp64][sample]; one box kind per engine
 };
 
@@ -471,11 +472,16 @@ struct Timed {
 
 // The pair kernel variant for (box table, sample step, pair scheme).
 template <typename real>
-auto pair_kernel(bool multi, bool sample, int scheme)
+auto pair_kernel(bool multi, bool sample, int scheme, int tile)
 {
     if (scheme == DPD_PAIR_STAGED)
         return multi ? (sample ? k_pair_forces_staged<real, true, true> : k_pair_forces_staged<real, false, true>)
                      : (sample ? k_pair_forces_staged<real, true, false> : k_pair_forces_staged<real, false, false>);
+    if (scheme == DPD_PAIR_HALF_SHELL && tile == kPairBlock)
+        return multi ? (sample ? k_pair_forces_half<real, true, true, kPairBlock>
+                               : k_pair_forces_half<real, false, true, kPairBlock>)
+                     : (sample ? k_pair_forces_half<real, true, false, kPairBlock>
+                               : k_pair_forces_half<real, false, false, kPairBlock>);
     if (scheme == DPD_PAIR_HALF_SHELL)
         return multi ? (sample ? k_pair_forces_half<real, true, true> : k_pair_forces_half<real, false, true>)
                      : (sample ? k_pair_forces_half<real, true, false> : k_pair_forces_half<real, false, false>);
@@ -489,7 +495,8 @@ size_t pair_dyn_bytes(const dpd_engine* e, bool multi)
 {
     if (e->pair_scheme == DPD_PAIR_STAGED) return StgLayout<real>(e->ntypes, e->pair_hitcap, multi).total;
     if (e->pair_scheme == DPD_PAIR_HALF_SHELL)
-        return half_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
+        return e->pair_tile == kPairBlock ? half_smem_bytes<real, kPairBlock>(e->ntypes, e->pair_hitcap, multi)
+                                          : half_smem_bytes<real, kHalfBlock>(e->ntypes, e->pair_hitcap, multi);
     return pair_smem_bytes<real>(e->ntypes, e->pair_hitcap, multi);
 }
 
@@ -502,7 +509,7 @@ int set_pair_attributes(dpd_engine* e)
     const int pv = sizeof(real) == 8 ? 1 : 0;
     for (int sv = 0; sv < 2; ++sv) {
         if (e->pair_attr_set[pv][sv]) continue;
-        auto kern = pair_kernel<real>(multi, sv != 0, e->pair_scheme);
+        auto kern = pair_kernel<real>(multi, sv != 0, e->pair_scheme, e->pair_tile);
         const size_t dyn = pair_dyn_bytes<real>(e, multi);
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         if (e->pair_carveout >= 0)
@@ -652,7 +659,7 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
     }
     {
         const bool multi = e->hboxes.size() > 1;
-        auto kern = pair_kernel<real>(multi, sample, e->pair_scheme);
+        auto kern = pair_kernel<real>(multi, sample, e->pair_scheme, e->pair_tile);
         const size_t dyn = pair_dyn_bytes<real>(e, multi);
         if ((rc = set_pair_attributes<real>(e))) return rc;
         // the half shell accumulates into F with atomics
@@ -661,7 +668,7 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
             CU(cudaMemsetAsync(e->d_stress, 0, (size_t)9 * n * sizeof(real), st));
         // one tile per block by default; bps > 0 selects a persistent grid of
         // sms * bps blocks walking contiguous tiles
-        const int block = e->pair_scheme == DPD_PAIR_HALF_SHELL ? kHalfBlock : kPairBlock;
+        const int block = e->pair_scheme == DPD_PAIR_HALF_SHELL ? e->pair_tile : kPairBlock;
         const int tiles = blocks_for(n, block);
         const int tpb = e->pair_bps > 0 ? std::max(1, blocks_for(tiles, (int64_t)e->sms * e->pair_bps)) : 1;
         Timed t(e, DPD_KERNEL_PAIR_FORCES);
@@ -753,6 +760,7 @@ void parse_tuning(dpd_engine* e, const char* spec)
             else if (key == "carveout") e->pair_carveout = std::min(std::max(val, -1), 100);
             else if (key == "half") e->pair_scheme = val ? DPD_PAIR_HALF_SHELL : DPD_PAIR_FULL_SHELL;
             else if (key == "scheme" && val >= DPD_PAIR_FULL_SHELL && val <= DPD_PAIR_STAGED) e->pair_scheme = val;
+            else if (key == "tile" && (val == kHalfBlock || val == kPairBlock)) e->pair_tile = val;
             else if (key == "ahead") e->ahead_enabled = val != 0;
             else if (key == "pdl") e->pdl = val != 0;
         }
@@ -986,6 +994,20 @@ int dpd_engine_set_launch_shape(dpd_engine* e, int32_t hitcap, int32_t persisten
     e->pair_hitcap = hitcap;
     e->pair_bps = persistent_blocks_per_sm;
     e->pair_carveout = smem_carveout;
+    memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
+    drop_graphs(e);
+    return DPD_OK;
+}
+
+int dpd_engine_set_pair_tile(dpd_engine* e, int32_t beads_per_block)
+{
+    if (!e) return DPD_E_ARG;
+    if (beads_per_block == 0) beads_per_block = kHalfBlock;
+    if (beads_per_block != kHalfBlock && beads_per_block != kPairBlock)
+        return fail(e, DPD_E_ARG, "half-shell tiles hold 64 or 128 beads");
+    CU(cudaSetDevice(e->device));
+    CU(cudaStreamSynchronize(e->s()));
+    e->pair_tile = beads_per_block;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
     return DPD_OK;

@@ -26,18 +26,20 @@ namespace dpd {
 
 constexpr int kPairWarps = 4;
 constexpr int kPairBlock = 32 * kPairWarps;   // full-shell and staged tiles
-// Half-shell tiles: two warps.  Measured on the B200 against four and eight
-// warps (same registers per SM): the mixed-precision kernel 2-3 % faster
-// (bilayer 77.1 vs 79.2 us, melt 886 vs 901 us), FP64 even; one warp slower.
+// Half-shell tiles: two warps by default (dpd_engine_set_pair_tile selects
+// 64 or 128 beads per block at run time).  Measured on the B200 against four
+// and eight warps (same registers per SM): the mixed-precision kernel 2-3 %
+// faster (bilayer 77.1 vs 79.2 us, melt 886 vs 901 us), FP64 even; one warp
+// slower.
 constexpr int kHalfBlock = 64;
 // Resident blocks per SM the pair kernels are compiled for: 8 (64 registers,
 // 32 warps) in FP32; the FP64 variants keep 6 to limit spills.
 template <typename real, bool MULTI = false> struct PairOcc {
     static constexpr int value = sizeof(real) == 8 ? 6 : 8;
 };
-// The same warps per SM for the half-shell kernel's smaller blocks.
-template <typename real, bool MULTI = false> struct HalfOcc {
-    static constexpr int value = PairOcc<real, MULTI>::value * kPairBlock / kHalfBlock;
+// The same warps per SM for the half-shell kernel's tiles of BLOCK beads.
+template <typename real, bool MULTI = false, int BLOCK = kHalfBlock> struct HalfOcc {
+    static constexpr int value = PairOcc<real, MULTI>::value * kPairBlock / BLOCK;
 };
 constexpr int kHitCapMax = 64;           // upper bound of the run-time hit-list capacity
 // Cell pruning threshold on the squared distance to a cell's nearest point:
@@ -740,26 +742,26 @@ __device__ __forceinline__ void half_shell_tile_lanes(
 // Dynamic shared memory of k_pair_forces_half: pair tables (single box), hit
 // lists (hitcap rows plus the spare row of the branch-free test loop), then
 // the balanced pass's per-thread scratch.
-template <typename real>
+template <typename real, int BLOCK>
 __host__ __device__ constexpr size_t half_scratch_bytes()
 {
-    return (2 * 4 * sizeof(real) + 2 * sizeof(int)) * (size_t)kHalfBlock;
+    return (2 * 4 * sizeof(real) + 2 * sizeof(int)) * (size_t)BLOCK;
 }
-template <typename real>
+template <typename real, int BLOCK>
 __host__ __device__ constexpr size_t half_smem_bytes(int nt, int hitcap, bool multi)
 {
-    return pair_smem_bytes<real, kHalfBlock>(nt, hitcap + 1, multi) + half_scratch_bytes<real>();
+    return pair_smem_bytes<real, BLOCK>(nt, hitcap + 1, multi) + half_scratch_bytes<real, BLOCK>();
 }
-template <typename real>
+template <typename real, int BLOCK>
 __device__ __forceinline__ HalfShared<real> half_shared(unsigned char* base)
 {
     typedef typename Vec4<real>::type V4;
     HalfShared<real> sh;
     sh.hpos = reinterpret_cast<V4*>(base);
-    sh.hvel = sh.hpos + kHalfBlock;
+    sh.hvel = sh.hpos + BLOCK;
     sh.hxw = nullptr;
-    sh.wcnt = reinterpret_cast<int*>(sh.hvel + kHalfBlock);
-    sh.wexc = sh.wcnt + kHalfBlock;
+    sh.wcnt = reinterpret_cast<int*>(sh.hvel + BLOCK);
+    sh.wexc = sh.wcnt + BLOCK;
     return sh;
 }
 
@@ -925,8 +927,8 @@ template <typename real, bool MULTI>
 constexpr bool kHalfBalanced = sizeof(real) == 4 && !MULTI;
 
 // F must be zero on entry, and on sample steps (VIRIAL) the stress array too.
-template <typename real, bool VIRIAL, bool MULTI>
-__global__ void __launch_bounds__(kHalfBlock, HalfOcc<real, MULTI>::value) k_pair_forces_half(
+template <typename real, bool VIRIAL, bool MULTI, int BLOCK = kHalfBlock>
+__global__ void __launch_bounds__(BLOCK, HalfOcc<real, MULTI, BLOCK>::value) k_pair_forces_half(
     int n, const StepConst* __restrict__ K, const Box* __restrict__ boxes, const int64_t* __restrict__ step_ptr,
     const real* __restrict__ tab, const int* __restrict__ cell, const int* __restrict__ start,
     const typename Vec4<real>::type* __restrict__ pos4, const typename Vec4<real>::type* __restrict__ vel4,
@@ -940,9 +942,9 @@ __global__ void __launch_bounds__(kHalfBlock, HalfOcc<real, MULTI>::value) k_pai
     real* Tsh = reinterpret_cast<real*>(pair_dyn);
     unsigned char* lbase = pair_dyn + (MULTI ? 0 : pair_tables_bytes<real>(nt));
     uint32_t* lists = reinterpret_cast<uint32_t*>(lbase);
-    const HalfShared<real> sh = half_shared<real>(lbase + sizeof(uint32_t) * (size_t)(hitcap + 1) * kHalfBlock);
+    const HalfShared<real> sh = half_shared<real, BLOCK>(lbase + sizeof(uint32_t) * (size_t)(hitcap + 1) * BLOCK);
     if (!MULTI)
-        for (int k = threadIdx.x; k < 3 * nt * nt; k += kHalfBlock) Tsh[k] = tab[k];
+        for (int k = threadIdx.x; k < 3 * nt * nt; k += BLOCK) Tsh[k] = tab[k];
     const int64_t step = *step_ptr;
     uint32_t keys0[10];
     {
@@ -953,12 +955,12 @@ __global__ void __launch_bounds__(kHalfBlock, HalfOcc<real, MULTI>::value) k_pai
     __syncthreads();   // tables
     const int tile0 = blockIdx.x * tiles_per_block;
     for (int tile = tile0; tile < tile0 + tiles_per_block; ++tile) {
-        if (tile * kHalfBlock >= n) break;
+        if (tile * BLOCK >= n) break;
         if (kHalfBalanced<real, MULTI>)
-            half_shell_tile<real, VIRIAL, MULTI, kHalfBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
+            half_shell_tile<real, VIRIAL, MULTI, BLOCK>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4, F,
                                                  stress, hitcap, lists, sh, keys0, xs);
         else
-            half_shell_tile_lanes<real, VIRIAL, MULTI, kHalfBlock>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
+            half_shell_tile_lanes<real, VIRIAL, MULTI, BLOCK>(tile, n, nt, boxes, step, tab, Tsh, cell, start, pos4, vel4,
                                                        F, stress, hitcap, lists, xs);
     }
 }

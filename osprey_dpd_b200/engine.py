@@ -45,7 +45,7 @@ EXPORTED = [
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
     "dpd_write_paraview", "dpd_engine_write_paraview", "dpd_engine_renormalise_mom",
     "dpd_engine_slab_setup", "dpd_engine_slab_pack", "dpd_engine_slab_unpack", "dpd_engine_slab_counts",
-    "dpd_engine_bead_ids", "dpd_engine_slab_observables",
+    "dpd_engine_bead_ids", "dpd_engine_slab_observables", "dpd_engine_set_pair_tile",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -123,6 +123,7 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_set_sample_period.argtypes = [vp, C.c_int64]
     L.dpd_engine_set_launch_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
     L.dpd_engine_set_pair_scheme.argtypes = [vp, C.c_int32]
+    L.dpd_engine_set_pair_tile.argtypes = [vp, C.c_int32]
     L.dpd_engine_set_slice_stress.argtypes = [vp, C.c_int32, C.c_int32, vp, C.c_int32, vp]
     L.dpd_engine_set_monitor.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, C.c_int64, vp, vp, vp, C.c_int32, vp]
     L.dpd_engine_monitor.argtypes = [vp, C.POINTER(DpdMonitor), vp, vp, vp, vp]
@@ -437,6 +438,10 @@ class DpdEngine:
         """PAIR_FULL_SHELL (reproducible), PAIR_HALF_SHELL (each pair once) or
         PAIR_STAGED (each pair once, neighbour rows staged in shared memory)."""
         self._check(load().dpd_engine_set_pair_scheme(self.h, int(scheme)), "set_pair_scheme")
+
+    def set_pair_tile(self, beads_per_block: int) -> None:
+        """Beads per block of the half-shell kernel: 64 (default) or 128."""
+        self._check(load().dpd_engine_set_pair_tile(self.h, int(beads_per_block)), "set_pair_tile")
 
     def set_sample_period(self, period: int) -> None:
         self._check(load().dpd_engine_set_sample_period(self.h, int(period)), "set_sample_period")

@@ -92,8 +92,9 @@ def _dense_cluster_system():
                        np.concatenate([s.v, np.zeros((extra, 3))]))
 
 
-@pytest.mark.parametrize("tune", ["half=1", "half=1,hitcap=8", "half=1,hitcap=64,bps=1", "scheme=2",
-                                  "scheme=2,hitcap=8", "scheme=2,hitcap=64,bps=1"])
+@pytest.mark.parametrize("tune", ["half=1", "half=1,hitcap=8", "half=1,hitcap=64,bps=1", "half=1,tile=128",
+                                  "half=1,tile=128,hitcap=8", "scheme=2", "scheme=2,hitcap=8",
+                                  "scheme=2,hitcap=64,bps=1"])
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
 def test_half_shell_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precision, tune, monkeypatch):
     """Selected through DPD_TUNE, with a 60-bead cell and extreme hit-list sizes."""
@@ -108,14 +109,15 @@ def test_half_shell_dense_cell_and_launch_shapes(engine_mod, oracle_mod, precisi
     assert eng.status() == 0
 
 
-@SCHEMES
+@pytest.mark.parametrize("scheme,tile", [(1, 64), (1, 128), (2, 0)], ids=["half", "half_tile128", "staged"])
 @pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
-def test_half_shell_replica_batch(engine_mod, oracle_mod, precision, scheme):
+def test_half_shell_replica_batch(engine_mod, oracle_mod, precision, scheme, tile):
     edges, fracs, a_ab, seeds = W.replica_table(4, lo=4, hi=7)
     systems = [W.binary_mixture(n=int(edges[r]), seed=int(seeds[r]), a_ab=float(a_ab[r]), frac_a=float(fracs[r]))
                for r in range(4)]
     batch = engine_mod.DpdBatch(systems, precision=precision)
     batch.set_pair_scheme(scheme)
+    batch.set_pair_tile(tile)
     batch.step(1, 3)
     f = batch.split(batch.download()["f"])
     tol = 1e-4 if precision == 0 else 1e-10
