@@ -844,3 +844,248 @@ int dpdo_random_state(int64_t n, const double L[3], double kT, uint64_t seed, in
     for (int64_t i = 0; i < 3 * n; ++i) v3[i] = sqrt(kT) * v3[i] / vtotal;
     return 0;
 }
+
+/* ---------------------------------------------------------------- lamella initial state
+ *
+ * CLamellaBuilder::Assemble (LamellaBuilder.cpp:126-1010) with the geometry
+ * of CInitialStateLamella::ValidateData (InitialStateLamella.cpp:705-770),
+ * no walls and no polymerised bonds, restated operation by operation:
+ *   - the bilayer polymers (type lipid_type, in polymer order) split into the
+ *     upper monolayer (the first (long)(upper_fraction * total)) and the
+ *     lower one; each monolayer's polymers sit on the vertices of a hexagonal
+ *     lattice of spacing 0.999 sqrt(1.1547 area / count), walked row by row
+ *     from (0.001 e1x, 0.001 e2y) (LamellaBuilder.cpp:250-290, 382-650);
+ *   - per polymer: the tail at centre + sign 0.2, the head at the monolayer's
+ *     head plane, the beads between on the head-tail line spaced
+ *     0.5 thickness / (beads head..tail - 1) (linearise), or scattered about
+ *     the axis with three draws each;
+ *   - the other polymers, in polymer order, in the free regions below and
+ *     above the bilayer (CBuilder::isRandom::Assemble, Builder.cpp:293-480):
+ *     one draw choosing the region by its share of the free length, three
+ *     draws per bead ((0.95 L) u in-plane, region start + width u along the
+ *     normal), then the polymer's bonds shortened as the random builder's;
+ *   - unPBC = x (Builder.cpp:4391-4404);
+ *   - in-plane Maxwell velocities (CBuilder::AssignMaxwellVelocities, 2-d
+ *     branch, Builder.cpp:4207-4330): per bead the table index and
+ *     phi = 2 pi u, v = vmag (cos phi, sin phi); centre-of-mass velocity
+ *     removed, velocities divided by sqrt(sum v.v / (2 N kT)), the pair placed
+ *     in the two in-plane axes (normal x: (0, VY, VX); y: (VX, 0, VY);
+ *     z: (VX, VY, 0)).
+ * Beads: n in polymer order; polymer p holds beads [poly_first[p],
+ * poly_first[p+1]); head_offset / tail_offset are the bilayer polymer's head
+ * and tail bead offsets; normal 0, 1, 2 = x, y, z; bonds as bead indices in
+ * polymer order.  Returns 0, -1 for bad arguments, -2 when the bilayer does
+ * not fit the box, -3 when the lattice runs out of the box (the reference's
+ * "lamella lattice outside SimBox"). */
+int dpdo_lamella_state(int64_t n, const double L[3], double kT, uint64_t seed, int64_t skip, int64_t npoly,
+                       const int64_t* poly_first, const int32_t* poly_type, int32_t lipid_type,
+                       int32_t head_offset, int32_t tail_offset, int32_t normal, double centre_frac,
+                       double thickness, int32_t linearise, double upper_fraction, int64_t nb,
+                       const int64_t* bond_head, const int64_t* bond_tail, double* x3, double* v3)
+{
+    if (n < 1 || npoly < 1 || normal < 0 || normal > 2 || poly_first[0] != 0 || poly_first[npoly] != n) return -1;
+    /* the lattice lengths (InitialStateLamella.cpp:705-730) and the axes that
+     * take the lattice's two coordinates (LamellaBuilder.cpp:440-600: normal x:
+     * y, z; normal y: z, x; normal z: x, y) */
+    const double l1 = normal == 0 ? L[1] : L[0], l2 = normal == 2 ? L[1] : L[2], Ln = L[normal];
+    const int p0 = normal == 0 ? 1 : (normal == 1 ? 2 : 0), p1 = normal == 0 ? 2 : (normal == 1 ? 0 : 1);
+    const double centre = centre_frac * Ln;
+    if (centre + 0.5 * thickness > Ln || centre - 0.5 * thickness < 0.0) return -2;
+    double lower = centre - 0.5 * thickness, upper = centre + 0.5 * thickness;
+    const double area = l1 * l2;
+    int64_t total = 0, first_lipid = -1, size = 0;
+    for (int64_t p = 0; p < npoly; ++p)
+        if (poly_type[p] == lipid_type) {
+            if (first_lipid < 0) { first_lipid = p; size = poly_first[p + 1] - poly_first[p]; }
+            else if (poly_first[p + 1] - poly_first[p] != size) return -1;
+            ++total;
+        }
+    if (total == 0 || head_offset < 0 || tail_offset < 0 || head_offset >= size || tail_offset >= size ||
+        head_offset == tail_offset)
+        return -1;
+    /* beads head..tail inclusive (LamellaBuilder.cpp:300-336) */
+    int64_t counter = 0;
+    {
+        int bcount = 0, pend = -1;
+        for (int64_t k = 0; k < size; ++k) {
+            if (k == head_offset && !bcount) { bcount = 1; pend = tail_offset; counter++; }
+            else if (k == tail_offset && !bcount) { bcount = 1; pend = head_offset; counter++; }
+            else if (k == pend) { bcount = 0; counter++; }
+            else if (bcount) counter++;
+        }
+    }
+    int64_t mtot[2], mfirst[2], lat[2];
+    double mhead[2];
+    const double msign[2] = {1.0, -1.0};
+    mtot[0] = (int64_t)(upper_fraction * (double)total);
+    mtot[1] = total - mtot[0];
+    int mono = 0;
+    if (mtot[0] == 0) {
+        mono = 1; mfirst[0] = 0; mfirst[1] = 0; lat[0] = 0; lat[1] = mtot[1];
+        mhead[0] = 0.0; mhead[1] = lower; upper = centre;
+    } else if (mtot[1] == 0) {
+        mono = 1; mfirst[0] = 0; mfirst[1] = 0; lat[0] = mtot[0]; lat[1] = 0;
+        mhead[0] = upper; mhead[1] = 0.0; lower = centre;
+    } else {
+        mfirst[0] = 0; mfirst[1] = mtot[0]; lat[0] = mtot[0]; lat[1] = mtot[1];
+        mhead[0] = upper; mhead[1] = lower;
+    }
+    double hs[2];
+    if (mono) {
+        if (mtot[0] == 0) { hs[0] = 0.0; hs[1] = 0.999 * sqrt(1.1547 * area / (double)lat[1]); }
+        else { hs[0] = 0.999 * sqrt(1.1547 * area / (double)lat[0]); hs[1] = 0.0; }
+    } else {
+        hs[0] = 0.999 * sqrt(1.1547 * area / (double)lat[0]);
+        hs[1] = 0.999 * sqrt(1.1547 * area / (double)lat[1]);
+    }
+    const double e1x[2] = {hs[0], hs[1]}, e2x[2] = {0.5 * hs[0], 0.5 * hs[1]};
+    const double e2y[2] = {0.866025 * hs[0], 0.866025 * hs[1]};
+    double cspace[2];
+    cspace[0] = 0.5 * thickness / (double)(counter - 1);
+    cspace[1] = cspace[0];
+    /* the bilayer polymers in polymer order */
+    int64_t* lip = (int64_t*)malloc(sizeof(int64_t) * (size_t)total);
+    if (!lip) return -1;
+    for (int64_t p = 0, k = 0; p < npoly; ++p)
+        if (poly_type[p] == lipid_type) lip[k++] = p;
+    uint64_t st = seed;
+    for (int64_t k = 0; k < skip; ++k) (void)rb_draw(&st);
+    for (int mi = 0; mi < 2; ++mi) {
+        double hexp[3] = {0.001 * e1x[mi], 0.001 * e2y[mi], 0.0};
+        double xp[3] = {hexp[0], hexp[1], hexp[2]};
+        int64_t rowCounter = 0;
+        for (int64_t iv = mfirst[mi]; iv < mfirst[mi] + lat[mi]; ++iv) {
+            const int64_t b0 = poly_first[lip[iv]];
+            double* head = x3 + 3 * (b0 + head_offset);
+            double* tail = x3 + 3 * (b0 + tail_offset);
+            tail[p0] = xp[0];
+            tail[p1] = xp[1];
+            tail[normal] = centre + msign[mi] * 0.2;
+            head[p0] = xp[0];
+            head[p1] = xp[1];
+            head[normal] = mhead[mi];
+            double beadCounter = 1.0;
+            for (int64_t k = 0; k < size; ++k) {
+                if (k == head_offset || k == tail_offset) continue;
+                double* q = x3 + 3 * (b0 + k);
+                if (linearise) {
+                    q[p0] = xp[0];
+                    q[p1] = xp[1];
+                    q[normal] = head[normal] - msign[mi] * beadCounter * cspace[mi];
+                    beadCounter += 1.0;
+                } else {
+                    /* three draws, axes in x, y, z order as the reference's statements */
+                    for (int d = 0; d < 3; ++d) {
+                        if (d == normal) q[d] = centre + 0.5 * msign[mi] * thickness * rb_draw(&st);
+                        else if (d == p0) q[d] = xp[0] + 0.5 * e1x[mi] * rb_draw(&st);
+                        else q[d] = xp[1] + 0.5 * e2y[mi] * rb_draw(&st);
+                    }
+                    if (q[p0] > L[p0]) q[p0] -= 0.5 * e1x[mi];
+                    if (q[p1] > L[p1]) q[p1] -= 0.5 * e2y[mi];
+                }
+            }
+            /* the next vertex (LamellaBuilder.cpp:605-650) */
+            hexp[0] += e1x[mi];
+            if (hexp[0] > l1 + (double)rowCounter * e2x[mi]) {
+                rowCounter++;
+                hexp[0] = (double)rowCounter * e2x[mi];
+                hexp[1] += e2y[mi];
+                xp[0] = hexp[0];
+                xp[1] = hexp[1];
+                if (hexp[1] >= l2) { free(lip); return -3; }
+            } else if (hexp[0] > l1) {
+                xp[0] = hexp[0] - l1;
+            } else {
+                xp[0] = hexp[0];
+                xp[1] = hexp[1];
+            }
+        }
+    }
+    free(lip);
+    /* the other polymers in the free regions (Builder.cpp:293-480) */
+    const double ex[6] = {0.0, 0.0, lower, upper, Ln - 0.0, Ln};
+    double freeLength = 0.0, ratio[2];
+    for (int i = 1; i < 3; ++i) freeLength += ex[2 * i] - ex[2 * i - 1];
+    {
+        double cum = 0.0;
+        for (int i = 1; i < 3; ++i) { cum += (ex[2 * i] - ex[2 * i - 1]) / freeLength; ratio[i - 1] = cum; }
+    }
+    int64_t bq = 0;   /* bonds in polymer order: the next bond to look at */
+    for (int64_t p = 0; p < npoly; ++p) {
+        const int64_t b0 = poly_first[p], b1 = poly_first[p + 1];
+        while (bq < nb && bond_head[bq] < b0) ++bq;
+        if (poly_type[p] == lipid_type) continue;
+        const double rindex = rb_draw(&st);
+        int index = 0, unassigned = 1;
+        for (int k = 0; k < 2; ++k)
+            if (unassigned && rindex <= ratio[k]) { unassigned = 0; index = k; }
+        const double width = ex[2 * index + 2] - ex[2 * index + 1];
+        for (int64_t b = b0; b < b1; ++b) {
+            double xp[3];
+            for (int d = 0; d < 3; ++d) {
+                if (d == normal) xp[d] = ex[2 * index + 1] + width * rb_draw(&st);
+                else xp[d] = 0.95 * L[d] * rb_draw(&st);
+            }
+            for (int d = 0; d < 3; ++d) x3[3 * b + d] = xp[d];
+        }
+        for (int64_t k = bq; k < nb && bond_head[k] < b1 && bond_head[k] >= b0; ++k) {
+            double* h = x3 + 3 * bond_head[k];
+            double* t = x3 + 3 * bond_tail[k];
+            const double rd[3] = {t[0] - h[0], t[1] - h[1], t[2] - h[2]};
+            const double rmag = sqrt(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+            const double ru[3] = {rd[0] / rmag, rd[1] / rmag, rd[2] / rmag};
+            for (int d = 0; d < 3; ++d)
+                if (fabs(rd[d]) > 1.0) t[d] = h[d] + ru[d];
+        }
+    }
+    /* in-plane Maxwell velocities (Builder.cpp:4207-4330, 2-d branch) */
+    const int64_t M = n > 10000000 ? n : 10000000;
+    double* tab = (double*)malloc(sizeof(double) * (size_t)M);
+    double* vx = (double*)malloc(sizeof(double) * (size_t)n);
+    double* vy = (double*)malloc(sizeof(double) * (size_t)n);
+    if (!tab || !vx || !vy) { free(tab); free(vx); free(vy); return -1; }
+    {
+        const double dM = (double)M;
+        double factor = 1.0;
+        for (int64_t j = 0; j < M - 1; ++j) {
+            const double vel = sqrt(2.0 * log(dM * factor / (dM - factor)));
+            factor = exp(0.5 * vel * vel);
+            tab[j] = vel;
+        }
+        tab[M - 1] = tab[M - 2];
+    }
+    const double twopi = 2.0 * 3.141592653589793238;   /* xxBase::m_globalTwoPI */
+    double vcm[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t index = (int64_t)((double)(size_t)M * rb_draw(&st));
+        const double vmag = tab[index];
+        const double vphi = twopi * rb_draw(&st);
+        vx[i] = vmag * cos(vphi);
+        vy[i] = vmag * sin(vphi);
+        vcm[0] += vx[i];
+        vcm[1] += vy[i];
+    }
+    free(tab);
+    const double dn = (double)n;
+    vcm[0] /= dn;
+    vcm[1] /= dn;
+    vcm[2] /= dn;
+    double vtotal = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        vx[i] -= vcm[0];
+        vy[i] -= vcm[1];
+        const double vz = 0.0 - vcm[2];
+        vtotal = vtotal + vx[i] * vx[i] + vy[i] * vy[i] + vz * vz;
+    }
+    vtotal = sqrt(vtotal / (2.0 * dn * kT));
+    for (int64_t i = 0; i < n; ++i) {
+        const double VX = vx[i] / vtotal, VY = vy[i] / vtotal;
+        double* v = v3 + 3 * i;
+        if (normal == 0) { v[0] = 0.0; v[1] = VY; v[2] = VX; }
+        else if (normal == 1) { v[0] = VX; v[1] = 0.0; v[2] = VY; }
+        else { v[0] = VX; v[1] = VY; v[2] = 0.0; }
+    }
+    free(vx);
+    free(vy);
+    return 0;
+}

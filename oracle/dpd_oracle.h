@@ -112,6 +112,14 @@ int dpdo_renormalise_mom(dpdo_sim* s);
  * Returns 0, or -1 - i when bead i falls outside the box. */
 int dpdo_random_state(int64_t n, const double L[3], double kT, uint64_t seed, int64_t skip, int64_t nb,
                       const int64_t* bond_head, const int64_t* bond_tail, double* x3, double* v3);
+/* CLamellaBuilder::Assemble restated (no walls, no polymerised bonds); see
+ * dpd_oracle.c.  Returns 0, -1 bad arguments, -2 bilayer outside the box,
+ * -3 lattice outside the box. */
+int dpdo_lamella_state(int64_t n, const double L[3], double kT, uint64_t seed, int64_t skip, int64_t npoly,
+                       const int64_t* poly_first, const int32_t* poly_type, int32_t lipid_type,
+                       int32_t head_offset, int32_t tail_offset, int32_t normal, double centre_frac,
+                       double thickness, int32_t linearise, double upper_fraction, int64_t nb,
+                       const int64_t* bond_head, const int64_t* bond_tail, double* x3, double* v3);
 
 #ifdef __cplusplus
 }

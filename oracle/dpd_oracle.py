@@ -68,6 +68,9 @@ def lib() -> C.CDLL:
         L.dpdo_slice_errors.restype = C.c_int64
         L.dpdo_random_state.argtypes = [C.c_int64, vp, C.c_double, C.c_uint64, C.c_int64, C.c_int64, vp, vp,
                                         vp, vp]
+        L.dpdo_lamella_state.argtypes = [C.c_int64, vp, C.c_double, C.c_uint64, C.c_int64, C.c_int64, vp, vp,
+                                         C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                         C.c_int32, C.c_double, C.c_int64, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -192,20 +195,47 @@ def random_state(n: int, L, kT: float, seed: int, skip: int = 0, bond_head=None,
     return x, v
 
 
+def lamella_state(L, kT: float, seed: int, poly_first, poly_type, lipid_type: int, head_offset: int,
+                  tail_offset: int, normal: int = 2, centre: float = 0.5, thickness: float = 5.0,
+                  linearise: bool = True, upper_fraction: float = 0.5, skip: int = 0, bond_head=None,
+                  bond_tail=None):
+    """CLamellaBuilder::Assemble restated (dpdo_lamella_state): (x, v), each
+    (n, 3) in bead order; polymer p holds beads [poly_first[p],
+    poly_first[p+1]); bonds as bead indices in polymer order."""
+    pf = np.ascontiguousarray(poly_first, dtype=np.int64)
+    pt = np.ascontiguousarray(poly_type, dtype=np.int32)
+    n = int(pf[-1])
+    x = np.zeros((n, 3))
+    v = np.zeros((n, 3))
+    Lv = np.ascontiguousarray(L, dtype=np.float64)
+    bh = np.ascontiguousarray(bond_head if bond_head is not None else [], dtype=np.int64)
+    bt = np.ascontiguousarray(bond_tail if bond_tail is not None else [], dtype=np.int64)
+    rc = lib().dpdo_lamella_state(n, _p(Lv), kT, seed, skip, len(pt), _p(pf), _p(pt), lipid_type, head_offset,
+                                  tail_offset, normal, centre, thickness, int(bool(linearise)), upper_fraction,
+                                  len(bh), _p(bh), _p(bt), _p(x), _p(v))
+    if rc != 0:
+        raise ValueError({-1: "bad arguments", -2: "the bilayer does not fit the box",
+                          -3: "lamella lattice outside the box"}.get(rc, str(rc)))
+    return x, v
+
+
 def philox_pair(seed: int, step: int, id_lo: int, id_hi: int) -> int:
     return int(lib().dpdo_philox_pair(seed, step, id_lo, id_hi))
 
 
 def run_reference(system, steps: int, workdir: str = None, kT: float = None, gamma_scale: float = 1.0,
                   inject: bool = True, dump: bool = True, topology: bool = False, timeout: float = None,
-                  rng_seed: int = None, slices: int = 0, initial: bool = False, paraview: bool = False):
+                  rng_seed: int = None, slices: int = 0, initial: bool = False, paraview: bool = False,
+                  state=None):
     """Runs the unmodified reference (oracle/_ref/osprey_ref_driver) on
     ``system`` for ``steps`` steps; ``rng_seed`` restarts its pair-noise LCG
     at that value just before the step loop; ``slices`` > 0 sets the analysis
     grid to that many z slices and also returns the last step's slice stress
     profile; ``initial`` adds the builder's state before any step as
     summary["initial"]; ``paraview`` the bytes of the reference's Paraview
-    snapshot of the last step as summary["paraview"].  Returns (json summary, dump dict or None, topology dict or None)
+    snapshot of the last step as summary["paraview"]; ``state`` the control
+    file's initial-state block (workloads.lamella_block, default random).
+    Returns (json summary, dump dict or None, topology dict or None)
     or, with ``slices``, (summary, dump, topology, slice dict)."""
     from osprey_dpd_b200 import workloads  # local import: test-side helper
 
@@ -215,7 +245,7 @@ def run_reference(system, steps: int, workdir: str = None, kT: float = None, gam
     wd = workdir or tempfile.mkdtemp(prefix="dpdref_")
     run = "r"
     workloads.write_dmpci(system, os.path.join(wd, "dmpci." + run), steps, kT=kT, gamma_scale=gamma_scale,
-                          grid_z=max(1, int(slices)))
+                          grid_z=max(1, int(slices)), state=state)
     args = [REF_DRIVER, run]
     if inject:
         workloads.write_state(system, os.path.join(wd, "state.bin"))

@@ -388,14 +388,30 @@ def polymer_fractions(system: DpdSystem) -> List[float]:
     return fr
 
 
+def lamella_block(polymer: str, normal=(0, 0, 1), centre: float = 0.5, thickness: float = 5.0,
+                  linearise: bool = True, upper_fraction: float = 0.5) -> List[str]:
+    """The `State lamella` block of a control data file (CInitialStateLamella,
+    InitialStateLamella.cpp): the bilayer polymer, the normal axis, the
+    mid-plane as a fraction of the box length, the bilayer thickness, straight
+    or scattered chains, the fraction in the upper monolayer; no polymerised
+    bonds."""
+    return ["State\tlamella", f"        Polymer\t\t\t{polymer}",
+            f"        Normal\t\t\t{normal[0]} {normal[1]} {normal[2]}", f"        Centre\t\t\t{centre!r}",
+            f"        Thickness\t\t{thickness!r}", f"        Linearise\t\t{1 if linearise else 0}",
+            f"        UpperFraction\t{upper_fraction!r}", "        Polymerise\t\t0"]
+
+
 def write_dmpci(system: DpdSystem, path: str, steps: int, kT: float = None, seed: int = None,
-                gamma_scale: float = 1.0, title: str = "synthetic", grid_z: int = 1) -> None:
+                gamma_scale: float = 1.0, title: str = "synthetic", grid_z: int = 1,
+                state: List[str] = None) -> None:
     """Osprey-DPD control data file (InputDPDFile.cpp:400-800) for ``system``
     running ``steps`` steps with sampling, display and restart only at the end;
-    ``grid_z`` analysis-grid slices along z (the slice stress profile's)."""
+    ``grid_z`` analysis-grid slices along z (the slice stress profile's);
+    ``state`` the initial-state block (default `State random`, or
+    lamella_block(...))."""
     T = len(system.type_names)
     lines = ["dpd", "", f'Title\t" {title} "', "Date    03/12/26",
-             f'Comment\t" generated {system.name} system "', "", "State\trandom", ""]
+             f'Comment\t" generated {system.name} system "', ""] + (state or ["State\trandom"]) + [""]
     for i, name in enumerate(system.type_names):
         lines.append(f"Bead  {name}")
         lines.append("      0.5")
