@@ -147,6 +147,31 @@ DPD_API int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id,
                                     uint64_t rng_seed, int64_t rng_skip, int64_t nb, const int64_t* bond_head,
                                     const int64_t* bond_tail, double* x3_out, double* v3_out);
 
+/* Builds the lamella initial state of CLamellaBuilder::Assemble
+ * (LamellaBuilder.cpp:126-1010; no walls, no polymerised bonds) on the device
+ * and uploads it as dpd_engine_upload_beads would (unPBC = x, F = 0, all
+ * movable), with the in-plane Maxwell velocities of
+ * CBuilder::AssignMaxwellVelocities (Builder.cpp:4207-4330).  Beads in the
+ * reference's creation order (id, type); polymer p holds beads
+ * [poly_first[p], poly_first[p+1]) (npoly + 1 entries) and has type
+ * poly_type[p]; the bilayer is made of the polymers of type lipid_type, whose
+ * head and tail beads sit at head_offset / tail_offset; normal 0, 1, 2 = x, y,
+ * z; centre a fraction of the box length along the normal; thickness, straight
+ * (linearise) or scattered chains, the upper monolayer's share as the
+ * control file's State lamella block gives them.  The reference's generator
+ * starts at rng_seed with rng_skip draws consumed first; bonds are bead
+ * indices in polymer order (the other polymers' bonds are shortened as the
+ * reference does).  Positions equal the reference's bit for bit; velocities
+ * agree to a few ulps (device sin/cos, tree sums).  x3_out / v3_out receive
+ * the built state when not NULL.  DPD_E_ARG when the bilayer or its lattice
+ * does not fit the box. */
+DPD_API int dpd_engine_build_lamella(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type,
+                                     int64_t npoly, const int64_t* poly_first, const int32_t* poly_type,
+                                     int32_t lipid_type, int32_t head_offset, int32_t tail_offset, int32_t normal,
+                                     double centre, double thickness, int32_t linearise, double upper_fraction,
+                                     uint64_t rng_seed, int64_t rng_skip, int64_t nb, const int64_t* bond_head,
+                                     const int64_t* bond_tail, double* x3_out, double* v3_out);
+
 /* Bonds (CBond: head id, tail id, k2, l0; Bond.h:45-52) and bond pairs
  * (CBondPair: indices of its first and second bond in this bond list, k3,
  * phi0 in radians; BondPair.h:23-30). */

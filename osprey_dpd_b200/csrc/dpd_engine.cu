@@ -1460,6 +1460,258 @@ int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id, const i
     return upload_staged(e, n, nullptr, id, type, in);
 }
 
+int dpd_engine_build_lamella(dpd_engine* e, int64_t n, const int64_t* id, const int32_t* type, int64_t npoly,
+                             const int64_t* poly_first, const int32_t* poly_type, int32_t lipid_type,
+                             int32_t head_offset, int32_t tail_offset, int32_t normal, double centre_frac,
+                             double thickness, int32_t linearise, double upper_fraction, uint64_t rng_seed,
+                             int64_t rng_skip, int64_t nb, const int64_t* bond_head, const int64_t* bond_tail,
+                             double* x3_out, double* v3_out)
+{
+    if (!e) return DPD_E_ARG;
+    if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || npoly < 1 || npoly > n || !poly_first || !poly_type ||
+        rng_skip < 0 || nb < 0 || (nb > 0 && (!bond_head || !bond_tail)) || normal < 0 || normal > 2 ||
+        !(thickness > 0.0) || !(upper_fraction >= 0.0 && upper_fraction <= 1.0))
+        return fail(e, DPD_E_ARG, "bad arguments");
+    if (e->hboxes.size() != 1) return fail(e, DPD_E_ARG, "the lamella builder fills a single box");
+    if (poly_first[0] != 0 || poly_first[npoly] != n) return fail(e, DPD_E_ARG, "polymers must cover the beads");
+    for (int64_t p = 0; p < npoly; ++p)
+        if (poly_first[p + 1] <= poly_first[p]) return fail(e, DPD_E_ARG, "empty or unordered polymer");
+    for (int64_t k = 0; k < nb; ++k)
+        if (bond_head[k] < 0 || bond_head[k] >= n || bond_tail[k] < 0 || bond_tail[k] >= n ||
+            bond_head[k] == bond_tail[k])
+            return fail(e, DPD_E_ARG, "bond bead index out of range");
+    const Box& B = e->hboxes[0];
+    // InitialStateLamella.cpp:705-770: lattice lengths, mid-plane, head planes
+    LamellaParams P{};
+    P.normal = normal;
+    P.p0 = normal == 0 ? 1 : (normal == 1 ? 2 : 0);   // LamellaBuilder.cpp:440-600
+    P.p1 = normal == 0 ? 2 : (normal == 1 ? 0 : 1);
+    for (int d = 0; d < 3; ++d) P.L[d] = B.L[d];
+    const double l1 = normal == 0 ? B.L[1] : B.L[0], l2 = normal == 2 ? B.L[1] : B.L[2], Ln = B.L[normal];
+    const double centre = centre_frac * Ln;
+    if (centre + 0.5 * thickness > Ln || centre - 0.5 * thickness < 0.0)
+        return fail(e, DPD_E_ARG, "the bilayer does not fit the box");
+    double lower = centre - 0.5 * thickness, upper = centre + 0.5 * thickness;
+    const double area = l1 * l2;
+    // the bilayer polymers (type lipid_type, in polymer order), all one size
+    std::vector<int64_t> lip;
+    int64_t size = 0;
+    for (int64_t p = 0; p < npoly; ++p)
+        if (poly_type[p] == lipid_type) {
+            const int64_t m = poly_first[p + 1] - poly_first[p];
+            if (lip.empty()) size = m;
+            else if (m != size) return fail(e, DPD_E_ARG, "bilayer polymers of different sizes");
+            lip.push_back(p);
+        }
+    const int64_t total = (int64_t)lip.size();
+    if (total == 0 || head_offset < 0 || tail_offset < 0 || head_offset >= size || tail_offset >= size ||
+        head_offset == tail_offset)
+        return fail(e, DPD_E_ARG, "no bilayer polymers, or bad head / tail offsets");
+    int64_t counter = 0;   // beads head..tail inclusive (LamellaBuilder.cpp:300-336)
+    {
+        bool bcount = false;
+        int64_t pend = -1;
+        for (int64_t k = 0; k < size; ++k) {
+            if (k == head_offset && !bcount) { bcount = true; pend = tail_offset; counter++; }
+            else if (k == tail_offset && !bcount) { bcount = true; pend = head_offset; counter++; }
+            else if (k == pend) { bcount = false; counter++; }
+            else if (bcount) counter++;
+        }
+    }
+    // monolayers (LamellaBuilder.cpp:180-222) and their lattices (:250-290)
+    int64_t mtot[2], mfirst[2], lat[2];
+    P.msign[0] = 1.0;
+    P.msign[1] = -1.0;
+    mtot[0] = (int64_t)(upper_fraction * (double)total);
+    mtot[1] = total - mtot[0];
+    const bool mono1 = mtot[0] == 0 || mtot[1] == 0;
+    if (mtot[0] == 0) {
+        mfirst[0] = mfirst[1] = 0; lat[0] = 0; lat[1] = mtot[1];
+        P.mhead[0] = 0.0; P.mhead[1] = lower; upper = centre;
+    } else if (mtot[1] == 0) {
+        mfirst[0] = mfirst[1] = 0; lat[0] = mtot[0]; lat[1] = 0;
+        P.mhead[0] = upper; P.mhead[1] = 0.0; lower = centre;
+    } else {
+        mfirst[0] = 0; mfirst[1] = mtot[0]; lat[0] = mtot[0]; lat[1] = mtot[1];
+        P.mhead[0] = upper; P.mhead[1] = lower;
+    }
+    double hs[2];
+    if (mono1) {
+        if (mtot[0] == 0) { hs[0] = 0.0; hs[1] = 0.999 * std::sqrt(1.1547 * area / (double)lat[1]); }
+        else { hs[0] = 0.999 * std::sqrt(1.1547 * area / (double)lat[0]); hs[1] = 0.0; }
+    } else {
+        hs[0] = 0.999 * std::sqrt(1.1547 * area / (double)lat[0]);
+        hs[1] = 0.999 * std::sqrt(1.1547 * area / (double)lat[1]);
+    }
+    double e2x[2];
+    for (int mi = 0; mi < 2; ++mi) {
+        P.e1x[mi] = hs[mi];
+        e2x[mi] = 0.5 * hs[mi];
+        P.e2y[mi] = 0.866025 * hs[mi];
+    }
+    P.cspace[0] = 0.5 * thickness / (double)(counter - 1);
+    P.cspace[1] = P.cspace[0];
+    P.centre = centre;
+    P.thickness = thickness;
+    P.size = (int)size;
+    P.head_offset = head_offset;
+    P.tail_offset = tail_offset;
+    P.lipid_type = lipid_type;
+    P.linearise = linearise ? 1 : 0;
+    // the lattice walk of each monolayer (LamellaBuilder.cpp:382-650): the
+    // site of every bilayer polymer, in the reference's floating-point order
+    std::vector<double> site(2 * (size_t)total);
+    std::vector<int> mono((size_t)total);
+    for (int mi = 0; mi < 2; ++mi) {
+        double hexp[2] = {0.001 * P.e1x[mi], 0.001 * P.e2y[mi]};
+        double xp[2] = {hexp[0], hexp[1]};
+        int64_t rowCounter = 0;
+        for (int64_t iv = mfirst[mi]; iv < mfirst[mi] + lat[mi]; ++iv) {
+            site[2 * (size_t)iv] = xp[0];
+            site[2 * (size_t)iv + 1] = xp[1];
+            mono[(size_t)iv] = mi;
+            hexp[0] += P.e1x[mi];
+            if (hexp[0] > l1 + (double)rowCounter * e2x[mi]) {
+                rowCounter++;
+                hexp[0] = (double)rowCounter * e2x[mi];
+                hexp[1] += P.e2y[mi];
+                xp[0] = hexp[0];
+                xp[1] = hexp[1];
+                if (hexp[1] >= l2) return fail(e, DPD_E_ARG, "lamella lattice outside the box");
+            } else if (hexp[0] > l1) {
+                xp[0] = hexp[0] - l1;
+            } else {
+                xp[0] = hexp[0];
+                xp[1] = hexp[1];
+            }
+        }
+    }
+    // each polymer's first draw: the bilayer polymers in order (three per
+    // scattered bead), then the other polymers in polymer order (one, then
+    // three per bead); the velocities after all of them
+    std::vector<int64_t> pdraw((size_t)npoly);
+    std::vector<int> plip((size_t)npoly, -1), bpoly((size_t)n), ptype(poly_type, poly_type + npoly);
+    const int64_t per_lipid = P.linearise ? 0 : 3 * (size - 2);
+    for (int64_t j = 0; j < total; ++j) {
+        pdraw[(size_t)lip[(size_t)j]] = per_lipid * j;
+        plip[(size_t)lip[(size_t)j]] = (int)j;
+    }
+    int64_t draws = per_lipid * total;
+    for (int64_t p = 0; p < npoly; ++p) {
+        for (int64_t b = poly_first[p]; b < poly_first[p + 1]; ++b) bpoly[(size_t)b] = (int)p;
+        if (poly_type[p] == lipid_type) continue;
+        pdraw[(size_t)p] = draws;
+        draws += 1 + 3 * (poly_first[p + 1] - poly_first[p]);
+    }
+    P.vel_base = (uint64_t)draws;
+    P.seed = rng_seed;
+    P.skip = (uint64_t)rng_skip;
+    // the free regions along the normal (LamellaBuilder.cpp:960-990, Builder.cpp:350-372)
+    const double ex[6] = {0.0, 0.0, lower, upper, Ln - 0.0, Ln};
+    for (int k = 0; k < 6; ++k) P.ex[k] = ex[k];
+    {
+        double freeLength = 0.0, cum = 0.0;
+        for (int i = 1; i < 3; ++i) freeLength += ex[2 * i] - ex[2 * i - 1];
+        for (int i = 1; i < 3; ++i) { cum += (ex[2 * i] - ex[2 * i - 1]) / freeLength; P.ratio[i - 1] = cum; }
+    }
+    // the other polymers' bonds (shortened per polymer in its bond order)
+    std::vector<int64_t> comp_ptr(1, 0), comp_bonds;
+    {
+        int64_t cur = -1;
+        for (int64_t k = 0; k < nb; ++k) {
+            const int64_t p = bpoly[(size_t)bond_head[k]];
+            if (poly_type[p] == lipid_type) continue;
+            if (bpoly[(size_t)bond_tail[k]] != p) return fail(e, DPD_E_ARG, "a bond joins two polymers");
+            if (p < cur) return fail(e, DPD_E_ARG, "bonds not in polymer order");
+            if (p != cur) {
+                if (cur >= 0) comp_ptr.push_back((int64_t)comp_bonds.size());
+                cur = p;
+            }
+            comp_bonds.push_back(k);
+        }
+        if (cur >= 0) comp_ptr.push_back((int64_t)comp_bonds.size());
+    }
+    const int ncomp = (int)comp_ptr.size() - 1;
+    const std::vector<double>& tab = maxwell_table(n);
+    P.ntab = (int64_t)tab.size();
+    CU(cudaSetDevice(e->device));
+    if (int rc0 = drop_ahead(e)) return rc0;   // the new state replaces the drifted one
+    CU(cudaStreamSynchronize(e->s()));
+    cudaStream_t st = e->s();
+    int rc;
+    if ((rc = stage_buffers(e, n))) return rc;
+    double* up = e->d_up;
+    int* upi = reinterpret_cast<int*>(up + 13 * (size_t)n);
+    const int nblk = blocks_for(n, kRbThreads);
+    // scratch of the build, released at the end
+    double* d_tab = nullptr;
+    double* d_part = nullptr;
+    double* d_site = nullptr;
+    int64_t* d_i64 = nullptr;   // pfirst (npoly + 1), pdraw (npoly), bond heads, tails, comp_ptr, comp_bonds
+    int* d_i32 = nullptr;       // bpoly (n), ptype, plip (npoly), mono (total)
+    auto release = [&]() { dfree(e, d_tab); dfree(e, d_part); dfree(e, d_site); dfree(e, d_i64); dfree(e, d_i32); };
+    const size_t n64 = (size_t)(2 * npoly + 1) + (nb > 0 ? 2 * (size_t)nb + comp_ptr.size() + comp_bonds.size() : 0);
+    const size_t n32 = (size_t)n + 2 * (size_t)npoly + (size_t)total;
+    if ((rc = dalloc(e, &d_tab, tab.size())) || (rc = dalloc(e, &d_part, 3 * (size_t)nblk + 8)) ||
+        (rc = dalloc(e, &d_site, site.size())) || (rc = dalloc(e, &d_i64, n64)) || (rc = dalloc(e, &d_i32, n32))) {
+        release();
+        return rc;
+    }
+    UploadIn in{};
+    in.x = up;
+    in.v = up + 6 * (size_t)n;
+    in.id = reinterpret_cast<const int64_t*>(up + 12 * (size_t)n);
+    in.type = upi;
+    auto run = [&]() -> int {
+        int64_t* dpf = d_i64;
+        int64_t* dpd = dpf + npoly + 1;
+        int* dbp = d_i32;
+        int* dpt = dbp + n;
+        int* dpl = dpt + npoly;
+        int* dmo = dpl + npoly;
+        CU(cudaMemcpyAsync(up + 12 * (size_t)n, id, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(upi, type, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(d_site, site.data(), sizeof(double) * site.size(), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dpf, poly_first, sizeof(int64_t) * (npoly + 1), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dpd, pdraw.data(), sizeof(int64_t) * npoly, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dbp, bpoly.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dpt, ptype.data(), sizeof(int) * npoly, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dpl, plip.data(), sizeof(int) * npoly, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dmo, mono.data(), sizeof(int) * total, cudaMemcpyHostToDevice, st));
+        k_lb_beads<<<nblk, kRbThreads, 0, st>>>((int)n, P, dbp, dpf, dpt, dpd, dpl, d_site, dmo, d_tab, up,
+                                                up + 6 * (size_t)n, d_part);
+        if (int r = check_launch(e, "k_lb_beads")) return r;
+        if (ncomp > 0) {
+            int64_t* dh = dpd + npoly;
+            int64_t* dt = dh + nb;
+            int64_t* dp = dt + nb;
+            int64_t* dc = dp + comp_ptr.size();
+            CU(cudaMemcpyAsync(dh, bond_head, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dt, bond_tail, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dp, comp_ptr.data(), sizeof(int64_t) * comp_ptr.size(), cudaMemcpyHostToDevice, st));
+            CU(cudaMemcpyAsync(dc, comp_bonds.data(), sizeof(int64_t) * comp_bonds.size(), cudaMemcpyHostToDevice,
+                               st));
+            k_rb_bonds<<<blocks_for(ncomp, kRbThreads), kRbThreads, 0, st>>>(ncomp, dp, dc, dh, dt, up);
+            if (int r = check_launch(e, "k_rb_bonds")) return r;
+        }
+        double* stats = d_part + 3 * (size_t)nblk;   // vcm[3], vtotal
+        k_rb_vcm<<<1, 32, 0, st>>>(nblk, (int)n, d_part, stats);
+        k_rb_center<<<nblk, kRbThreads, 0, st>>>((int)n, stats, up + 6 * (size_t)n, d_part);
+        k_lb_vtotal<<<1, 32, 0, st>>>(nblk, (int)n, e->params.kT, d_part, stats);
+        k_lb_scale<<<nblk, kRbThreads, 0, st>>>((int)n, normal, stats, up + 6 * (size_t)n);
+        if (int r = check_launch(e, "k_lb_scale")) return r;
+        if (x3_out) CU(cudaMemcpyAsync(x3_out, up, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        if (v3_out) CU(cudaMemcpyAsync(v3_out, up + 6 * (size_t)n, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        return DPD_OK;
+    };
+    rc = run();
+    release();
+    if (rc) return rc;
+    return upload_staged(e, n, nullptr, id, type, in);
+}
+
 int dpd_engine_upload_topology(dpd_engine* e, int64_t nb, const int64_t* bond_head_id, const int64_t* bond_tail_id,
                                const double* k2, const double* l0, int64_t na, const int64_t* first_bond,
                                const int64_t* second_bond, const double* k3, const double* phi0)

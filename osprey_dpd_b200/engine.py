@@ -45,7 +45,7 @@ EXPORTED = [
     "dpd_engine_set_restart_layout", "dpd_engine_write_restart", "dpd_engine_build_random",
     "dpd_write_paraview", "dpd_engine_write_paraview", "dpd_engine_renormalise_mom",
     "dpd_engine_slab_setup", "dpd_engine_slab_pack", "dpd_engine_slab_unpack", "dpd_engine_slab_counts",
-    "dpd_engine_bead_ids", "dpd_engine_slab_observables", "dpd_engine_set_pair_tile",
+    "dpd_engine_bead_ids", "dpd_engine_slab_observables", "dpd_engine_set_pair_tile", "dpd_engine_build_lamella",
 ]
 
 KERNEL_NAMES = ["update_pos", "scan_cells", "permute", "gather", "pair_forces", "update_mom",
@@ -102,6 +102,9 @@ def load(path: Optional[str] = None) -> C.CDLL:
     L.dpd_engine_create.argtypes = [C.POINTER(DpdParams), C.POINTER(vp)]
     L.dpd_engine_upload_beads.argtypes = [vp, C.c_int64] + [vp] * 7
     L.dpd_engine_build_random.argtypes = [vp, C.c_int64, vp, vp, C.c_uint64, C.c_int64, C.c_int64, vp, vp, vp, vp]
+    L.dpd_engine_build_lamella.argtypes = [vp, C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_uint64,
+                                           C.c_int64, C.c_int64, vp, vp, vp, vp]
     L.dpd_write_paraview.argtypes = [C.c_char_p, C.c_int64, vp, vp]
     L.dpd_engine_write_paraview.argtypes = [vp, C.c_char_p, vp, vp]
     L.dpd_engine_upload_topology.argtypes = [vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp]
@@ -256,6 +259,30 @@ class DpdEngine:
         v = np.zeros((n, 3))
         self._check(load().dpd_engine_build_random(self.h, n, _p(idv), _p(tv), int(seed), int(skip), len(bh), _p(bh),
                                                    _p(bt), _p(x), _p(v)), "build_random")
+        self.n = n
+        return x, v
+
+    def build_lamella(self, ids, types, poly_first, poly_type, lipid_type: int, head_offset: int, tail_offset: int,
+                      normal: int = 2, centre: float = 0.5, thickness: float = 5.0, linearise: bool = True,
+                      upper_fraction: float = 0.5, seed: int = 0, skip: int = 0, bond_head=None, bond_tail=None):
+        """The lamella initial state of CLamellaBuilder::Assemble built on the
+        device and uploaded (dpd_engine_build_lamella); beads in the
+        reference's creation order, polymer p holding beads
+        [poly_first[p], poly_first[p+1]).  Returns the built (x, v)."""
+        n = len(ids)
+        idv = np.ascontiguousarray(ids, np.int64)
+        tv = np.ascontiguousarray(types, np.int32)
+        pf = np.ascontiguousarray(poly_first, np.int64)
+        pt = np.ascontiguousarray(poly_type, np.int32)
+        bh = np.ascontiguousarray(bond_head if bond_head is not None else [], np.int64)
+        bt = np.ascontiguousarray(bond_tail if bond_tail is not None else [], np.int64)
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        self._check(load().dpd_engine_build_lamella(self.h, n, _p(idv), _p(tv), len(pt), _p(pf), _p(pt),
+                                                    int(lipid_type), int(head_offset), int(tail_offset), int(normal),
+                                                    float(centre), float(thickness), int(bool(linearise)),
+                                                    float(upper_fraction), int(seed), int(skip), len(bh), _p(bh),
+                                                    _p(bt), _p(x), _p(v)), "build_lamella")
         self.n = n
         return x, v
 
