@@ -221,7 +221,9 @@ def tune_candidates(reproducible: bool):
     return autotune.DEFAULT_CANDIDATES + autotune.HALF_SHELL_CANDIDATES + autotune.STAGED_CANDIDATES
 
 
-FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (32, 0, -1, 1, 64), "staged": (16, 0, 100, 2)}
+# default shape per scheme (half shell: hit lists of 24 and two-warp tiles, the
+# autotuner's choice on the bilayer and the fastest capacity on the melt)
+FIXED_SHAPES = {"full": (32, 0, -1, 0), "half": (24, 0, -1, 1, 64), "staged": (16, 0, 100, 2)}
 SCHEME_NAMES = {0: "full", 1: "half", 2: "staged"}
 PAIR_KERNELS = {"full": "k_pair_forces", "half": "k_pair_forces_half", "staged": "k_pair_forces_staged"}
 
