@@ -1163,6 +1163,7 @@ static int upload_impl(dpd_engine* e, int64_t n, const int32_t* box, const int64
                        const double* f3)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab's beads come from its exchange (dpd_engine_slab_unpack)");
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || !x3 || !v3) return fail(e, DPD_E_ARG, "bad bead arrays");
     if (!box && e->hboxes.size() > 1) return fail(e, DPD_E_ARG, "a batch needs the box of every bead");
     CU(cudaSetDevice(e->device));
@@ -1355,6 +1356,7 @@ int dpd_engine_build_random(dpd_engine* e, int64_t n, const int64_t* id, const i
                             double* x3_out, double* v3_out)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab's beads come from its exchange (dpd_engine_slab_unpack)");
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || rng_skip < 0 || nb < 0 ||
         (nb > 0 && (!bond_head || !bond_tail)))
         return fail(e, DPD_E_ARG, "bad arguments");
@@ -1468,6 +1470,7 @@ int dpd_engine_build_lamella(dpd_engine* e, int64_t n, const int64_t* id, const 
                              double* x3_out, double* v3_out)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab's beads come from its exchange (dpd_engine_slab_unpack)");
     if (n < 1 || n > ((int64_t)1 << 30) || !id || !type || npoly < 1 || npoly > n || !poly_first || !poly_type ||
         rng_skip < 0 || nb < 0 || (nb > 0 && (!bond_head || !bond_tail)) || normal < 0 || normal > 2 ||
         !(thickness > 0.0) || !(upper_fraction >= 0.0 && upper_fraction <= 1.0))
@@ -1913,6 +1916,7 @@ int dpd_engine_set_slice_stress(dpd_engine* e, int32_t nslices, int32_t nbondtyp
                                 int32_t nbptypes, const int32_t* bondpair_type)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "the slice profile covers a whole box; a slab also holds ghosts");
     if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "the slice stress profile needs a single-box engine");
     if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads (and the topology) before the slice profile");
     if (nslices < 0 || nslices > 65536 || nbondtypes < 0 || nbptypes < 0 || nbondtypes > 65536 || nbptypes > 65536)
@@ -2165,6 +2169,7 @@ int dpd_engine_set_restart_layout(dpd_engine* e, int64_t n, const int64_t* order
                                   const int32_t* poly_type, const double* radius_by_type)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "restart files cover a whole box; a slab also holds ghosts");
     if (!e->uploaded) return fail(e, DPD_E_STATE, "upload beads before the restart layout");
     if (n != e->n || !order || !poly_id || !poly_type || !radius_by_type)
         return fail(e, DPD_E_ARG, "the restart layout needs every bead, its polymer id and type, and the radii");
@@ -2297,6 +2302,7 @@ int dpd_write_paraview(const char* path, int64_t n, const double* x3, const int3
 int dpd_engine_write_paraview(dpd_engine* e, const char* path, const uint8_t* type_visible, const int32_t* display_id)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "snapshots cover a whole box; a slab also holds ghosts");
     if (!path) return fail(e, DPD_E_ARG, "null path");
     if (e->hboxes.size() > 1) return fail(e, DPD_E_STATE, "snapshots are written for single-box engines");
     const int64_t n = e->n;
@@ -2391,6 +2397,7 @@ int dpd_engine_set_conservative(dpd_engine* e, int32_t on)
 int dpd_engine_renormalise_mom(dpd_engine* e)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab holds ghosts: renormalise through the ranks' owned sums");
     if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
     if (e->hboxes.size() != 1) return fail(e, DPD_E_ARG, "momentum renormalisation is for single-box engines");
     if (!(e->params.kT > 0.0)) return fail(e, DPD_E_ARG, "momentum renormalisation needs kT > 0");
@@ -2585,6 +2592,7 @@ int dpd_engine_cells(dpd_engine* e, int32_t* cell)
 int dpd_engine_observables(dpd_engine* e, dpd_obs* out)
 {
     if (!e) return DPD_E_ARG;
+    if (e->slab) return fail(e, DPD_E_STATE, "a slab also holds ghosts: dpd_engine_slab_observables");
     if (!out) return fail(e, DPD_E_ARG, "null output");
     if (!e->uploaded) return fail(e, DPD_E_STATE, "no beads uploaded");
     CU(cudaSetDevice(e->device));

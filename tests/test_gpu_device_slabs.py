@@ -245,3 +245,21 @@ def test_device_slabs_over_gloo_ranks():
         assert obs["n"] == s.n
         assert abs(obs["kT"] - ref_obs["kT"]) <= 1e-9 * ref_obs["kT"]
         assert abs(obs["pressure"] - ref_obs["pressure"]) <= 1e-8 * abs(ref_obs["pressure"])
+
+
+def test_slab_refuses_whole_box_calls():
+    """A slab's local box also holds ghosts: the whole-box calls refuse it
+    and name the slab form where there is one."""
+    from osprey_dpd_b200 import engine as E, slabs as S
+    s = _system("polymer")
+    sl = S.DeviceSlabs(s, None, device=0, rank=0, world=2, precision=E.FP64)
+    e = sl.eng
+    for call in (lambda: e.observables(), lambda: e.renormalise_mom(), lambda: e.set_slice_stress_for(s, 4),
+                 lambda: e.set_monitor_for(s), lambda: e.set_restart_layout_for(s),
+                 lambda: e.upload_beads(s.ids, s.types, None, s.x, s.unpbc, s.v),
+                 lambda: e.build_random(s.ids, s.types, 5),
+                 lambda: e.upload_topology(s.bond_head, s.bond_tail, s.bond_k2, s.bond_l0, s.angle_first,
+                                           s.angle_second, s.angle_k3, s.angle_phi0)):
+        with pytest.raises(E.EngineError):
+            call()
+    sl.close()
