@@ -426,7 +426,9 @@ DPD_API int dpd_batch_observables(dpd_engine* e, int32_t box, dpd_obs* out);
  * so every owned bead sees exactly the forces it sees in the whole box and no
  * force travels back.  In upload order the local beads are the owned ones
  * first (dpd_engine_download returns them in the first n_owned rows), then
- * the ghosts. */
+ * the ghosts.  Calls that describe a whole box (bead uploads and builders,
+ * topology uploads, observables, renormalisation, the slice profile, the
+ * monitor, restart and snapshot layouts) return DPD_E_STATE on a slab. */
 
 /* Turns an engine holding its slab's owned beads (the first n_owned of the
  * upload; all of them normally) into a slab, and takes the WHOLE box's
