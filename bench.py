@@ -509,8 +509,8 @@ def run_replica_sweep(args, dev, torch, E):
 
 
 def time_melt(engine_mod, dev, torch, warmup: int, steps: int = 20):
-    """The 6,291,456-bead polymer solution (north_star's >= 1.5e9 bead-steps/s
-    target), mixed precision, the half-shell scheme: per-step CUDA-event times
+    """The 6,291,456-bead polymer solution (target: >= 1.5e9 bead-steps/s),
+    mixed precision, the half-shell scheme: per-step CUDA-event times
     of single-step calls; its state (~1.3 GB) exceeds L2, so no flush."""
     system, desc = workload("polymer")
     ms, prof, launches, status = time_engine(engine_mod, system, engine_mod.MIXED, steps, warmup, dev, torch, False,
@@ -523,7 +523,7 @@ def time_melt(engine_mod, dev, torch, warmup: int, steps: int = 20):
 
 
 def time_sweep(engine_mod, dev, torch, nrep: int = 512, graph_steps: int = 100):
-    """The 512-replica A/B sweep (north_star's >= 3x over replicas one at a
+    """The 512-replica A/B sweep (target: >= 3x over the replicas one at a
     time): one batch of all replicas as captured 100-step graphs against the
     same replicas stepped engine by engine, one 100-step call each."""
     ns = argparse.Namespace(replicas=nrep, graph_steps=graph_steps, steps=1, warmup=1, pair_scheme="half",
