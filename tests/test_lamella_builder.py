@@ -62,3 +62,21 @@ def test_lattice_outside_the_box_is_an_error():
     g = load("lamella_z_straight")
     with pytest.raises(ValueError):
         O.lamella_state(g["L"], 1.0, 1, g["poly_first"], g["poly_type"], 0, 0, 8, 2, 0.5, 12.0, True, 0.5)
+
+
+def test_control_file_lamella_block(tmp_path):
+    """workloads.lamella_block: the State lamella block of a control data
+    file as CInitialStateLamella reads it (InitialStateLamella.cpp), in place
+    of State random."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from osprey_dpd_b200 import workloads as W
+    s = W.bilayer(cells=(8, 8, 12), nlipids=40)
+    path = tmp_path / "dmpci.t"
+    W.write_dmpci(s, str(path), 10, state=W.lamella_block("Lipid", normal=(0, 1, 0), centre=0.4, thickness=4.5,
+                                                         linearise=False, upper_fraction=0.25))
+    text = path.read_text().split("\n")
+    k = text.index("State\tlamella")
+    body = [t.split() for t in text[k + 1:k + 8]]
+    assert body == [["Polymer", "Lipid"], ["Normal", "0", "1", "0"], ["Centre", "0.4"], ["Thickness", "4.5"],
+                    ["Linearise", "0"], ["UpperFraction", "0.25"], ["Polymerise", "0"]]
+    assert "State\trandom" not in text

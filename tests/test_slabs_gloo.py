@@ -150,3 +150,23 @@ def test_slab_bounds_and_limits():
     from osprey_dpd_b200 import slabs
     assert [slabs.slab_bounds(10, 3, r) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
     assert slabs.slab_bounds(12, 1, 0) == (0, 12)
+
+
+def test_combine_owned_sums():
+    """DeviceSlabs.combine: kT = sum v^2 / 3N and P = (sum v^2 + trace W) / 3V
+    of the whole box from the slabs' owned sums (CMonitor::
+    CalculateSingleBeadData, Monitor.cpp:979-982)."""
+    sys.path.insert(0, ROOT)
+    from osprey_dpd_b200 import slabs as S
+    parts = [{"n": 10, "sum_v": np.array([1.0, 0.0, -1.0]), "sum_v2": np.array([10.0, 11.0, 9.0]),
+              "virial": np.arange(9.0), "has_virial": True},
+             {"n": 20, "sum_v": np.array([-1.0, 0.5, 1.0]), "sum_v2": np.array([20.0, 19.0, 21.0]),
+              "virial": np.ones(9), "has_virial": True}]
+    o = S.DeviceSlabs.combine(parts, volume=100.0)
+    assert o["n"] == 30
+    np.testing.assert_allclose(o["sum_v"], [0.0, 0.5, 0.0])
+    assert o["kT"] == (30.0 + 60.0) / 90.0
+    tr = (0.0 + 4.0 + 8.0) + 3.0
+    assert o["pressure"] == (90.0 + tr) / 300.0
+    parts[1]["has_virial"] = False
+    assert S.DeviceSlabs.combine(parts, 100.0)["pressure"] is None
