@@ -24,10 +24,11 @@ def _cases():
 
 
 FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("stats_", "restart_", "random_", "paraview_", "glue_")))
+                  if not os.path.basename(p).startswith(("stats_", "restart_", "random_", "paraview_", "glue_",
+                                                         "lamella_")))
 # stats_*: tests/golden/make_stats.py; restart_*: tests/golden/make_restart_golden.py;
 # random_*: tests/golden/make_random_golden.py; paraview_*: tests/golden/make_paraview_golden.py;
-# glue_*: tests/golden/make_glue_golden.py
+# glue_*: tests/golden/make_glue_golden.py; lamella_*: tests/golden/make_lamella_golden.py
 
 
 @pytest.mark.parametrize("name", FIXTURES)
