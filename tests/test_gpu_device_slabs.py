@@ -263,3 +263,15 @@ def test_slab_refuses_whole_box_calls():
         with pytest.raises(E.EngineError):
             call()
     sl.close()
+
+
+def test_device_slabs_at_benchmark_size():
+    """The benchmark's 393,216-bead H3T6 bilayer in four slabs (one process,
+    FP64, full shell) against one engine stepping the whole box: 3 steps,
+    every bead owned once, the same bounds as the small boxes."""
+    from osprey_dpd_b200 import engine as E, workloads as W2
+    s = W2.bilayer()
+    ref, ids = _single_box(s, E.FP64, steps=3)
+    got, owned, status = _local_run(s, 4, E.FP64, steps=3)
+    assert owned == [s.n] * 3 and all(st == 0 for st in status)
+    _compare(got, ref, ids)
