@@ -144,16 +144,24 @@ __device__ __forceinline__ void publish_status(const unsigned* status, unsigned*
 // ------------------------------------------------------------- UpdatePos
 
 // One bead's drift and cell move; returns its new cell and writes x, img and
-// cell of slot s.  x0, v0, f0 are the bead's position, velocity and force.
+// cell of slot s (a frozen bead's unchanged ones too: the output may be the
+// separate buffers of a drift done ahead).  x0, v0, f0 are the bead's
+// position, velocity and force.
 __device__ __forceinline__ int drift_and_move(const StepConst* __restrict__ K, const Box* __restrict__ boxes,
                                               int n, int s, int c, int tfl, const double x0[3], const double v0[3],
                                               const double f0[3], uint32_t im0, double* __restrict__ x,
                                               uint32_t* __restrict__ img, int* __restrict__ cell, unsigned& bad)
 {
-    if (flag_frozen(tfl)) return c;
+    if (flag_frozen(tfl)) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d * n + s] = x0[d];
+        img[s] = im0;
+        cell[s] = c;
+        return c;
+    }
+    const Box& B = boxes[flag_box(tfl)];
     int cnew = c;
     const double dt = K->dt, h2 = K->halfdt2;
-    const Box& B = boxes[flag_box(tfl)];
     const int nx = B.nc[0], ny = B.nc[1], nz = B.nc[2];
     const int cl = c - B.cell_base;
     int ci[3];

@@ -39,6 +39,26 @@ def test_frozen_beads(engine_mod, oracle_mod, precision):
     assert np.array_equal(eng.cells(), orc.cells())
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+def test_frozen_beads_across_calls(engine_mod, oracle_mod, precision):
+    """Frozen beads, bonded ones among them, over several calls: the last
+    step of a call drifts the next step's state into separate buffers, which
+    must carry the frozen beads' unchanged positions, images and cells too."""
+    s = W.bilayer(cells=(12, 12, 12), nlipids=60)
+    s.movable[::5] = 0
+    eng, orc = _both(engine_mod, oracle_mod, s, precision)
+    for first in (1, 3, 4):
+        eng.step(first, 2 if first == 1 else 1)
+    eng.step(5, 2)
+    orc.step(1, 6)
+    g, o = eng.download(), orc.state()
+    fz = s.movable == 0
+    assert np.array_equal(g["x"][fz], s.x[fz]) and np.array_equal(g["v"][fz], s.v[fz])
+    assert np.array_equal(eng.cells(), orc.cells())
+    assert rel_err(g["f"], o["f"]) < (1e-4 if precision == 0 else 1e-10)
+    assert eng.status() == 0
+
+
 def test_face_landing_bead_keeps_its_cell(engine_mod, oracle_mod):
     s = _sparse_box(5)
     s.x[0] = [1.5, 1.5, 1.5]
