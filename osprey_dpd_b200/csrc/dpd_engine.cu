@@ -583,11 +583,18 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
     double* x_in = ahead_in ? e->d_xa : e->d_x[a];
     uint32_t* img_in = ahead_in ? e->d_imga : e->d_img[a];
     int* cell_in = ahead_in ? e->d_cella : e->d_cell[a];
+    // The full shell keeps every cell's beads in the order of their previous
+    // slots (bitwise reproducible forces): arrival ranks, a permutation, then a
+    // gather.  The half-shell schemes add forces with atomics in no fixed order
+    // anyway: their beads are scattered into the cells by k_gather, one kernel
+    // less, and without ranks the counting atomics return nothing.
+    const bool stable = e->pair_scheme == DPD_PAIR_FULL_SHELL;
+    int* rank_out = stable ? e->d_rank : nullptr;
     if (first && !from_ahead) {
         {
             Timed t(e, DPD_KERNEL_UPDATE_POS);
             CU(launch_step(e, k_update_pos<real>, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_x[a], e->d_v[a],
-                           (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a], e->d_rank, e->d_count,
+                           (const real*)e->d_F, e->d_tf[a], e->d_img[a], e->d_cell[a], rank_out, e->d_count,
                            e->d_block_count, e->d_status, first ? e->d_seen : (unsigned*)nullptr));
         }
         if ((rc = check_launch(e, "k_update_pos"))) return rc;
@@ -597,14 +604,9 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         // the call's first kernel publishes the status word (k_update_pos when it runs)
         CU(launch_step(e, k_scan_cells, e->nchunk, kScanThreads, 0, st, (int)e->ncell, n, e->d_count,
                        e->d_block_count, e->d_start, (const unsigned*)e->d_status,
-                       (first && from_ahead) ? e->d_seen : (unsigned*)nullptr));
+                       (first && from_ahead) ? e->d_seen : (unsigned*)nullptr, stable ? 1 : 0));
     }
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
-    // The full shell keeps every cell's beads in the order of their previous
-    // slots (bitwise reproducible forces): arrival permutation, then a gather.
-    // The half-shell schemes add forces with atomics in no fixed order anyway:
-    // their beads are scattered to cell start + arrival rank, one kernel less.
-    const bool stable = e->pair_scheme == DPD_PAIR_FULL_SHELL;
     if (stable) {
         {
             Timed t(e, DPD_KERNEL_PERMUTE);
@@ -622,7 +624,7 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
                        e->d_bid[a], e->d_tf[a], img_in, cell_in, e->d_x[b], e->d_v[b], (real*)e->d_Fold,
                        e->d_bid[b], e->d_tf[b], e->d_img[b], e->d_cell[b], e->d_pid[a], e->d_pid[b], (V4*)e->d_pos4,
                        (V4*)e->d_vel4, e->d_ubuf, (const double*)(e->off_active ? e->d_off : nullptr), zero_F,
-                       (const int*)(stable ? nullptr : e->d_rank), (int)e->nchunk, e->d_block_count));
+                       (int)e->nchunk, e->d_block_count, stable ? (int*)nullptr : e->d_count));
     }
     if ((rc = check_launch(e, "k_gather"))) return rc;
     // bond and bond-pair forces: a branch beside the pair kernel (on the
@@ -725,7 +727,7 @@ int queue_step(dpd_engine* e, bool sample, bool first, bool last, bool from_ahea
         CU(launch_step(e, kern, nb, kThreads, 0, st, n, e->d_K, e->d_boxes, e->d_step, (const double*)e->d_x[b],
                        e->d_v[b], (real*)e->d_F, (const real*)e->d_Fold, e->d_bid[b], e->d_tf[b],
                        (const double4*)e->d_Fb, (const double*)e->d_Sb, (real*)e->d_stress, e->d_partials,
-                       (const uint32_t*)e->d_img[b], (const int*)e->d_cell[b], e->d_rank, e->d_count,
+                       (const uint32_t*)e->d_img[b], (const int*)e->d_cell[b], rank_out, e->d_count,
                        e->d_block_count, e->d_status, xo, imgo, cello));
     }
     if ((rc = check_launch(e, "k_update_mom"))) return rc;
@@ -1020,6 +1022,8 @@ int dpd_engine_set_pair_scheme(dpd_engine* e, int32_t scheme)
         return fail(e, DPD_E_ARG, "unknown pair scheme");
     CU(cudaSetDevice(e->device));
     CU(cudaStreamSynchronize(e->s()));
+    // a drift done ahead counted arrivals for the old scheme's gather (ranks or not)
+    if (int rc0 = drop_ahead(e)) return rc0;
     e->pair_scheme = scheme;
     memset(e->pair_attr_set, 0, sizeof e->pair_attr_set);
     drop_graphs(e);
@@ -1251,7 +1255,7 @@ static int upload_staged(dpd_engine* e, int64_t n, const int32_t* box, const int
     e->n = n;
     // cell starts, then the slot order: by cell, inside a cell by upload index
     k_scan_cells<<<e->nchunk, kScanThreads, 0, st>>>((int)e->ncell, (int)n, e->d_count, e->d_block_count, e->d_start,
-                                                     (const unsigned*)e->d_status, (unsigned*)nullptr);
+                                                     (const unsigned*)e->d_status, (unsigned*)nullptr, 1);
     if ((rc = check_launch(e, "k_scan_cells"))) return rc;
     CU(cudaMemsetAsync(e->d_block_count, 0, sizeof(int) * (size_t)e->nchunk, st));
     k_up_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>((int)n, e->d_up_cell, e->d_start, e->d_count,

@@ -224,8 +224,10 @@ __device__ __forceinline__ int drift_and_move(const StepConst* __restrict__ K, c
 
 // Warp-aggregated counting of the beads arriving in each cell: lanes bound
 // for the same cell take one atomic (beads are cell-sorted, so a warp spans
-// ~11 cells) and ranks follow lane order inside the group; one atomic per scan
-// chunk per warp as well.  Called by every lane of the warp.
+// ~11 cells); with `rank`, each bead's rank inside its cell (lane order inside
+// the group) for a gather in a fixed order, else the count alone, by
+// reductions that return nothing (k_gather then claims the slots).  One
+// reduction per scan chunk per warp as well.  Called by every lane of the warp.
 __device__ __forceinline__ void count_arrival(bool live, int s, int cnew, int* __restrict__ rank,
                                               int* __restrict__ count, int* __restrict__ block_count)
 {
@@ -234,10 +236,14 @@ __device__ __forceinline__ void count_arrival(bool live, int s, int cnew, int* _
         const int lane = threadIdx.x & 31;
         const unsigned peers = __match_any_sync(act, cnew);
         const int leader = __ffs(peers) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&count[cnew], __popc(peers));
-        base = __shfl_sync(act, base, leader);
-        rank[s] = base + __popc(peers & ((1u << lane) - 1u));
+        if (rank) {
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&count[cnew], __popc(peers));
+            base = __shfl_sync(act, base, leader);
+            rank[s] = base + __popc(peers & ((1u << lane) - 1u));
+        } else if (lane == leader) {
+            atomicAdd(&count[cnew], __popc(peers));   // result unused: a reduction
+        }
         const int chunk = cnew / kScanChunk;
         const unsigned cpeers = __match_any_sync(act, chunk);
         if (lane == __ffs(cpeers) - 1) atomicAdd(&block_count[chunk], __popc(cpeers));   // result unused: a reduction
@@ -287,10 +293,10 @@ __global__ void __launch_bounds__(256, 6) k_update_pos(
 
 // start[c] = sum of count[0..c); one block per chunk of kScanChunk cells.  The
 // chunk's base is the sum of the per-chunk totals counted by k_update_pos.
-// Counts are cleared for the next step.
+// With clear, the counts are cleared for the next step.
 static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     int ncell, int n, int* __restrict__ count, const int* __restrict__ block_count,
-    int* __restrict__ start, const unsigned* status, unsigned* seen)
+    int* __restrict__ start, const unsigned* status, unsigned* seen, int clear)
 {
     pdl_wait();
     pdl_launch();
@@ -298,6 +304,18 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     __shared__ int warp_sum[kScanThreads / 32];
     __shared__ int base_s;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    // this thread's cell counts first (one 16-byte load), so their memory
+    // round trip overlaps the one of the chunk totals below
+    const int c0 = b * kScanChunk + t * kScanPerThread;
+    int vals[kScanPerThread];
+    static_assert(kScanPerThread == 4, "one int4 per thread");
+    if (c0 + kScanPerThread <= ncell) {
+        const int4 q = *reinterpret_cast<const int4*>(count + c0);
+        vals[0] = q.x; vals[1] = q.y; vals[2] = q.z; vals[3] = q.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanPerThread; ++k) vals[k] = (c0 + k < ncell) ? count[c0 + k] : 0;
+    }
     int acc = 0;
     for (int k = t; k < b; k += kScanThreads) acc += block_count[k];
 #pragma unroll
@@ -311,15 +329,9 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     }
     __syncthreads();
     const int base = base_s;
-    const int c0 = b * kScanChunk + t * kScanPerThread;
-    int vals[kScanPerThread];
     int tot = 0;
 #pragma unroll
-    for (int k = 0; k < kScanPerThread; ++k) {
-        const int c = c0 + k;
-        vals[k] = (c < ncell) ? count[c] : 0;
-        tot += vals[k];
-    }
+    for (int k = 0; k < kScanPerThread; ++k) tot += vals[k];
     // exclusive scan of per-thread totals across the block
     int inc = tot;
 #pragma unroll
@@ -333,12 +345,14 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_cells(
     int wbase = 0;
     for (int w = 0; w < wid; ++w) wbase += warp_sum[w];
     int run = base + wbase + inc - tot;
+    // clear = 0 leaves the counts for k_gather to claim slots from (it
+    // returns them to zero)
 #pragma unroll
     for (int k = 0; k < kScanPerThread; ++k) {
         const int c = c0 + k;
         if (c < ncell) {
             start[c] = run;
-            count[c] = 0;
+            if (clear) count[c] = 0;
         }
         run += vals[k];
     }
@@ -373,19 +387,22 @@ __global__ void __launch_bounds__(256, 6) k_gather(
     uint32_t* __restrict__ img_out, int* __restrict__ cell_out, const int* __restrict__ pid_in,
     int* __restrict__ pid_out, typename Vec4<real>::type* __restrict__ pos4,
     typename Vec4<real>::type* __restrict__ vel4, double4* __restrict__ ubuf, const double* __restrict__ off,
-    int zero_F, const int* __restrict__ rank, int nchunk, int* __restrict__ block_count)
+    int zero_F, int nchunk, int* __restrict__ block_count, int* __restrict__ claim)
 {
     pdl_wait();
     pdl_launch();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    // Scatter mode (rank != NULL): thread t moves source slot t to its cell
-    // start plus its arrival rank, in no fixed order inside the cell, and the
-    // arrival permutation (k_permute) is not needed; it also clears the
-    // per-chunk totals for the next step.  Gather mode: thread t fills slot t
-    // from perm, in the order of the beads' previous slots.
-    if (rank && t < nchunk) block_count[t] = 0;
+    // Scatter mode (claim = the arrival counts): thread t moves source slot t
+    // into its cell, to a slot that the warp's beads bound for the cell take
+    // from the count by one atomic subtraction (in no fixed order inside the
+    // cell), which leaves every count at zero for the next step; the arrival
+    // permutation (k_permute) is not needed, and the per-chunk totals are
+    // cleared for the next step.  Gather mode: thread t fills slot t from
+    // perm, in the order of the beads' previous slots.
+    if (claim && t < nchunk) block_count[t] = 0;
+    const unsigned act = claim ? __ballot_sync(0xffffffffu, t < n) : 0u;
     if (t >= n) return;
-    const int s = rank ? t : perm[t];
+    const int s = claim ? t : perm[t];
     // the bead's state is independent of its final slot: load it before the
     // rank scan so both memory round trips overlap
     const int c = cell_in[s];
@@ -402,8 +419,14 @@ __global__ void __launch_bounds__(256, 6) k_gather(
         fs[q] = F_in[q * n + s];
     }
     int o;
-    if (rank) {
-        o = start[c] + rank[s];
+    if (claim) {
+        const int lane = threadIdx.x & 31;
+        const unsigned peers = __match_any_sync(act, c);
+        const int leader = __ffs(peers) - 1, k = __popc(peers);
+        int top = 0;
+        if (lane == leader) top = atomicSub(&claim[c], k);
+        top = __shfl_sync(peers, top, leader);
+        o = start[c] + top - k + __popc(peers & ((1u << lane) - 1u));
     } else {
         const int beg = start[c], end = start[c + 1];
         int k = 0;

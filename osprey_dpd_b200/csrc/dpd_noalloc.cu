@@ -264,7 +264,7 @@ static int pair_forces_on_current_device(const dpd_params* p, int64_t step, int6
     k_na_clear<<<nblk(std::max(nc, 1)), kNaThreads, 0, st>>>(nc, nchunk, dCount, dChunk, dStatus);
     k_na_bin<<<nblk(nn), kNaThreads, 0, st>>>(nn, dK, x3, dCell, dRank, dCount, dChunk, dStatus);
     k_scan_cells<<<nchunk, kScanThreads, 0, st>>>(nc, nn, dCount, dChunk, dStart, (const unsigned*)nullptr,
-                                                  (unsigned*)nullptr);
+                                                  (unsigned*)nullptr, 1);
     k_na_place<<<nblk(nn), kNaThreads, 0, st>>>(nn, dCell, dRank, dStart, dPerm);
     k_na_shadows<<<nblk(nn), kNaThreads, 0, st>>>(nn, dK, dPerm, dCell, dStart, x3, v3, type, id, dOrder,
                                                   dSlotCell, dPos, dVel, dStatus);
