@@ -1,24 +1,31 @@
 // dpd_kernels.cuh -- sm_100a kernels of one DPD timestep.
 //
 // Device layout ("slot order"): beads sorted by CNT cell, cells in the
-// reference's index order nx*(ny*iz+iy)+ix (SimBox.cpp:888-920), and inside a
-// cell by their slot in the previous step (a stable counting sort), so the
-// order -- and every floating-point sum -- is deterministic.  Per-bead arrays
-// are structure-of-arrays; 3-vectors are three planes of n values.
+// reference's index order nx*(ny*iz+iy)+ix (SimBox.cpp:888-920).  Under the
+// full-shell pair scheme the beads of a cell keep the order of their
+// previous slots (a stable counting sort), so the order -- and every
+// floating-point sum -- is deterministic; the half-shell schemes add forces
+// with atomics in no fixed order anyway and scatter each cell's beads in
+// any order.  Per-bead arrays are structure-of-arrays; 3-vectors are three
+// planes of n values.
 //
 // One step, in the reference's order (CSimBox::Evolve, SimBox.cpp:977-1120):
 //   k_update_pos   UpdatePos: drift, incremental cell move + PBC wrap,
-//                  per-cell counts                 (CNTCell.cpp:1634-2262)
+//                  per-cell arrival counts         (CNTCell.cpp:1634-2262);
+//                  first step of a call only, the others drift in the
+//                  k_update_mom before them
 //   k_scan_cells   cell start offsets (exclusive prefix sum of the counts)
-//   k_permute      arrival slot -> new slot map
-//   k_gather       stable per-cell order, permutes the state, writes the
-//                  cell-relative FP32/FP64 shadows the force kernel reads
-//   k_pair_forces  conservative + dissipative + random pair forces over the
-//                  27 neighbour cells                (CNTCell.cpp:1103-1572)
-//   k_update_mom   bond and bond-pair forces, UpdateMom, FP64 sums on
-//                  sample steps                      (Bond.cpp:111-162,
-//                  BondPair.cpp:138-286, CNTCell.cpp:2280-2310,
-//                  Monitor.cpp:790-1040)
+//   k_permute      arrival slot -> new slot map (full shell only)
+//   k_gather       permutes the state into the new slot order (half shell:
+//                  slots claimed from the counts), writes the cell-relative
+//                  FP32/FP64 shadows the force kernel reads
+//   k_bonds        bond and bond-pair forces, FP64, beside the pair kernel
+//                  (Bond.cpp:111-162, BondPair.cpp:138-286)
+//   pair kernel    conservative + dissipative + random pair forces over the
+//                  neighbour cells (pair_forces.cuh; CNTCell.cpp:1103-1572)
+//   k_update_mom   adds the bonded forces, UpdateMom, FP64 sums on sample
+//                  steps, then the next step's UpdatePos
+//                  (CNTCell.cpp:2280-2310, Monitor.cpp:790-1040)
 // Non-template kernels have internal linkage so that more than one
 // translation unit of the library can include this header.
 #pragma once
